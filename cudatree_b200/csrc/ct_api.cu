@@ -1,0 +1,215 @@
+// extern "C" entry points of libcudatree_b200.so (declared in
+// include/cudatree_b200.h).  Each one validates its arguments on the host,
+// launches on the caller's stream and returns a status code.
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ct_internal.cuh"
+
+namespace ct {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features);
+int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
+                      uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
+size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
+int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
+        const ct_fit_options* o, const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
+int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
+                 const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
+                 uint32_t* ov);
+int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_trees, const float* x,
+            uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
+            cudaStream_t st);
+size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features);
+int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
+            size_t wsb, cudaStream_t st);
+
+}  // namespace ct
+
+using namespace ct;
+
+#define CT_GUARD(body)                                   \
+  try {                                                  \
+    body                                                 \
+  } catch (const std::exception& e) {                    \
+    set_last_error(std::string("exception: ") + e.what()); \
+    return CT_ERR_INTERNAL;                              \
+  }
+
+extern "C" {
+
+const char* ct_version(void) { return "cudatree_b200 0.1.0 (sm_100a)"; }
+
+int ct_last_error(char* buf, size_t len) {
+  const std::string& s = g_last_error;
+  if (buf && len) {
+    const size_t n = s.size() < len - 1 ? s.size() : len - 1;
+    std::memcpy(buf, s.data(), n);
+    buf[n] = 0;
+  }
+  return (int)s.size();
+}
+
+int ct_presort_workspace_size(uint32_t n_rows, uint32_t n_features, size_t* bytes) {
+  CT_ARG_CHECK(bytes, "bytes is NULL");
+  *bytes = presort_workspace_bytes(n_rows, n_features);
+  return CT_OK;
+}
+
+int ct_presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out,
+               void* workspace, size_t workspace_bytes, void* stream) {
+  CT_GUARD(return presort(x_fm, n_rows, n_features, index_bytes, out, workspace, workspace_bytes,
+                          (cudaStream_t)stream);)
+}
+
+int ct_bootstrap_workspace_size(const ct_problem* p, size_t* bytes) {
+  CT_ARG_CHECK(p && bytes, "NULL argument");
+  *bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features);
+  return CT_OK;
+}
+
+int ct_bootstrap_compact(const ct_problem* p, const ct_lists* lists, uint32_t slot, uint32_t tree,
+                         uint32_t* n_in_dev, void* workspace, size_t workspace_bytes, void* stream) {
+  CT_GUARD({
+    CT_TRY(check_problem(p));
+    CT_ARG_CHECK(lists && lists->si0 && lists->mark && n_in_dev, "NULL argument");
+    if (p->bootstrap) CT_ARG_CHECK(workspace, "workspace is NULL");
+    if (workspace) CT_CUDA_TRY(cudaMemsetAsync(workspace, 0, 16, (cudaStream_t)stream));
+    return bootstrap_compact(p, lists, slot, tree, n_in_dev, workspace, workspace_bytes, (cudaStream_t)stream);
+  })
+}
+
+int ct_split_workspace_size(const ct_problem* p, uint32_t n_nodes, uint64_t total_samples, size_t* bytes) {
+  CT_ARG_CHECK(p && bytes, "NULL argument");
+  View v = make_view(p, nullptr);
+  *bytes = level_scratch_bytes(v, level_caps(v, DEFAULT_SCAN_PIECE, LevelBounds{n_nodes, total_samples}));
+  return CT_OK;
+}
+
+static int carve_api_scratch(const ct_problem* p, const ct_lists* l, uint32_t n_nodes, uint64_t total,
+                             void* ws, size_t wsb, View* v, LevelScratch* s) {
+  *v = make_view(p, l);
+  Arena a{reinterpret_cast<char*>(ws), wsb, 0};
+  if (!carve_level_scratch(a, *v, level_caps(*v, DEFAULT_SCAN_PIECE, LevelBounds{n_nodes, total}), s)) {
+    set_last_error("workspace too small");
+    return CT_ERR_OOM;
+  }
+  return CT_OK;
+}
+
+static int node_total(const ct_node* nodes, uint32_t n_nodes, uint64_t* total, cudaStream_t st) {
+  // total samples bound: read the node sizes (API path only; the fit keeps it on the host)
+  std::vector<ct_node> h(n_nodes);
+  CT_CUDA_TRY(cudaMemcpyAsync(h.data(), nodes, n_nodes * sizeof(ct_node), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  uint64_t t = 0;
+  for (auto& n : h) t += n.n;
+  *total = t;
+  return CT_OK;
+}
+
+int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* nodes, const uint32_t* totals,
+                   uint32_t n_nodes, ct_split_result* out, uint32_t* selected, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+  CT_GUARD({
+    CT_TRY(check_problem(p));
+    CT_ARG_CHECK(lists && lists->si0 && lists->si1 && nodes && totals && out, "NULL argument");
+    if (n_nodes == 0) return CT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t total = 0;
+    CT_TRY(node_total(nodes, n_nodes, &total, st));
+    View v;
+    LevelScratch s;
+    CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
+    s.result = out;
+    CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
+    CT_TRY(launch_reset_step(s.ctr, n_nodes, st));
+    CT_TRY(launch_split(v, p->index_bytes, p->label_bytes, nodes, totals, s, LevelBounds{n_nodes, total},
+                        DEFAULT_SCAN_PIECE, st));
+    if (selected)
+      CT_CUDA_TRY(cudaMemcpyAsync(selected, s.sel, (size_t)n_nodes * p->max_features * sizeof(uint32_t),
+                                  cudaMemcpyDeviceToDevice, st));
+    Counters h;
+    CT_CUDA_TRY(cudaMemcpyAsync(&h, s.ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h.error) {
+      set_last_error("split scan: device capacity check failed");
+      return CT_ERR_CAPACITY;
+    }
+    return CT_OK;
+  })
+}
+
+int ct_partition_workspace_size(const ct_problem* p, uint32_t n_nodes, uint64_t total_samples, size_t* bytes) {
+  return ct_split_workspace_size(p, n_nodes, total_samples, bytes);
+}
+
+int ct_partition_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* nodes,
+                       const ct_split_result* splits, uint32_t n_nodes, void* workspace, size_t workspace_bytes,
+                       void* stream) {
+  CT_GUARD({
+    CT_TRY(check_problem(p));
+    CT_ARG_CHECK(lists && lists->si0 && lists->si1 && lists->mark && nodes && splits, "NULL argument");
+    if (n_nodes == 0) return CT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint64_t total = 0;
+    CT_TRY(node_total(nodes, n_nodes, &total, st));
+    View v;
+    LevelScratch s;
+    CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
+    s.result = const_cast<ct_split_result*>(splits);
+    CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
+    CT_TRY(launch_reset_step(s.ctr, n_nodes, st));
+    TreeView tv;
+    std::memset(&tv, 0, sizeof(tv));
+    CT_TRY(launch_partition(v, p->index_bytes, p->label_bytes, nodes, s, LevelBounds{n_nodes, total}, tv, st));
+    Counters h;
+    CT_CUDA_TRY(cudaMemcpyAsync(&h, s.ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    if (h.error & DEV_ERR_TIMEOUT) {
+      set_last_error("partition look-back wait gave up");
+      return CT_ERR_TIMEOUT;
+    }
+    if (h.error) {
+      set_last_error("partition: device capacity check failed");
+      return CT_ERR_CAPACITY;
+    }
+    return CT_OK;
+  })
+}
+
+int ct_fit_workspace_size(const ct_problem* p, uint32_t n_trees, const ct_fit_options* opt, size_t* bytes) {
+  CT_ARG_CHECK(p && opt && bytes, "NULL argument");
+  *bytes = fit_workspace_bytes(p, n_trees, opt);
+  return CT_OK;
+}
+
+int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint32_t n_trees,
+           const ct_fit_options* opt, const ct_tree_buffers* trees, void* workspace, size_t workspace_bytes,
+           void* stream) {
+  CT_GUARD(return fit(p, lists, first_tree, n_trees, opt, trees, workspace, workspace_bytes,
+                      (cudaStream_t)stream);)
+}
+
+int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature,
+                         const float* threshold, const uint32_t* value, uint32_t n_nodes, uint32_t* out_left,
+                         uint32_t* out_right, uint16_t* out_feature, float* out_threshold, uint32_t* out_value) {
+  CT_ARG_CHECK(left && right && feature && threshold && value && out_left && out_right && out_feature &&
+                   out_threshold && out_value,
+               "NULL argument");
+  CT_GUARD(return canonicalize(left, right, feature, threshold, value, n_nodes, out_left, out_right, out_feature,
+                               out_threshold, out_value);)
+}
+
+int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,
+               uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
+               void* stream) {
+  CT_GUARD(return predict(nodes, tree_offset, n_trees, x, n_rows, n_features, n_classes, votes, pred,
+                          (cudaStream_t)stream);)
+}
+
+}  // extern "C"

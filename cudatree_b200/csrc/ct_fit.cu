@@ -1,0 +1,398 @@
+// Forest fit orchestration.
+//
+// CT_FIT_PLAIN mirrors the reference tree builder (random_tree.py:461-676):
+// one tree at a time; nodes larger than bfs_threshold are split one by one
+// in depth-first order with a host round trip per node (random_tree.py:580-676),
+// smaller nodes are queued and split breadth-first one level per step for the
+// tree (random_tree.py:309-458).
+//
+// CT_FIT_BATCHED grows every tree of the call at once, level-synchronously:
+// one step splits every pending node of every tree, with one host read of
+// the step counters per level.  Both forms run the same level kernels and the
+// same canonical rule, so their trees are identical after canonical
+// renumbering.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "ct_internal.cuh"
+
+namespace ct {
+
+size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features);
+int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
+                      uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
+
+namespace {
+
+constexpr uint32_t CHUNK_NODES_MAX = 1u << 20;
+
+template <typename IdxT, typename LabT>
+__global__ void k_root(View v, const uint32_t* n_in, uint32_t slot, uint64_t seed, uint32_t tree,
+                       TreeView tv, ct_node* out, uint32_t* out_tot, uint32_t cap, Counters* ctr) {
+  extern __shared__ uint32_t hist[];
+  __shared__ uint32_t s_idx;
+  const uint32_t C = v.n_classes;
+  for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) hist[c] = 0;
+  __syncthreads();
+  const uint32_t n = n_in[slot];
+  const IdxT* lst = list_ptr<IdxT>(v, 0, slot, 0);
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&hist[label_of<LabT>(v, lst[i])], 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t ts = slot + tv.slot_base;
+    tv.n_nodes[ts] = 1;
+    ct_node nd;
+    nd.slot = slot;
+    nd.start = 0;
+    nd.n = n;
+    nd.raw_id = 0;
+    nd.key = root_key(tree_key(seed, tree));
+    nd.impurity = 1.0f;
+    nd.buf = 0;
+    s_idx = NONE;
+    if (n < v.mss || n == 0) {
+      const size_t off = (size_t)ts * tv.capacity;
+      tv.left[off] = 0;
+      tv.right[off] = 0;
+      tv.feature[off] = 0;
+      tv.threshold[off] = 0.f;
+      tv.value[off] = n ? label_of<LabT>(v, lst[0]) : 0u;
+    } else {
+      const uint32_t idx = atomicAdd(&ctr->n_next, 1u);
+      if (idx < cap) {
+        out[idx] = nd;
+        atomicAdd(&ctr->next_total, (unsigned long long)n);
+        s_idx = idx;
+      } else {
+        atomicOr(&ctr->error, DEV_ERR_CAPACITY);
+      }
+    }
+  }
+  __syncthreads();
+  if (s_idx != NONE)
+    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) out_tot[(size_t)s_idx * C + c] = hist[c];
+}
+
+__global__ void k_begin_level(Counters* c) {
+  c->n_next = 0;
+  c->n_small = 0;
+  c->next_total = 0;
+  c->small_total = 0;
+}
+
+struct FitLayout {
+  uint32_t n_slots;
+  uint32_t cap_list;
+  uint32_t chunk;
+  uint32_t scan_piece;
+  uint32_t* n_in;
+  ct_node* list[2];
+  uint32_t* tot[2];
+  LevelScratch s;
+  void* boot_ws;
+  size_t boot_bytes;
+  size_t bytes;
+};
+
+bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char* base, size_t size,
+            FitLayout* L) {
+  View v = make_view(p, nullptr);
+  const uint32_t slots = (o->mode == CT_FIT_PLAIN) ? 1u : n_trees;
+  const uint64_t S = (uint64_t)slots * p->n_rows;
+  const uint64_t cap_list64 = S / 2 + slots + 2;
+  L->n_slots = slots;
+  L->cap_list = (uint32_t)std::min<uint64_t>(cap_list64, 0xffffffffull);
+  L->chunk = std::min<uint32_t>(L->cap_list, CHUNK_NODES_MAX);
+  L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
+  Arena a{base, size, 0};
+  L->n_in = a.take<uint32_t>(slots);
+  for (int i = 0; i < 2; ++i) {
+    L->list[i] = a.take<ct_node>(L->cap_list);
+    L->tot[i] = a.take<uint32_t>((size_t)L->cap_list * p->n_classes);
+  }
+  L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features);
+  L->boot_ws = a.take<char>(L->boot_bytes);
+  LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
+  carve_level_scratch(a, v, caps, &L->s);
+  L->bytes = a.used + 256;
+  return base != nullptr && a.ok();
+}
+
+struct Host {
+  Counters c;
+};
+
+int read_counters(const FitLayout& L, Counters* h, cudaStream_t st) {
+  CT_CUDA_TRY(cudaMemcpyAsync(h, L.s.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h->error) {
+    if (h->error & DEV_ERR_TIMEOUT) {
+      set_last_error("device look-back wait gave up (timeout)");
+      return CT_ERR_TIMEOUT;
+    }
+    if (h->error & DEV_ERR_CAPACITY) {
+      set_last_error("device work-list or tree capacity exceeded");
+      return CT_ERR_CAPACITY;
+    }
+    set_last_error("device consistency check failed");
+    return CT_ERR_INTERNAL;
+  }
+  return CT_OK;
+}
+
+int check_boot_error(const FitLayout& L, cudaStream_t st) {
+  uint32_t w[2] = {0, 0};
+  CT_CUDA_TRY(cudaMemcpyAsync(w, L.boot_ws, sizeof(w), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (w[1]) {
+    set_last_error("bootstrap compaction look-back wait gave up");
+    return CT_ERR_TIMEOUT;
+  }
+  return CT_OK;
+}
+
+template <typename IdxT, typename LabT>
+int launch_root(const View& v, const FitLayout& L, uint32_t slot, uint64_t seed, uint32_t tree,
+                const TreeView& tv, int cur, cudaStream_t st) {
+  k_root<IdxT, LabT><<<1, 256, v.n_classes * sizeof(uint32_t), st>>>(v, L.n_in, slot, seed, tree, tv,
+                                                                     L.list[cur], L.tot[cur], L.cap_list,
+                                                                     L.s.ctr);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot, uint32_t tree,
+         const TreeView& tv, int cur, cudaStream_t st) {
+  const uint32_t ib = p->index_bytes, lb = p->label_bytes;
+  if (ib == 2 && lb == 1) return launch_root<uint16_t, uint8_t>(v, L, slot, p->seed, tree, tv, cur, st);
+  if (ib == 2 && lb == 2) return launch_root<uint16_t, uint16_t>(v, L, slot, p->seed, tree, tv, cur, st);
+  if (ib == 4 && lb == 1) return launch_root<uint32_t, uint8_t>(v, L, slot, p->seed, tree, tv, cur, st);
+  return launch_root<uint32_t, uint16_t>(v, L, slot, p->seed, tree, tv, cur, st);
+}
+
+// One step over list[cur][0..n) -> children appended to list[1-cur].
+int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, int cur, uint32_t n,
+         uint64_t total, cudaStream_t st) {
+  const uint32_t ib = p->index_bytes, lb = p->label_bytes, C = p->n_classes;
+  for (uint32_t lo = 0; lo < n; lo += L.chunk) {
+    const uint32_t cn = std::min(L.chunk, n - lo);
+    const ct_node* nodes = L.list[cur] + lo;
+    const uint32_t* tot = L.tot[cur] + (size_t)lo * C;
+    const LevelBounds b{cn, total};
+    CT_TRY(launch_reset_step(L.s.ctr, cn, st));
+    CT_TRY(launch_split(v, ib, lb, nodes, tot, L.s, b, L.scan_piece, st));
+    CT_TRY(launch_partition(v, ib, lb, nodes, L.s, b, tv, st));
+    CT_TRY(launch_children(v, ib, lb, nodes, tot, L.s, b, tv, L.list[1 - cur], L.tot[1 - cur], L.cap_list,
+                           0, nullptr, 0, st));
+  }
+  return CT_OK;
+}
+
+int level_loop(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, int cur,
+               uint32_t n, uint64_t total, cudaStream_t st) {
+  Counters h;
+  while (n > 0) {
+    k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+    CT_CUDA_TRY(cudaGetLastError());
+    CT_TRY(step(p, v, L, tv, cur, n, total, st));
+    CT_TRY(read_counters(L, &h, st));
+    n = h.n_next;
+    total = h.next_total;
+    cur = 1 - cur;
+  }
+  return CT_OK;
+}
+
+TreeView tree_view(const ct_tree_buffers* t, uint32_t slot_base) {
+  TreeView tv;
+  tv.left = t->left;
+  tv.right = t->right;
+  tv.feature = t->feature;
+  tv.threshold = t->threshold;
+  tv.value = t->value;
+  tv.n_nodes = t->n_nodes;
+  tv.capacity = t->capacity;
+  tv.slot_base = slot_base;
+  tv.enabled = 1;
+  return tv;
+}
+
+uint32_t default_bfs_threshold(const ct_problem* p) {
+  // reference random_forest.py:278-289 ("Titan" coefficients)
+  double t = 4746.0 + 4.0 * p->n_classes + 0.0651 * p->n_rows - 75.0 * p->max_features;
+  long v = (long)t;
+  v = std::min<long>(v, 50000);
+  v = std::max<long>(v, 2000);
+  return (uint32_t)v;
+}
+
+int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
+                const FitLayout& L, const ct_tree_buffers* trees, cudaStream_t st) {
+  View v = make_view(p, l);
+  TreeView tv = tree_view(trees, 0);
+  CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
+  CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
+  for (uint32_t s = 0; s < n_trees; ++s)
+    CT_TRY(bootstrap_compact(p, l, s, first_tree + s, L.n_in, L.boot_ws, L.boot_bytes, st));
+  CT_TRY(check_boot_error(L, st));
+  k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+  for (uint32_t s = 0; s < n_trees; ++s) CT_TRY(root(p, v, L, s, first_tree + s, tv, 0, st));
+  Counters h;
+  CT_TRY(read_counters(L, &h, st));
+  return level_loop(p, v, L, tv, 0, h.n_next, h.next_total, st);
+}
+
+int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
+              const ct_fit_options* o, const FitLayout& L, const ct_tree_buffers* trees,
+              cudaStream_t st) {
+  View v = make_view(p, l);
+  const uint32_t C = p->n_classes;
+  const uint32_t thr = o->bfs_threshold ? o->bfs_threshold : default_bfs_threshold(p);
+  struct Pending {
+    ct_node nd;
+    std::vector<uint32_t> tot;
+  };
+  CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
+  for (uint32_t t = 0; t < n_trees; ++t) {
+    TreeView tv = tree_view(trees, t);
+    CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
+    CT_TRY(bootstrap_compact(p, l, 0, first_tree + t, L.n_in, L.boot_ws, L.boot_bytes, st));
+    CT_TRY(check_boot_error(L, st));
+    k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+    CT_TRY(root(p, v, L, 0, first_tree + t, tv, 0, st));
+    Counters h;
+    CT_TRY(read_counters(L, &h, st));
+    if (h.n_next == 0) continue;
+    std::vector<Pending> stack, bfs;
+    Pending r;
+    r.tot.resize(C);
+    CT_CUDA_TRY(cudaMemcpyAsync(&r.nd, L.list[0], sizeof(ct_node), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaMemcpyAsync(r.tot.data(), L.tot[0], C * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    stack.push_back(std::move(r));
+    while (!stack.empty()) {
+      Pending cur = std::move(stack.back());
+      stack.pop_back();
+      if (cur.nd.n <= thr) {
+        bfs.push_back(std::move(cur));
+        continue;
+      }
+      CT_CUDA_TRY(cudaMemcpyAsync(L.list[0], &cur.nd, sizeof(ct_node), cudaMemcpyHostToDevice, st));
+      CT_CUDA_TRY(cudaMemcpyAsync(L.tot[0], cur.tot.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+      k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+      CT_TRY(step(p, v, L, tv, 0, 1, cur.nd.n, st));
+      CT_TRY(read_counters(L, &h, st));
+      std::vector<ct_node> kids(h.n_next);
+      std::vector<uint32_t> ktot((size_t)h.n_next * C);
+      if (h.n_next) {
+        CT_CUDA_TRY(cudaMemcpyAsync(kids.data(), L.list[1], h.n_next * sizeof(ct_node),
+                                    cudaMemcpyDeviceToHost, st));
+        CT_CUDA_TRY(cudaMemcpyAsync(ktot.data(), L.tot[1], ktot.size() * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, st));
+        CT_CUDA_TRY(cudaStreamSynchronize(st));
+      }
+      // depth-first, left subtree first: push the right child below the left
+      std::vector<uint32_t> order(h.n_next);
+      for (uint32_t i = 0; i < h.n_next; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return kids[a].start > kids[b].start; });
+      for (uint32_t i : order) {
+        Pending c;
+        c.nd = kids[i];
+        c.tot.assign(ktot.begin() + (size_t)i * C, ktot.begin() + (size_t)(i + 1) * C);
+        stack.push_back(std::move(c));
+      }
+    }
+    if (!bfs.empty()) {
+      if (bfs.size() > L.cap_list) {
+        set_last_error("BFS queue exceeds list capacity");
+        return CT_ERR_CAPACITY;
+      }
+      std::vector<ct_node> nodes(bfs.size());
+      std::vector<uint32_t> tots(bfs.size() * C);
+      uint64_t total = 0;
+      for (size_t i = 0; i < bfs.size(); ++i) {
+        nodes[i] = bfs[i].nd;
+        std::memcpy(&tots[i * C], bfs[i].tot.data(), C * sizeof(uint32_t));
+        total += bfs[i].nd.n;
+      }
+      CT_CUDA_TRY(cudaMemcpyAsync(L.list[0], nodes.data(), nodes.size() * sizeof(ct_node),
+                                  cudaMemcpyHostToDevice, st));
+      CT_CUDA_TRY(cudaMemcpyAsync(L.tot[0], tots.data(), tots.size() * sizeof(uint32_t),
+                                  cudaMemcpyHostToDevice, st));
+      CT_TRY(level_loop(p, v, L, tv, 0, (uint32_t)nodes.size(), total, st));
+    }
+  }
+  return CT_OK;
+}
+
+}  // namespace
+
+size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o) {
+  FitLayout L;
+  layout(p, n_trees, o, nullptr, 0, &L);
+  return L.bytes;
+}
+
+int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
+        const ct_fit_options* o, const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st) {
+  CT_TRY(check_problem(p));
+  CT_ARG_CHECK(l && l->si0 && l->si1 && l->mark, "lists are NULL");
+  CT_ARG_CHECK(trees && trees->left && trees->right && trees->feature && trees->threshold && trees->value &&
+                   trees->n_nodes,
+               "tree buffers are NULL");
+  CT_ARG_CHECK(o && (o->mode == CT_FIT_PLAIN || o->mode == CT_FIT_BATCHED), "bad fit mode");
+  CT_ARG_CHECK(n_trees >= 1, "n_trees must be >= 1");
+  CT_ARG_CHECK(trees->capacity >= 2u * p->n_rows, "tree capacity must be >= 2 * n_rows");
+  CT_ARG_CHECK(l->stride >= p->n_rows, "list stride must be >= n_rows");
+  const uint32_t need_slots = (o->mode == CT_FIT_PLAIN) ? 1u : n_trees;
+  CT_ARG_CHECK(l->n_slots >= need_slots, "lists hold too few tree slots");
+  FitLayout L;
+  if (!layout(p, n_trees, o, reinterpret_cast<char*>(ws), wsb, &L)) {
+    set_last_error("fit workspace too small");
+    return CT_ERR_OOM;
+  }
+  if (o->mode == CT_FIT_PLAIN) return fit_plain(p, l, first_tree, n_trees, o, L, trees, st);
+  return fit_batched(p, l, first_tree, n_trees, L, trees, st);
+}
+
+// ---------------------------------------------------------------------------
+int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
+                 const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
+                 uint32_t* ov) {
+  CT_ARG_CHECK(n >= 1, "tree has no nodes");
+  std::vector<uint32_t> order;
+  std::vector<uint32_t> newid(n, NONE);
+  order.reserve(n);
+  order.push_back(0);
+  newid[0] = 0;
+  for (size_t h = 0; h < order.size(); ++h) {
+    const uint32_t r = order[h];
+    if (left[r] != 0 && right[r] != 0) {
+      if (left[r] >= n || right[r] >= n || newid[left[r]] != NONE || newid[right[r]] != NONE) {
+        set_last_error("raw tree is not a binary tree rooted at node 0");
+        return CT_ERR_INTERNAL;
+      }
+      newid[left[r]] = (uint32_t)order.size();
+      order.push_back(left[r]);
+      newid[right[r]] = (uint32_t)order.size();
+      order.push_back(right[r]);
+    }
+  }
+  if (order.size() != n) {
+    set_last_error("raw tree has unreachable nodes");
+    return CT_ERR_INTERNAL;
+  }
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t r = order[i];
+    const bool inner = left[r] != 0 && right[r] != 0;
+    ol[i] = inner ? newid[left[r]] : 0;
+    orr[i] = inner ? newid[right[r]] : 0;
+    of[i] = (uint16_t)feature[r];
+    ot[i] = threshold[r];
+    ov[i] = value[r];
+  }
+  return CT_OK;
+}
+
+}  // namespace ct

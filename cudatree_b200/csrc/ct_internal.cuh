@@ -1,0 +1,199 @@
+// Internal work-list records and launch helpers shared by the .cu files.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include <cuda/atomic>
+
+#include "ct_common.cuh"
+
+namespace ct {
+
+// -------------------------------------------------------------- errors ---
+void set_last_error(const std::string& msg);
+#define CT_CUDA_TRY(expr)                                                              \
+  do {                                                                                 \
+    cudaError_t _e = (expr);                                                           \
+    if (_e != cudaSuccess) {                                                           \
+      ::ct::set_last_error(std::string(#expr) + ": " + cudaGetErrorString(_e));        \
+      return CT_ERR_CUDA;                                                              \
+    }                                                                                  \
+  } while (0)
+#define CT_TRY(expr)                \
+  do {                              \
+    int _s = (expr);                \
+    if (_s != CT_OK) return _s;     \
+  } while (0)
+#define CT_ARG_CHECK(cond, msg)                 \
+  do {                                          \
+    if (!(cond)) {                              \
+      ::ct::set_last_error(msg);                \
+      return CT_ERR_ARG;                        \
+    }                                           \
+  } while (0)
+
+// Device-side error bits (Counters::error).
+enum : uint32_t { DEV_ERR_TIMEOUT = 1u, DEV_ERR_CAPACITY = 2u, DEV_ERR_INTERNAL = 4u };
+constexpr uint32_t NONE = 0xffffffffu;
+
+// -------------------------------------------------------------- records ---
+struct ScanPiece {        // one split-scan work item: part j of segment (node, slot)
+  uint32_t node;
+  uint32_t slot;
+  uint32_t j;
+  uint32_t npieces;       // pieces of this segment
+  uint32_t carry;         // carry-table row of this piece (npieces > 1)
+  uint32_t pad[3];
+};
+struct PieceBest {
+  double score;
+  uint32_t pos;
+  float il;
+  float ir;
+  uint32_t pad;
+};
+struct SplitRec {         // a node that splits this step
+  uint32_t node;
+  uint32_t feature;
+  uint32_t pos;
+  uint32_t children;      // raw id of the left child (fit mode)
+};
+struct PartPiece {
+  uint32_t split;
+  uint32_t j;
+  uint32_t npieces;
+  uint32_t status;        // status column of this piece (npieces > 1)
+};
+struct Counters {
+  uint32_t n_nodes;       // nodes in the current chunk
+  uint32_t n_scan_pieces;
+  uint32_t n_carry;
+  uint32_t n_splits;
+  uint32_t n_part_pieces;
+  uint32_t n_status;
+  uint32_t ticket;
+  uint32_t error;
+  uint32_t n_next;        // nodes appended to the next list
+  uint32_t n_small;       // nodes appended to the subtree list
+  uint32_t pad[2];
+  unsigned long long next_total;
+  unsigned long long small_total;
+};
+
+// View of the problem + lists passed by value to kernels.
+struct View {
+  const float* x_fm;
+  const void* labels;
+  void* si0;
+  void* si1;
+  uint8_t* mark;
+  uint32_t stride;
+  uint32_t n_rows;
+  uint32_t n_features;
+  uint32_t n_classes;
+  uint32_t max_features;
+  uint32_t mss;
+  int feistel_h;
+};
+
+template <typename IdxT>
+__device__ __forceinline__ IdxT* list_ptr(const View& v, uint32_t buf, uint32_t slot, uint32_t f) {
+  IdxT* base = reinterpret_cast<IdxT*>(buf ? v.si1 : v.si0);
+  return base + ((size_t)slot * v.n_features + f) * v.stride;
+}
+template <typename LabT>
+__device__ __forceinline__ uint32_t label_of(const View& v, uint32_t row) {
+  return (uint32_t)reinterpret_cast<const LabT*>(v.labels)[row];
+}
+
+// Raw tree arrays (fit mode).
+struct TreeView {
+  uint32_t* left;
+  uint32_t* right;
+  uint32_t* feature;
+  float* threshold;
+  uint32_t* value;
+  uint32_t* n_nodes;
+  uint32_t capacity;
+  uint32_t slot_base;     // tree slot = list slot + slot_base
+  uint32_t enabled;
+};
+
+// Scratch of one level step, carved from the caller's workspace.
+struct LevelScratch {
+  uint32_t cap_nodes;
+  uint32_t cap_scan;
+  uint32_t cap_carry;
+  uint32_t cap_part;
+  uint32_t cap_status;
+  uint32_t* sel;          // [cap_nodes][max_features]
+  uint32_t* nsel;         // [cap_nodes]
+  uint32_t* piece_base;   // [cap_nodes]
+  uint32_t* piece_cnt;    // [cap_nodes]
+  ScanPiece* pieces;      // [cap_scan]
+  uint32_t* carry;        // [cap_carry][n_classes]
+  PieceBest* best;        // [cap_scan]
+  ct_split_result* result;// [cap_nodes]
+  SplitRec* splits;       // [cap_nodes]
+  uint32_t* split_left;   // [cap_nodes][n_classes]
+  PartPiece* part;        // [cap_part]
+  uint64_t* status;       // [n_features][cap_status]
+  Counters* ctr;
+};
+
+// Bump allocator over a caller workspace (256-byte aligned carving).
+struct Arena {
+  char* base;
+  size_t size;
+  size_t used;
+  template <typename T>
+  T* take(size_t count) {
+    size_t off = (used + 255) & ~size_t(255);
+    size_t bytes = count * sizeof(T);
+    used = off + bytes;
+    if (base == nullptr || used > size) return nullptr;
+    return reinterpret_cast<T*>(base + off);
+  }
+  bool ok() const { return used <= size; }
+};
+
+// Tile shapes.
+constexpr uint32_t DEFAULT_SCAN_PIECE = 2048;   // elements per split-scan work item
+constexpr uint32_t PART_ROUNDS = 16;            // rounds of 32 held in registers
+constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
+constexpr int WARPS_PER_BLOCK = 4;
+constexpr int THREADS_PER_BLOCK = 32 * WARPS_PER_BLOCK;
+
+// Bounds of one step: nodes in the chunk and samples they hold.
+struct LevelBounds {
+  uint64_t nodes;
+  uint64_t samples;
+};
+struct LevelCaps {
+  uint32_t nodes, scan, carry, part, status;
+};
+LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b);
+bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s);
+size_t level_scratch_bytes(const View& v, const LevelCaps& c);
+
+// Level-step launches (ct_level.cu).  Node count of the chunk is in
+// s.ctr->n_nodes (device) and bounded by b.nodes.
+int launch_split(const View& v, uint32_t index_bytes, uint32_t label_bytes, const ct_node* nodes,
+                 const uint32_t* tot, const LevelScratch& s, LevelBounds b, uint32_t scan_piece,
+                 cudaStream_t st);
+int launch_partition(const View& v, uint32_t index_bytes, uint32_t label_bytes,
+                     const ct_node* nodes, const LevelScratch& s, LevelBounds b,
+                     const TreeView& tv, cudaStream_t st);
+int launch_children(const View& v, uint32_t index_bytes, uint32_t label_bytes, const ct_node* nodes,
+                    const uint32_t* tot, const LevelScratch& s, LevelBounds b, const TreeView& tv,
+                    ct_node* next, uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut,
+                    ct_node* small, uint32_t cap_small, cudaStream_t st);
+// Counter resets between steps (device-side, stream ordered).
+int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
+
+View make_view(const ct_problem* p, const ct_lists* l);
+int check_problem(const ct_problem* p);
+
+}  // namespace ct

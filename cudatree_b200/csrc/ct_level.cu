@@ -1,0 +1,775 @@
+// Level-step kernels of the split search and the stable partition.
+//
+//   k_select       feature subset of each node (reference DFS: first m of a
+//                  shuffled permutation, random_tree.py:624; BFS: non-constant
+//                  features only, bfs_module.cu:130-140)
+//   k_scan_hist    class histograms of all but the last piece of long segments
+//   k_scan_carry   exclusive per-class prefix over those pieces
+//                  (reference scan_gini_large + scan_reduce, dfs_module.cu:24-106)
+//   k_split_scan   Gini scan of one piece: per-element class rank via
+//                  __match_any_sync, int64 warp scans of the sum of squared
+//                  counts, fp64 impurity (reference compute_2d, dfs_module.cu:310-443)
+//   k_split_reduce min-impurity reduction + threshold
+//                  (reference reduce_2d / find_min_imp / get_thresholds)
+//   k_plan         node record, child ids, partition work list
+//   k_fill_mark    mark table + left class totals (reference fill_table)
+//   k_partition    stable partition of every feature's node range with warp
+//                  ballot/popc ranks and a decoupled look-back across pieces
+//                  (reference scan_reshuffle, dfs_module.cu:224-307)
+//   k_children     child records for the next step
+#include <cfloat>
+
+#include "ct_internal.cuh"
+
+namespace ct {
+
+namespace {
+
+constexpr uint64_t ST_AGG = 1ull << 62;
+constexpr uint64_t ST_INC = 2ull << 62;
+constexpr uint64_t ST_FLAG = 3ull << 62;
+constexpr uint64_t ST_VAL = (1ull << 62) - 1;
+constexpr uint32_t SPIN_LIMIT = 1u << 20;
+
+__device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
+
+__device__ __forceinline__ uint32_t global_warp() {
+  return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+
+__device__ __forceinline__ void publish(uint64_t* p, uint64_t v) {
+  cuda::atomic_ref<uint64_t, cuda::thread_scope_device> a(*p);
+  a.store(v, cuda::memory_order_release);
+}
+__device__ __forceinline__ uint64_t poll(uint64_t* p) {
+  cuda::atomic_ref<uint64_t, cuda::thread_scope_device> a(*p);
+  return a.load(cuda::memory_order_acquire);
+}
+__device__ __forceinline__ uint32_t read_error(const Counters* c) {
+  return *reinterpret_cast<const volatile uint32_t*>(&c->error);
+}
+// Work-list count clamped to its capacity; 0 once an earlier kernel of the
+// step flagged an error, so no kernel reads a record that was not written.
+__device__ __forceinline__ uint32_t live_count(const LevelScratch& s, uint32_t count, uint32_t cap) {
+  return read_error(s.ctr) ? 0u : min(count, cap);
+}
+
+// (score, pos) lexicographic minimum across the warp.
+__device__ __forceinline__ void warp_argmin2(double& score, uint32_t& pos, float& p, float& q) {
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    double os = __shfl_xor_sync(FULL, score, s);
+    uint32_t op = __shfl_xor_sync(FULL, pos, s);
+    float a = __shfl_xor_sync(FULL, p, s);
+    float b = __shfl_xor_sync(FULL, q, s);
+    if (os < score || (os == score && op < pos)) {
+      score = os;
+      pos = op;
+      p = a;
+      q = b;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t scan_piece) {
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= min(s.ctr->n_nodes, s.cap_nodes)) return;
+  const ct_node nd = nodes[w];
+  const uint32_t m = v.max_features;
+  uint32_t taken = 0;
+  if (nd.n >= 2) {
+    for (uint32_t i0 = 0; i0 < v.n_features && taken < m; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      bool usable = false;
+      uint32_t f = 0;
+      if (i < v.n_features) {
+        f = feature_perm(i, v.n_features, nd.key, v.feistel_h);
+        const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+        const float* xf = v.x_fm + (size_t)f * v.n_rows;
+        usable = xf[lst[0]] != xf[lst[nd.n - 1]];
+      }
+      const unsigned mask = __ballot_sync(FULL, usable);
+      const uint32_t rank = __popc(mask & lanemask_lt());
+      if (usable && taken + rank < m) s.sel[(size_t)w * m + taken + rank] = f;
+      taken += min((uint32_t)__popc(mask), m - taken);
+    }
+  }
+  const uint32_t pps = ceil_div(nd.n, scan_piece);
+  uint32_t npieces = taken * pps;
+  uint32_t base = 0, cbase = 0;
+  if (lane == 0) {
+    if (npieces) base = atomicAdd(&s.ctr->n_scan_pieces, npieces);
+    if (npieces && pps > 1) cbase = atomicAdd(&s.ctr->n_carry, npieces);
+    const bool overflow = (base + (uint64_t)npieces > s.cap_scan) ||
+                          (pps > 1 && cbase + (uint64_t)npieces > s.cap_carry);
+    if (overflow) {
+      atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+      npieces = 0;
+    }
+    s.nsel[w] = taken;
+    s.piece_base[w] = base;
+    s.piece_cnt[w] = npieces;
+  }
+  npieces = __shfl_sync(FULL, npieces, 0);
+  base = __shfl_sync(FULL, base, 0);
+  cbase = __shfl_sync(FULL, cbase, 0);
+  for (uint32_t q = lane; q < npieces; q += 32) {
+    ScanPiece pc;
+    pc.node = w;
+    pc.slot = q / pps;
+    pc.j = q - pc.slot * pps;
+    pc.npieces = pps;
+    pc.carry = cbase + q;
+    pc.pad[0] = pc.pad[1] = pc.pad[2] = 0;
+    s.pieces[base + q] = pc;
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t C = v.n_classes;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
+  const uint32_t pi = global_warp();
+  const uint32_t lane = lane_id();
+  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
+  const ScanPiece pc = s.pieces[pi];
+  if (pc.npieces <= 1 || pc.j + 1 == pc.npieces) return;
+  const ct_node nd = nodes[pc.node];
+  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
+  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+  for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
+  __syncwarp();
+  const uint32_t lo = pc.j * scan_piece;
+  const uint32_t hi = min(lo + scan_piece, nd.n);
+  for (uint32_t base = lo; base < hi; base += 32) {
+    const uint32_t p = base + lane;
+    const bool valid = p < hi;
+    const uint32_t c = valid ? label_of<LabT>(v, lst[p]) : NONE;
+    const unsigned grp = __match_any_sync(FULL, c);
+    if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
+    __syncwarp();
+  }
+  uint32_t* out = s.carry + (size_t)pc.carry * C;
+  for (uint32_t c = lane; c < C; c += 32) out[c] = cnt[c];
+}
+
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_scan_carry(LevelScratch s, uint32_t C) {
+  const uint32_t pi = global_warp();
+  const uint32_t lane = lane_id();
+  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
+  const ScanPiece pc = s.pieces[pi];
+  if (pc.npieces <= 1 || pc.j != 0) return;
+  for (uint32_t c = lane; c < C; c += 32) {
+    uint32_t run = 0;
+    for (uint32_t j = 0; j < pc.npieces; ++j) {
+      uint32_t* h = s.carry + (size_t)(pc.carry + j) * C + c;
+      const uint32_t t = (j + 1 < pc.npieces) ? *h : 0u;
+      *h = run;
+      run += t;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
+             LevelScratch s, uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t C = v.n_classes;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * C;
+  uint32_t* T = cnt + C;
+  const uint32_t pi = global_warp();
+  const uint32_t lane = lane_id();
+  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
+  const ScanPiece pc = s.pieces[pi];
+  const ct_node nd = nodes[pc.node];
+  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
+  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+  const float* xf = v.x_fm + (size_t)f * v.n_rows;
+  const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
+  int64_t sl = 0, sr = 0;
+  for (uint32_t c = lane; c < C; c += 32) {
+    const uint32_t k = carry ? carry[c] : 0u;
+    const uint32_t t = tot[(size_t)pc.node * C + c];
+    cnt[c] = k;
+    T[c] = t;
+    const int64_t r = (int64_t)t - (int64_t)k;
+    sl += (int64_t)k * k;
+    sr += r * r;
+  }
+  sl = warp_sum_i64(sl);
+  sr = warp_sum_i64(sr);
+  __syncwarp();
+  const uint32_t n = nd.n;
+  const double nn = (double)n;
+  const uint32_t lo = pc.j * scan_piece;
+  const uint32_t hi = min(lo + scan_piece, n);
+  double best = dinf();
+  uint32_t bpos = NONE;
+  float bil = 0.f, bir = 0.f;
+  for (uint32_t base = lo; base < hi; base += 32) {
+    const uint32_t p = base + lane;
+    const bool valid = p < hi;
+    uint32_t c = NONE;
+    float x = 0.f;
+    if (valid) {
+      const uint32_t row = lst[p];
+      c = label_of<LabT>(v, row);
+      x = xf[row];
+    }
+    float xn = __shfl_down_sync(FULL, x, 1);
+    if (valid && (lane == 31 || p + 1 == hi) && p + 1 < n) xn = xf[lst[p + 1]];
+    const unsigned grp = __match_any_sync(FULL, c);
+    uint32_t k = 0;
+    int64_t tc = 0;
+    if (valid) {
+      k = cnt[c] + __popc(grp & lanemask_lt());
+      tc = T[c];
+    }
+    __syncwarp();
+    if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
+    __syncwarp();
+    const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
+    const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
+    const int64_t il = warp_incl_scan_i64(dl);
+    const int64_t ir = warp_incl_scan_i64(dr);
+    const int64_t SL = sl + il;
+    const int64_t SR = sr + ir;
+    sl += __shfl_sync(FULL, il, 31);
+    sr += __shfl_sync(FULL, ir, 31);
+    if (valid && p + 1 < n && is_candidate(x, xn)) {
+      const double nl = (double)(p + 1);
+      const double nr = __dsub_rn(nn, nl);
+      const double gl = gini_part(SL, nl, nn);
+      const double gr = gini_part(SR, nr, nn);
+      const double sc = __dadd_rn(gl, gr);
+      if (sc < best) {
+        best = sc;
+        bpos = p;
+        bil = __double2float_rn(gl);
+        bir = __double2float_rn(gr);
+      }
+    }
+  }
+  warp_argmin2(best, bpos, bil, bir);
+  if (lane == 0) {
+    PieceBest pb;
+    pb.score = best;
+    pb.pos = bpos;
+    pb.il = bil;
+    pb.ir = bir;
+    pb.pad = 0;
+    s.best[pi] = pb;
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_split_reduce(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_nodes, s.cap_nodes)) return;
+  const uint32_t base = s.piece_base[w];
+  const uint32_t cnt = s.piece_cnt[w];
+  const uint32_t m = v.max_features;
+  double best = dinf();
+  uint32_t bf = NONE, bp = NONE;
+  float il = 0.f, ir = 0.f;
+  for (uint32_t q = lane; q < cnt; q += 32) {
+    const PieceBest pb = s.best[base + q];
+    const uint32_t f = s.sel[(size_t)w * m + s.pieces[base + q].slot];
+    if (pb.score < best || (pb.score == best && (f < bf || (f == bf && pb.pos < bp)))) {
+      best = pb.score;
+      bf = f;
+      bp = pb.pos;
+      il = pb.il;
+      ir = pb.ir;
+    }
+  }
+  warp_argmin3(best, bf, bp, il, ir);
+  if (lane == 0) {
+    ct_split_result r;
+    r.n_selected = s.nsel[w];
+    if (best < dinf()) {
+      const ct_node nd = nodes[w];
+      const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, bf) + nd.start;
+      const float* xf = v.x_fm + (size_t)bf * v.n_rows;
+      r.score = best;
+      r.feature = bf;
+      r.pos = bp;
+      r.imp_left = il;
+      r.imp_right = ir;
+      r.threshold = midpoint(xf[lst[bp]], xf[lst[bp + 1]]);
+    } else {
+      r.score = dinf();
+      r.feature = NONE;
+      r.pos = 0;
+      r.imp_left = 0.f;
+      r.imp_right = 0.f;
+      r.threshold = 0.f;
+    }
+    s.result[w] = r;
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_nodes, s.cap_nodes)) return;
+  const ct_node nd = nodes[w];
+  const ct_split_result r = s.result[w];
+  uint32_t split = r.feature != NONE;
+  uint32_t children = 0;
+  if (lane == 0 && tv.enabled) {
+    const size_t off = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+    if (split) {
+      const uint32_t c = atomicAdd(&tv.n_nodes[nd.slot + tv.slot_base], 2u);
+      if (c + 2ull > tv.capacity) {
+        atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+        split = 0;
+      } else {
+        children = c;
+        tv.left[off + nd.raw_id] = c;
+        tv.right[off + nd.raw_id] = c + 1;
+        tv.feature[off + nd.raw_id] = r.feature;
+        tv.threshold[off + nd.raw_id] = r.threshold;
+        tv.value[off + nd.raw_id] = 0;
+      }
+    }
+    if (!split) {
+      const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+      tv.left[off + nd.raw_id] = 0;
+      tv.right[off + nd.raw_id] = 0;
+      tv.feature[off + nd.raw_id] = 0;
+      tv.threshold[off + nd.raw_id] = 0.f;
+      tv.value[off + nd.raw_id] = label_of<LabT>(v, l0[0]);
+    }
+  }
+  split = __shfl_sync(FULL, split, 0);
+  children = __shfl_sync(FULL, children, 0);
+  if (!split) return;
+  const uint32_t npp = ceil_div(nd.n, PART_PIECE);
+  uint32_t sidx = 0, pbase = 0, sbase = 0, ok = 1;
+  if (lane == 0) {
+    sidx = atomicAdd(&s.ctr->n_splits, 1u);
+    pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
+    if (npp > 1) sbase = atomicAdd(&s.ctr->n_status, npp);
+    if (sidx >= s.cap_nodes || pbase + (uint64_t)npp > s.cap_part ||
+        (npp > 1 && sbase + (uint64_t)npp > s.cap_status)) {
+      atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+      ok = 0;
+    } else {
+      SplitRec sr;
+      sr.node = w;
+      sr.feature = r.feature;
+      sr.pos = r.pos;
+      sr.children = children;
+      s.splits[sidx] = sr;
+    }
+  }
+  ok = __shfl_sync(FULL, ok, 0);
+  if (!ok) return;
+  sidx = __shfl_sync(FULL, sidx, 0);
+  pbase = __shfl_sync(FULL, pbase, 0);
+  sbase = __shfl_sync(FULL, sbase, 0);
+  for (uint32_t c = lane; c < v.n_classes; c += 32) s.split_left[(size_t)sidx * v.n_classes + c] = 0;
+  for (uint32_t j = lane; j < npp; j += 32) {
+    PartPiece pp;
+    pp.split = sidx;
+    pp.j = j;
+    pp.npieces = npp;
+    pp.status = sbase + j;
+    s.part[pbase + j] = pp;
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t C = v.n_classes;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
+  const uint32_t pi = global_warp();
+  const uint32_t lane = lane_id();
+  if (pi >= live_count(s, s.ctr->n_part_pieces, s.cap_part)) return;
+  const PartPiece pp = s.part[pi];
+  const SplitRec sr = s.splits[pp.split];
+  const ct_node nd = nodes[sr.node];
+  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, sr.feature) + nd.start;
+  uint8_t* mk = v.mark + (size_t)nd.slot * v.n_rows;
+  for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
+  __syncwarp();
+  const uint32_t lo = pp.j * PART_PIECE;
+  const uint32_t hi = min(lo + PART_PIECE, nd.n);
+  for (uint32_t base = lo; base < hi; base += 32) {
+    const uint32_t p = base + lane;
+    uint32_t c = NONE;
+    if (p < hi) {
+      const uint32_t row = lst[p];
+      const bool left = p <= sr.pos;
+      mk[row] = left ? 1 : 0;
+      if (left) c = label_of<LabT>(v, row);
+    }
+    const unsigned grp = __match_any_sync(FULL, c);
+    if (c != NONE && (grp >> lane) == 1u) cnt[c] += __popc(grp);
+    __syncwarp();
+  }
+  uint32_t* out = s.split_left + (size_t)pp.split * C;
+  for (uint32_t c = lane; c < C; c += 32)
+    if (cnt[c]) atomicAdd(&out[c], cnt[c]);
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_partition(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
+  const uint32_t lane = lane_id();
+  uint32_t ticket = 0;
+  if (lane == 0) ticket = atomicAdd(&s.ctr->ticket, 1u);
+  ticket = __shfl_sync(FULL, ticket, 0);
+  const uint32_t npp = live_count(s, s.ctr->n_part_pieces, s.cap_part);
+  if ((uint64_t)ticket >= (uint64_t)npp * v.n_features) return;
+  const uint32_t f = ticket / npp;
+  const uint32_t pi = ticket - f * npp;
+  const PartPiece pp = s.part[pi];
+  const SplitRec sr = s.splits[pp.split];
+  const ct_node nd = nodes[sr.node];
+  const IdxT* in = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+  IdxT* out = list_ptr<IdxT>(v, nd.buf ^ 1u, nd.slot, f) + nd.start;
+  const uint8_t* mk = v.mark + (size_t)nd.slot * v.n_rows;
+  const uint32_t n = nd.n;
+  const uint32_t nl = sr.pos + 1;
+  const uint32_t lo = pp.j * PART_PIECE;
+
+  uint32_t rows[PART_ROUNDS];
+  unsigned lmask[PART_ROUNDS];
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    const uint32_t p = lo + r * 32 + lane;
+    rows[r] = p < n ? (uint32_t)in[p] : 0u;
+  }
+  uint32_t local = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    const uint32_t p = lo + r * 32 + lane;
+    const bool left = p < n && mk[rows[r]] != 0;
+    lmask[r] = __ballot_sync(FULL, left);
+    local += __popc(lmask[r]);
+  }
+
+  uint32_t carry = 0;
+  if (pp.npieces > 1) {
+    uint64_t* col = s.status + (size_t)f * s.cap_status + (pp.status - pp.j);
+    if (lane == 0) {
+      if (pp.j == 0) {
+        publish(col, ST_INC | local);
+      } else {
+        publish(col + pp.j, ST_AGG | local);
+        uint64_t acc = 0;
+        uint32_t k = pp.j - 1;
+        uint32_t spins = 0;
+        while (true) {
+          const uint64_t word = poll(col + k);
+          const uint64_t flag = word & ST_FLAG;
+          if (flag == 0) {
+            if (++spins > SPIN_LIMIT || read_error(s.ctr) != 0) {
+              atomicOr(&s.ctr->error, DEV_ERR_TIMEOUT);
+              acc = 0;
+              break;
+            }
+            __nanosleep(64);
+            continue;
+          }
+          acc += word & ST_VAL;
+          if (flag == ST_INC || k == 0) break;
+          --k;
+        }
+        carry = (uint32_t)acc;
+        publish(col + pp.j, ST_INC | (uint64_t)(carry + local));
+      }
+    }
+    carry = __shfl_sync(FULL, carry, 0);
+  }
+
+  uint32_t run = carry;
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    const uint32_t p = lo + r * 32 + lane;
+    if (p < n) {
+      const bool left = (lmask[r] >> lane) & 1u;
+      const uint32_t rl = run + __popc(lmask[r] & lt);
+      const uint32_t dst = left ? rl : nl + (p - rl);
+      if (dst < n) out[dst] = (IdxT)rows[r];
+    }
+    run += __popc(lmask[r]);
+  }
+}
+
+// ------------------------------------------------------------------------
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
+           LevelScratch s, TreeView tv, ct_node* next, uint32_t* next_tot, uint32_t cap_next,
+           uint32_t small_cut, ct_node* small, uint32_t cap_small) {
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_splits, s.cap_nodes)) return;
+  const SplitRec sr = s.splits[w];
+  const ct_node nd = nodes[sr.node];
+  const ct_split_result r = s.result[sr.node];
+  const uint32_t nl = sr.pos + 1;
+  const uint32_t C = v.n_classes;
+  for (int side = 0; side < 2; ++side) {
+    ct_node ch;
+    ch.slot = nd.slot;
+    ch.n = side ? nd.n - nl : nl;
+    ch.start = side ? nd.start + nl : nd.start;
+    ch.raw_id = sr.children + side;
+    ch.key = child_key(nd.key, side);
+    ch.impurity = side ? r.imp_right : r.imp_left;
+    ch.buf = nd.buf ^ 1u;
+    const bool leaf = ch.impurity == 0.0f || ch.n < v.mss;
+    if (leaf) {
+      if (lane == 0 && tv.enabled) {
+        const size_t off = (size_t)(nd.slot + tv.slot_base) * tv.capacity + ch.raw_id;
+        const IdxT* l0 = list_ptr<IdxT>(v, ch.buf, ch.slot, 0) + ch.start;
+        tv.left[off] = 0;
+        tv.right[off] = 0;
+        tv.feature[off] = 0;
+        tv.threshold[off] = 0.f;
+        tv.value[off] = label_of<LabT>(v, l0[0]);
+      }
+      continue;
+    }
+    if (small_cut != 0 && ch.n <= small_cut) {
+      if (lane == 0) {
+        const uint32_t idx = atomicAdd(&s.ctr->n_small, 1u);
+        if (idx < cap_small) {
+          small[idx] = ch;
+          atomicAdd(&s.ctr->small_total, (unsigned long long)ch.n);
+        } else {
+          atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+        }
+      }
+      continue;
+    }
+    uint32_t idx = 0;
+    if (lane == 0) {
+      idx = atomicAdd(&s.ctr->n_next, 1u);
+      if (idx < cap_next) {
+        next[idx] = ch;
+        atomicAdd(&s.ctr->next_total, (unsigned long long)ch.n);
+      } else {
+        atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+      }
+    }
+    idx = __shfl_sync(FULL, idx, 0);
+    if (idx >= cap_next) continue;
+    for (uint32_t c = lane; c < C; c += 32) {
+      const uint32_t left = s.split_left[(size_t)w * C + c];
+      next_tot[(size_t)idx * C + c] = side ? tot[(size_t)sr.node * C + c] - left : left;
+    }
+  }
+}
+
+__global__ void k_reset_step(Counters* c, uint32_t n_nodes) {
+  c->n_nodes = n_nodes;
+  c->n_scan_pieces = 0;
+  c->n_carry = 0;
+  c->n_splits = 0;
+  c->n_part_pieces = 0;
+  c->n_status = 0;
+  c->ticket = 0;
+}
+
+inline uint32_t blocks_for_warps(uint64_t warps) {
+  uint64_t b = (warps + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  return (uint32_t)(b == 0 ? 1 : b);
+}
+
+inline uint32_t clamp32(uint64_t x) { return x > 0xffffffffull ? 0xffffffffu : (uint32_t)x; }
+
+template <typename IdxT, typename LabT>
+void split_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const LevelScratch& s,
+                const LevelCaps& caps, uint32_t scan_piece, cudaStream_t st) {
+  const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
+  k_select<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, scan_piece);
+  if (caps.carry > 0) {
+    k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
+                                                                                         scan_piece);
+    k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
+  }
+  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 2 * sm1, st>>>(
+      v, nodes, tot, s, scan_piece);
+  k_split_reduce<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s);
+}
+
+template <typename IdxT, typename LabT>
+void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s, const LevelCaps& caps,
+                    const TreeView& tv, cudaStream_t st) {
+  const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
+  k_plan<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, tv);
+  k_fill_mark<IdxT, LabT><<<blocks_for_warps(caps.part), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s);
+  k_partition<IdxT><<<blocks_for_warps((uint64_t)caps.part * v.n_features), THREADS_PER_BLOCK, 0, st>>>(
+      v, nodes, s);
+}
+
+template <typename IdxT, typename LabT>
+void children_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const LevelScratch& s,
+                   const LevelCaps& caps, const TreeView& tv, ct_node* next, uint32_t* next_tot,
+                   uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small,
+                   cudaStream_t st) {
+  k_children<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(
+      v, nodes, tot, s, tv, next, next_tot, cap_next, small_cut, small, cap_small);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b) {
+  LevelCaps c;
+  const uint64_t m = v.max_features;
+  c.nodes = clamp32(b.nodes);
+  c.scan = clamp32(m * (b.samples / scan_piece + b.nodes) + 1);
+  c.carry = clamp32(m * (2 * b.samples / scan_piece) + 1);
+  c.part = clamp32(b.samples / PART_PIECE + b.nodes + 1);
+  c.status = clamp32(2 * b.samples / PART_PIECE + 1);
+  return c;
+}
+
+static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s) {
+  const size_t C = v.n_classes;
+  LevelScratch t;
+  t.cap_nodes = c.nodes;
+  t.cap_scan = c.scan;
+  t.cap_carry = c.carry;
+  t.cap_part = c.part;
+  t.cap_status = c.status;
+  t.ctr = a.take<Counters>(1);
+  t.sel = a.take<uint32_t>((size_t)c.nodes * v.max_features);
+  t.nsel = a.take<uint32_t>(c.nodes);
+  t.piece_base = a.take<uint32_t>(c.nodes);
+  t.piece_cnt = a.take<uint32_t>(c.nodes);
+  t.pieces = a.take<ScanPiece>(c.scan);
+  t.carry = a.take<uint32_t>((size_t)c.carry * C);
+  t.best = a.take<PieceBest>(c.scan);
+  t.result = a.take<ct_split_result>(c.nodes);
+  t.splits = a.take<SplitRec>(c.nodes);
+  t.split_left = a.take<uint32_t>((size_t)c.nodes * C);
+  t.part = a.take<PartPiece>(c.part);
+  t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
+  if (s) *s = t;
+  return a.used;
+}
+
+size_t level_scratch_bytes(const View& v, const LevelCaps& c) {
+  Arena a{nullptr, 0, 0};
+  return carve_or_size(a, v, c, nullptr) + 256;
+}
+
+bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s) {
+  carve_or_size(a, v, c, s);
+  return a.ok();
+}
+
+#define CT_DISPATCH(IB, LB, CALL)                                   \
+  do {                                                              \
+    if ((IB) == 2 && (LB) == 1) { CALL(uint16_t, uint8_t); }        \
+    else if ((IB) == 2 && (LB) == 2) { CALL(uint16_t, uint16_t); }  \
+    else if ((IB) == 4 && (LB) == 1) { CALL(uint32_t, uint8_t); }   \
+    else { CALL(uint32_t, uint16_t); }                              \
+  } while (0)
+
+int launch_split(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes, const uint32_t* tot,
+                 const LevelScratch& s, LevelBounds b, uint32_t scan_piece, cudaStream_t st) {
+  LevelCaps caps = level_caps(v, scan_piece, b);
+  caps.scan = min(caps.scan, s.cap_scan);
+  caps.carry = min(caps.carry, s.cap_carry);
+#define CALL(I, L) split_impl<I, L>(v, nodes, tot, s, caps, scan_piece, st)
+  CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int launch_partition(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes,
+                     const LevelScratch& s, LevelBounds b, const TreeView& tv, cudaStream_t st) {
+  LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
+  caps.part = min(caps.part, s.cap_part);
+  caps.status = min(caps.status, s.cap_status);
+  CT_CUDA_TRY(cudaMemsetAsync(s.status, 0, (size_t)s.cap_status * v.n_features * sizeof(uint64_t), st));
+#define CALL(I, L) partition_impl<I, L>(v, nodes, s, caps, tv, st)
+  CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int launch_children(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes, const uint32_t* tot,
+                    const LevelScratch& s, LevelBounds b, const TreeView& tv, ct_node* next,
+                    uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut, ct_node* small,
+                    uint32_t cap_small, cudaStream_t st) {
+  LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
+#define CALL(I, L) \
+  children_impl<I, L>(v, nodes, tot, s, caps, tv, next, next_tot, cap_next, small_cut, small, cap_small, st)
+  CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st) {
+  k_reset_step<<<1, 1, 0, st>>>(ctr, n_nodes);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+View make_view(const ct_problem* p, const ct_lists* l) {
+  View v;
+  v.x_fm = p->x_fm;
+  v.labels = p->labels;
+  v.si0 = l ? l->si0 : nullptr;
+  v.si1 = l ? l->si1 : nullptr;
+  v.mark = l ? l->mark : nullptr;
+  v.stride = l ? l->stride : 0;
+  v.n_rows = p->n_rows;
+  v.n_features = p->n_features;
+  v.n_classes = p->n_classes;
+  v.max_features = p->max_features;
+  v.mss = p->min_samples_split;
+  v.feistel_h = feistel_half_bits(p->n_features);
+  return v;
+}
+
+int check_problem(const ct_problem* p) {
+  CT_ARG_CHECK(p != nullptr, "problem is NULL");
+  CT_ARG_CHECK(p->x_fm && p->labels, "problem samples/labels are NULL");
+  CT_ARG_CHECK(p->n_rows >= 1, "n_rows must be >= 1");
+  CT_ARG_CHECK(p->n_features >= 1 && p->n_features <= CT_MAX_FEATURES, "n_features out of range");
+  CT_ARG_CHECK(p->n_classes >= 1 && p->n_classes <= CT_MAX_CLASSES, "n_classes out of range");
+  CT_ARG_CHECK(p->index_bytes == 2 || p->index_bytes == 4, "index_bytes must be 2 or 4");
+  CT_ARG_CHECK(p->index_bytes == 4 || p->n_rows <= 0xFFFFu, "uint16 indices need n_rows <= 65535");
+  CT_ARG_CHECK(p->label_bytes == 1 || p->label_bytes == 2, "label_bytes must be 1 or 2");
+  CT_ARG_CHECK(p->label_bytes == 2 || p->n_classes <= 0xFFu, "uint8 labels need n_classes <= 255");
+  CT_ARG_CHECK(p->max_features >= 1 && p->max_features <= p->n_features,
+               "max_features must be in [1, n_features]");
+  CT_ARG_CHECK(p->min_samples_split >= 1, "min_samples_split must be >= 1");
+  return CT_OK;
+}
+
+}  // namespace ct

@@ -1,0 +1,197 @@
+// Stable per-feature presort on the device (replaces the host
+// np.argsort of random_forest.py:247).
+//
+// Keys are the order-preserving uint32 image of each float (with -0.0 folded
+// onto +0.0); values are row ids.  Four 8-bit LSD radix passes, each
+//   k_digit_hist  per (tile, feature) digit histogram,
+//   k_digit_scan  per feature exclusive scan over (digit, tile),
+//   k_digit_move  stable scatter: warp-level ranks from __match_any_sync,
+//                 then per-digit prefix over the tile's warps.
+// A stable sort of keys that start in row order gives ties in row order,
+// which is the tie rule the split search and the leaf labels rely on.
+#include "ct_internal.cuh"
+
+namespace ct {
+
+namespace {
+
+constexpr int RS_WARPS = 8;
+constexpr int RS_ROUNDS = 16;
+constexpr uint32_t RS_TILE = RS_WARPS * RS_ROUNDS * 32;  // 4096
+constexpr int RS_THREADS = RS_WARPS * 32;
+
+struct RadixArgs {
+  const float* x;          // pass 0 source
+  const uint32_t* kin;
+  const uint32_t* vin;
+  uint32_t* kout;
+  uint32_t* vout;
+  void* final_out;         // last pass: row ids, index_bytes wide
+  uint32_t* hist;          // [F][256][tiles]
+  uint32_t n;
+  uint32_t tiles;
+  uint32_t shift;
+  uint32_t first;
+  uint32_t last;
+  uint32_t index_bytes;
+};
+
+__device__ __forceinline__ uint32_t load_key(const RadixArgs& a, uint32_t f, uint32_t i) {
+  return a.first ? f32_order(a.x[(size_t)f * a.n + i]) : a.kin[(size_t)f * a.n + i];
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_digit_hist(RadixArgs a) {
+  __shared__ uint32_t h[256];
+  const uint32_t tile = blockIdx.x, f = blockIdx.y;
+  for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
+  __syncthreads();
+  const uint32_t lo = tile * RS_TILE, hi = min(lo + RS_TILE, a.n);
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t d = (load_key(a, f, i) >> a.shift) & 255u;
+    atomicAdd(&h[d], 1u);
+  }
+  __syncthreads();
+  for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x)
+    a.hist[((size_t)f * 256 + d) * a.tiles + tile] = h[d];
+}
+
+__global__ void __launch_bounds__(1024) k_digit_scan(uint32_t* hist, uint32_t tiles) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t f = blockIdx.x;
+  uint32_t* row = hist + (size_t)f * 256 * tiles;
+  const uint32_t L = 256 * tiles;
+  const uint32_t per = (L + blockDim.x - 1) / blockDim.x;
+  const uint32_t lo = min(threadIdx.x * per, L), hi = min(lo + per, L);
+  uint32_t sum = 0;
+  for (uint32_t i = lo; i < hi; ++i) sum += row[i];
+  // block exclusive scan of per-thread sums
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = sum;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL, inc, s);
+    if (lane >= (uint32_t)s) inc += o;
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    uint32_t t = lane < (blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+    for (int s = 1; s < 32; s <<= 1) {
+      const uint32_t o = __shfl_up_sync(FULL, t, s);
+      if (lane >= (uint32_t)s) t += o;
+    }
+    warp_tot[lane] = t;
+  }
+  __syncthreads();
+  uint32_t run = inc - sum + (warp ? warp_tot[warp - 1] : 0);
+  for (uint32_t i = lo; i < hi; ++i) {
+    const uint32_t v = row[i];
+    row[i] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
+  __shared__ uint32_t wcnt[RS_WARPS][256];
+  const uint32_t tile = blockIdx.x, f = blockIdx.y;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
+  __syncwarp();
+  const uint32_t lo = tile * RS_TILE + warp * RS_ROUNDS * 32;
+  uint32_t key[RS_ROUNDS], val[RS_ROUNDS], rank[RS_ROUNDS];
+  const unsigned lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < RS_ROUNDS; ++r) {
+    const uint32_t i = lo + r * 32 + lane;
+    const bool ok = i < a.n;
+    key[r] = ok ? load_key(a, f, i) : 0xffffffffu;
+    val[r] = ok ? (a.first ? i : a.vin[(size_t)f * a.n + i]) : 0u;
+    const uint32_t d = ok ? (key[r] >> a.shift) & 255u : 256u;
+    const unsigned grp = __match_any_sync(FULL, d);
+    rank[r] = ok ? wcnt[warp][d] + __popc(grp & lt) : 0u;
+    __syncwarp();
+    if (ok && (grp >> lane) == 1u) wcnt[warp][d] += __popc(grp);
+    __syncwarp();
+  }
+  __syncthreads();
+  // exclusive prefix over warps, per digit (in place)
+  for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x) {
+    uint32_t run = a.hist[((size_t)f * 256 + d) * a.tiles + tile];
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) {
+      const uint32_t c = wcnt[w][d];
+      wcnt[w][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_ROUNDS; ++r) {
+    const uint32_t i = lo + r * 32 + lane;
+    if (i >= a.n) continue;
+    const uint32_t d = (key[r] >> a.shift) & 255u;
+    const uint32_t dst = wcnt[warp][d] + rank[r];
+    if (dst >= a.n) continue;
+    if (a.last) {
+      if (a.index_bytes == 2)
+        reinterpret_cast<uint16_t*>(a.final_out)[(size_t)f * a.n + dst] = (uint16_t)val[r];
+      else
+        reinterpret_cast<uint32_t*>(a.final_out)[(size_t)f * a.n + dst] = val[r];
+    } else {
+      a.kout[(size_t)f * a.n + dst] = key[r];
+      a.vout[(size_t)f * a.n + dst] = val[r];
+    }
+  }
+}
+
+}  // namespace
+
+size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features) {
+  const size_t tiles = ceil_div(n_rows, RS_TILE);
+  const size_t elems = (size_t)n_rows * n_features;
+  return 4 * elems * sizeof(uint32_t) + (size_t)n_features * 256 * tiles * sizeof(uint32_t) + 5 * 256;
+}
+
+int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
+            size_t wsb, cudaStream_t st) {
+  CT_ARG_CHECK(x_fm && out && ws, "presort: NULL argument");
+  CT_ARG_CHECK(n_rows >= 1 && n_features >= 1 && n_features <= 65535u, "presort: bad shape");
+  CT_ARG_CHECK(index_bytes == 4 || (index_bytes == 2 && n_rows <= 0xFFFFu), "presort: bad index width");
+  const uint32_t tiles = ceil_div(n_rows, RS_TILE);
+  const size_t elems = (size_t)n_rows * n_features;
+  Arena ar{reinterpret_cast<char*>(ws), wsb, 0};
+  uint32_t* k0 = ar.take<uint32_t>(elems);
+  uint32_t* v0 = ar.take<uint32_t>(elems);
+  uint32_t* k1 = ar.take<uint32_t>(elems);
+  uint32_t* v1 = ar.take<uint32_t>(elems);
+  uint32_t* hist = ar.take<uint32_t>((size_t)n_features * 256 * tiles);
+  if (!hist) {
+    set_last_error("presort workspace too small");
+    return CT_ERR_OOM;
+  }
+  RadixArgs a;
+  a.x = x_fm;
+  a.final_out = out;
+  a.hist = hist;
+  a.n = n_rows;
+  a.tiles = tiles;
+  a.index_bytes = index_bytes;
+  const dim3 grid(tiles, n_features);
+  for (uint32_t pass = 0; pass < 4; ++pass) {
+    a.shift = pass * 8;
+    a.first = pass == 0;
+    a.last = pass == 3;
+    a.kin = (pass & 1) ? k0 : k1;
+    a.vin = (pass & 1) ? v0 : v1;
+    a.kout = (pass & 1) ? k1 : k0;
+    a.vout = (pass & 1) ? v1 : v0;
+    k_digit_hist<<<grid, RS_THREADS, 0, st>>>(a);
+    k_digit_scan<<<n_features, 1024, 0, st>>>(hist, tiles);
+    k_digit_move<<<grid, RS_THREADS, 0, st>>>(a);
+  }
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+}  // namespace ct

@@ -1,0 +1,321 @@
+"""Drop-in ``RandomForestClassifier`` for CudaTree's fit/predict path.
+
+Surface of the reference ``cudatree/random_forest.py``:
+``RandomForestClassifier(n_estimators=10, max_features=None,
+min_samples_split=1, bootstrap=True, verbose=False, debug=False)``
+(:45-83), ``fit(samples, target, bfs_threshold=None)`` (:292-336),
+``predict(x)`` (:339-362), ``predict_proba(x)`` (:364-377), ``score``
+(:379), pickling through ``__reduce__`` (:18-23, :42-43), and the
+``fit_init`` / ``fit_release`` pair used by hybrid callers (:215-276).
+
+Everything between the host arrays and the fitted node arrays runs in
+``libcudatree_b200.so`` on the current CUDA device; PyTorch only owns the
+device buffers and the stream.  Two keyword-only extensions: ``seed`` (the
+reference draws from the global ``np.random`` state) and ``fit_mode``
+(``"batched"``: all trees of a chunk grow level-synchronously; ``"plain"``:
+the reference's per-node depth-first form).  Both give identical trees.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .random_tree import RandomClassifierTree
+
+
+def restore_forest(trees, dtype_labels, compt_table=None, n_features=None, params=None):
+    """Unpickle hook (reference random_forest.py:18-23).  Unlike the reference,
+    the restored forest keeps its label table and can predict."""
+    f = RandomForestClassifier(len(trees), **(params or {}))
+    f._trees = list(trees)
+    f.dtype_labels = np.dtype(dtype_labels)
+    if compt_table is not None:
+        f.compt_table = np.asarray(compt_table)
+        f.n_labels = int(f.compt_table.shape[0])
+    f.n_features = n_features
+    return f
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _device() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("cudatree_b200 needs a CUDA device (there is no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _dev_bytes(nbytes: int, dev) -> torch.Tensor:
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=dev)
+
+
+def _to_dev(a: np.ndarray, dev) -> torch.Tensor:
+    a = np.ascontiguousarray(a)
+    return torch.from_numpy(a.view(np.uint8).reshape(-1)).to(dev, non_blocking=False)
+
+
+def best_index_bytes(n_rows: int) -> int:
+    """Reference get_best_dtype(n) with uint8 promoted to uint16 (random_forest.py:224-227)."""
+    return 2 if n_rows <= 0xFFFF else 4
+
+
+def default_bfs_threshold(n_labels: int, n_samples: int, max_features: int) -> int:
+    """Reference random_forest.py:278-289 ("Titan" regression, clamped)."""
+    t = int(4746 + 4 * n_labels + 0.0651 * n_samples - 75 * max_features)
+    return max(min(t, 50000), 2000)
+
+
+PACKED_DTYPE = np.dtype([("threshold", "<f4"), ("feature", "<u4"), ("left", "<u4"), ("value", "<u4")])
+
+
+def pack_trees(trees):
+    """Flatten breadth-first trees into ct_packed_node records + tree offsets."""
+    sizes = [t.n_nodes for t in trees]
+    offsets = np.zeros(len(trees), dtype=np.uint32)
+    if trees:
+        offsets[1:] = np.cumsum(sizes[:-1])
+    packed = np.zeros(int(sum(sizes)), dtype=PACKED_DTYPE)
+    for t, off, n in zip(trees, offsets, sizes):
+        sl = packed[int(off):int(off) + n]
+        inner = t.left_children != 0
+        if np.any(t.right_children[inner] != t.left_children[inner] + 1):
+            raise ValueError("tree is not in breadth-first order (right != left + 1)")
+        sl["threshold"] = t.feature_threshold_array
+        sl["feature"] = t.feature_idx_array
+        sl["left"] = t.left_children
+        sl["value"] = t.values_array
+    return packed, offsets
+
+
+def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_votes):
+    dev = _device()
+    x = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    if x.ndim != 2 or x.shape[1] != n_features:
+        raise ValueError(f"x must have shape [n, {n_features}]")
+    n = x.shape[0]
+    if n == 0:
+        return np.zeros((0, n_classes) if want_votes else (0,), dtype=np.uint32)
+    nodes = packed if isinstance(packed, torch.Tensor) else _to_dev(packed, dev)
+    offs = offsets if isinstance(offsets, torch.Tensor) else _to_dev(offsets.astype(np.uint32), dev)
+    xd = torch.from_numpy(x).to(dev)
+    out = torch.empty((n, n_classes) if want_votes else (n,), dtype=torch.int32, device=dev)
+    _lib.call("ct_predict", _ptr(nodes), _ptr(offs), n_trees, _ptr(xd), n, n_features, n_classes,
+              _ptr(out) if want_votes else None, None if want_votes else _ptr(out), _stream())
+    return out.cpu().numpy().view(np.uint32)
+
+
+class RandomForestClassifier:
+    """A random forest classifier (Gini, fully grown trees) on one B200."""
+
+    def __init__(self, n_estimators=10, max_features=None, min_samples_split=1, bootstrap=True,
+                 verbose=False, debug=False, *, seed=None, fit_mode="batched"):
+        if fit_mode not in ("batched", "plain"):
+            raise ValueError("fit_mode must be 'batched' or 'plain'")
+        self.n_estimators = int(n_estimators)
+        self.max_features = max_features
+        self.min_samples_split = int(min_samples_split)
+        self.bootstrap = bool(bootstrap)
+        self.verbose = verbose
+        self.debug = debug
+        self.seed = seed
+        self.fit_mode = fit_mode
+        self._trees = []
+        self._packed = None
+        self.last_fit_timing = {}
+
+    # ------------------------------------------------------------ pickling
+    def _params(self):
+        return dict(max_features=self.max_features, min_samples_split=self.min_samples_split,
+                    bootstrap=self.bootstrap, seed=self.seed, fit_mode=self.fit_mode)
+
+    def __reduce__(self):
+        return restore_forest, (self._trees, getattr(self, "dtype_labels", np.dtype(np.uint8)).str,
+                                getattr(self, "compt_table", None), getattr(self, "n_features", None),
+                                self._params())
+
+    # ------------------------------------------------------------- fitting
+    def fit_init(self, samples, target):
+        """Validate, compact labels, upload and presort (random_forest.py:215-266)."""
+        x = np.asarray(samples)
+        y = np.asarray(target)
+        if x.ndim != 2:
+            raise ValueError("samples must be a 2-D array [n_samples, n_features]")
+        if y.ndim != 1 or y.shape[0] != x.shape[0]:
+            raise ValueError("target must be a 1-D array with one label per sample")
+        if x.shape[0] == 0:
+            raise ValueError("cannot fit on zero samples")
+        x32 = np.ascontiguousarray(x, dtype=np.float32)
+        if np.isnan(x32).any():
+            raise ValueError("samples contain NaN")
+        self.compt_table, y_c = np.unique(y, return_inverse=True)
+        self.n_labels = int(self.compt_table.shape[0])
+        if self.n_labels > _lib.MAX_CLASSES:
+            raise ValueError(f"at most {_lib.MAX_CLASSES} classes are supported")
+        self.n_samples, self.n_features = x32.shape
+        if self.n_features > _lib.MAX_FEATURES - 1:
+            raise ValueError("too many features")
+        self.stride = self.n_samples
+        self.index_bytes = best_index_bytes(self.n_samples)
+        self.dtype_indices = np.dtype(np.uint16 if self.index_bytes == 2 else np.uint32)
+        self.dtype_labels = np.dtype(np.uint8 if self.n_labels <= 0xFF else np.uint16)
+        m = self.max_features
+        if m is None:
+            m = int(math.ceil(math.sqrt(self.n_features)))
+        m = int(m)
+        if not (0 < m <= self.n_features):
+            raise ValueError("max_features must be in [1, n_features]")
+        self._m = m
+        self.bfs_threshold = default_bfs_threshold(self.n_labels, self.n_samples, m)
+        self._seed = int(np.random.randint(0, 2**62)) if self.seed is None else int(self.seed)
+        dev = _device()
+        t0 = time.perf_counter()
+        xd = torch.from_numpy(x32).to(dev)
+        self._x_fm = xd.t().contiguous()
+        self._labels = _to_dev(y_c.astype(self.dtype_labels), dev)
+        self._presort = _dev_bytes(self.n_features * self.n_samples * self.index_bytes, dev)
+        ws = C.c_size_t()
+        _lib.call("ct_presort_workspace_size", self.n_samples, self.n_features, C.byref(ws))
+        pws = _dev_bytes(ws.value, dev)
+        _lib.call("ct_presort", _ptr(self._x_fm), self.n_samples, self.n_features, self.index_bytes,
+                  _ptr(self._presort), _ptr(pws), ws.value, _stream())
+        del pws
+        self.last_fit_timing = {"upload_presort_s": time.perf_counter() - t0}
+
+    def _problem(self) -> _lib.Problem:
+        return _lib.Problem(_ptr(self._x_fm), _ptr(self._labels), _ptr(self._presort), self.n_samples,
+                            self.n_features, self.n_labels, self.index_bytes, self.dtype_labels.itemsize,
+                            self._m, self.min_samples_split, int(self.bootstrap), self._seed)
+
+    def fit_release(self):
+        self._x_fm = None
+        self._labels = None
+        self._presort = None
+
+    def _slot_bytes(self) -> int:
+        n, f = self.n_samples, self.n_features
+        return 2 * f * n * self.index_bytes + n + 2 * n * 20
+
+    def trees_in_flight(self, mode: str) -> int:
+        if mode == "plain":
+            return 1
+        prob = self._problem()
+        opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, 0, 0)
+        free, _ = torch.cuda.mem_get_info()
+        budget = int(free * 0.7)
+        k = self.n_estimators
+        while k > 1:
+            ws = C.c_size_t()
+            _lib.call("ct_fit_workspace_size", C.byref(prob), k, C.byref(opts), C.byref(ws))
+            if k * self._slot_bytes() + ws.value <= budget:
+                break
+            k = max(1, k // 2)
+        return k
+
+    def _fit_trees(self, first: int, count: int, mode: str, bfs_threshold: int):
+        dev = _device()
+        prob = self._problem()
+        n, f = self.n_samples, self.n_features
+        mode_id = _lib.CT_FIT_PLAIN if mode == "plain" else _lib.CT_FIT_BATCHED
+        k = min(self.trees_in_flight(mode), count)
+        slots = 1 if mode == "plain" else k
+        per_call = 1 if mode == "plain" else k
+        si0 = _dev_bytes(slots * f * n * self.index_bytes, dev)
+        si1 = _dev_bytes(slots * f * n * self.index_bytes, dev)
+        mark = _dev_bytes(slots * n, dev)
+        lists = _lib.Lists(_ptr(si0), _ptr(si1), _ptr(mark), n, slots)
+        cap = 2 * n
+        raw = {name: torch.empty(per_call * cap, dtype=torch.int32, device=dev)
+               for name in ("left", "right", "feature", "threshold", "value")}
+        n_nodes = torch.zeros(per_call, dtype=torch.int32, device=dev)
+        tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
+                              _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
+        opts = _lib.FitOptions(mode_id, int(bfs_threshold), 0, 0)
+        ws = C.c_size_t()
+        _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))
+        work = _dev_bytes(ws.value, dev)
+        trees = []
+        for t0 in range(first, first + count, per_call):
+            kk = min(per_call, first + count - t0)
+            _lib.call("ct_fit", C.byref(prob), C.byref(lists), t0, kk, C.byref(opts), C.byref(tb),
+                      _ptr(work), ws.value, _stream())
+            counts = n_nodes[:kk].cpu().numpy().astype(np.int64)
+            for s in range(kk):
+                trees.append(self._canonical_tree(raw, s * cap, int(counts[s])))
+        return trees
+
+    def _canonical_tree(self, raw, off, n_nodes):
+        host = {k: v[off:off + n_nodes].cpu().numpy() for k, v in raw.items()}
+        left = np.empty(n_nodes, np.uint32)
+        right = np.empty(n_nodes, np.uint32)
+        feat = np.empty(n_nodes, np.uint16)
+        thr = np.empty(n_nodes, np.float32)
+        val = np.empty(n_nodes, np.uint32)
+        src = [np.ascontiguousarray(host[k]) for k in ("left", "right", "feature", "threshold", "value")]
+        _lib.call("ct_tree_canonicalize", *[a.ctypes.data for a in src], n_nodes, left.ctypes.data,
+                  right.ctypes.data, feat.ctypes.data, thr.ctypes.data, val.ctypes.data)
+        tree = RandomClassifierTree(self)
+        tree.left_children = left
+        tree.right_children = right
+        tree.feature_idx_array = feat
+        tree.feature_threshold_array = thr
+        tree.values_array = val.astype(self.dtype_labels)
+        tree.dtype_labels = self.dtype_labels
+        tree.n_features = self.n_features
+        return tree
+
+    def fit(self, samples, target, bfs_threshold=None):
+        """Grow n_estimators trees (reference random_forest.py:292-336); returns self."""
+        t0 = time.perf_counter()
+        self.fit_init(samples, target)
+        if bfs_threshold is not None:
+            self.bfs_threshold = int(bfs_threshold)
+        if self.verbose:
+            print(f"bfs_threshold : {self.bfs_threshold}; bootstrap : {self.bootstrap}; "
+                  f"min_samples_split : {self.min_samples_split}; fit_mode : {self.fit_mode}")
+            print(f"n_samples : {self.n_samples}; n_features : {self.n_features}; "
+                  f"n_labels : {self.n_labels}; max_features : {self._m}")
+        self._trees = self._fit_trees(0, self.n_estimators, self.fit_mode, self.bfs_threshold)
+        self._packed = None
+        self.fit_release()
+        torch.cuda.synchronize()
+        self.last_fit_timing["fit_s"] = time.perf_counter() - t0
+        return self
+
+    # ----------------------------------------------------------- predict
+    def _device_forest(self):
+        if self._packed is None:
+            dev = _device()
+            packed, offsets = pack_trees(self._trees)
+            self._packed = (_to_dev(packed, dev), _to_dev(offsets, dev))
+        return self._packed
+
+    def _votes(self, x) -> np.ndarray:
+        if not self._trees:
+            raise ValueError("forest is not fitted")
+        nodes, offs = self._device_forest()
+        return _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, True)
+
+    def predict(self, x):
+        """Majority vote, lowest class on ties, in original label space (random_forest.py:339-362)."""
+        if not self._trees:
+            raise ValueError("forest is not fitted")
+        nodes, offs = self._device_forest()
+        res = _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, False)
+        return self.compt_table[res.astype(np.int64)]
+
+    def predict_proba(self, x):
+        """Vote fractions per class, float64 [n, n_labels] (random_forest.py:364-377)."""
+        return self._votes(x).astype(np.float64) / len(self._trees)
+
+    def score(self, X, Y):
+        return float(np.mean(self.predict(X) == np.asarray(Y)))

@@ -1,0 +1,200 @@
+/*
+ * cudatree_b200 — C ABI of the B200 random-forest fit + predict engine.
+ *
+ * Every entry point returns an int status (CT_OK == 0); ct_last_error() gives
+ * the text of the last failure on the calling thread.  Pointers named *_dev
+ * or documented as device pointers are CUDA device memory owned by the caller;
+ * `stream` is a cudaStream_t (NULL = legacy default stream).  The library
+ * allocates no device memory on these paths: callers size a workspace with
+ * the matching *_workspace_size call and pass it in.  The only objects the
+ * library owns across calls are the opaque handles of the serving engine.
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the EasonLiao/CudaTree source tree).
+ */
+#ifndef CUDATREE_B200_H
+#define CUDATREE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  CT_OK = 0,
+  CT_ERR_ARG = 1,         /* invalid argument or size                      */
+  CT_ERR_OOM = 2,         /* workspace too small / device memory exhausted  */
+  CT_ERR_CUDA = 3,        /* a CUDA runtime call failed                     */
+  CT_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up             */
+  CT_ERR_UNSUPPORTED = 5, /* shape outside the supported limits             */
+  CT_ERR_INTERNAL = 6,    /* device-side consistency check failed           */
+  CT_ERR_CAPACITY = 7     /* tree node capacity exceeded                    */
+};
+
+enum { CT_FIT_PLAIN = 0, CT_FIT_BATCHED = 1 };
+
+/* Limits of this build. */
+#define CT_MAX_CLASSES 1024u
+#define CT_MAX_FEATURES 65536u
+
+/* Training problem.  Device pointers.  Replaces the state fit_init builds
+ * (cudatree/random_forest.py:215-266): feature-major samples (:233), compacted
+ * labels (:85-99, :220), presorted indices (:247-248), dtype choice (:224-230). */
+typedef struct ct_problem {
+  const float* x_fm;          /* [n_features][n_rows] float32                    */
+  const void* labels;         /* [n_rows] class ids, uint8 or uint16             */
+  const void* presort;        /* [n_features][n_rows] stable ascending row order */
+  uint32_t n_rows;
+  uint32_t n_features;
+  uint32_t n_classes;
+  uint32_t index_bytes;       /* 2 (n_rows <= 65535) or 4                        */
+  uint32_t label_bytes;       /* 1 (n_classes <= 255) or 2                       */
+  uint32_t max_features;      /* features examined per node                      */
+  uint32_t min_samples_split; /* random_forest.py:47                             */
+  uint32_t bootstrap;         /* random_forest.py:48                             */
+  uint64_t seed;              /* forest seed for all random streams              */
+} ct_problem;
+
+/* Double-buffered per-tree index lists (reference sorted_indices_gpu and
+ * sorted_indices_gpu_, random_tree.py:466-467).  Slot s, buffer b, feature f
+ * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark is
+ * [n_slots][n_rows] bytes (reference mark_table, random_forest.py:168). */
+typedef struct ct_lists {
+  void* si0;
+  void* si1;
+  uint8_t* mark;
+  uint32_t stride;
+  uint32_t n_slots;
+} ct_lists;
+
+/* One tree node waiting for a split (reference queue entry idx_array /
+ * si_idx_array / nid_array, random_tree.py:617-621). 32 bytes. */
+typedef struct ct_node {
+  uint32_t slot;     /* tree slot holding the node's lists                 */
+  uint32_t start;    /* first position of the node in every feature list   */
+  uint32_t n;        /* samples in the node                                */
+  uint32_t raw_id;   /* node id in the slot's raw tree arrays              */
+  uint64_t key;      /* path key (selects the node's feature subset)       */
+  float impurity;    /* impurity reported by the parent split (root 1.0)   */
+  uint32_t buf;      /* which index-list buffer holds the node (0 or 1)    */
+} ct_node;
+
+/* Best split of one node (reference find_min_imp output, dfs_module.cu:202-206,
+ * plus the threshold of random_tree.py:641-644). 32 bytes. */
+typedef struct ct_split_result {
+  double score;       /* imp_left + imp_right in fp64; +inf if none        */
+  uint32_t feature;   /* chosen feature, 0xffffffff if none                */
+  uint32_t pos;       /* last position of the left child in that feature   */
+  float imp_left;
+  float imp_right;
+  float threshold;
+  uint32_t n_selected; /* non-constant features examined                   */
+} ct_split_result;
+
+/* Raw tree storage for n_slots trees, nodes in allocation order.  Replaces
+ * the per-tree node arrays of random_tree.py:284-289. */
+typedef struct ct_tree_buffers {
+  uint32_t* left;      /* [n_slots][capacity], 0 = leaf                    */
+  uint32_t* right;
+  uint32_t* feature;
+  float* threshold;
+  uint32_t* value;     /* leaf class id                                    */
+  uint32_t* n_nodes;   /* [n_slots]                                        */
+  uint32_t capacity;   /* >= 2 * n_rows                                    */
+} ct_tree_buffers;
+
+typedef struct ct_fit_options {
+  uint32_t mode;            /* CT_FIT_PLAIN or CT_FIT_BATCHED                       */
+  uint32_t bfs_threshold;   /* plain: nodes with n <= this go to the BFS queue
+                               (random_tree.py:616-622); 0 = reference formula     */
+  uint32_t subtree_cutoff;  /* batched: nodes with n <= this are grown whole by one
+                               warp (<= 32; 0 disables)                             */
+  uint32_t scan_piece;      /* elements per split-scan work item (0 = default)      */
+  uint32_t reserved[4];
+} ct_fit_options;
+
+/* ---------------------------------------------------------------- info --- */
+const char* ct_version(void);
+/* Copies the last error text of this thread into buf; returns its length. */
+int ct_last_error(char* buf, size_t len);
+
+/* ---------------------------------------------------- data preparation --- */
+/* Stable per-feature presort (replaces host np.argsort, random_forest.py:247).
+ * x_fm [n_features][n_rows] -> out [n_features][n_rows] row ids (index_bytes). */
+int ct_presort_workspace_size(uint32_t n_rows, uint32_t n_features, size_t* bytes);
+int ct_presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes,
+               void* out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* In-bag rows of tree `tree` and stable compaction of every presorted row
+ * into buffer 0 of `slot` (replaces _get_sorted_indices + bootstrap_fill.cu +
+ * bootstrap_reshuffle.cu, random_forest.py:113-144).  n_in_dev[slot] receives
+ * the in-bag count.  Without bootstrap the presort is copied. */
+int ct_bootstrap_workspace_size(const ct_problem* p, size_t* bytes);
+int ct_bootstrap_compact(const ct_problem* p, const ct_lists* lists, uint32_t slot, uint32_t tree,
+                         uint32_t* n_in_dev, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------- hot path, per level --- */
+/* Feature selection + Gini split scan + min-impurity reduction for n_nodes
+ * nodes (replaces scan_gini_large/scan_reduce/compute_2d/reduce_2d/
+ * find_min_imp, dfs_module.cu:24-208 + :310-491, and the BFS
+ * scan_bfs/compute_2d/reduce/get_thresholds, bfs_module.cu:25-235, :379-401).
+ * nodes/totals ([n_nodes][n_classes] uint32)/out/selected
+ * ([n_nodes][max_features] uint32) are device pointers. */
+int ct_split_workspace_size(const ct_problem* p, uint32_t n_nodes, uint64_t total_samples,
+                            size_t* bytes);
+int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* nodes,
+                   const uint32_t* totals, uint32_t n_nodes, ct_split_result* out,
+                   uint32_t* selected, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Mark table + stable partition of every feature's node range into the
+ * other buffer for each node whose split has a feature (replaces fill_table +
+ * scan_reshuffle, dfs_module.cu:210-307, bfs_module.cu:238-377). */
+int ct_partition_workspace_size(const ct_problem* p, uint32_t n_nodes, uint64_t total_samples,
+                                size_t* bytes);
+int ct_partition_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* nodes,
+                       const ct_split_result* splits, uint32_t n_nodes, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
+/* -------------------------------------------------------- forest fit --- */
+/* Grows trees first_tree .. first_tree+n_trees-1 into slots 0..n_trees-1 of
+ * `trees` (replaces RandomForestClassifier.fit's tree loop + RandomClassifierTree.fit,
+ * random_forest.py:292-336, random_tree.py:461-676).  Lists must hold n_trees slots. */
+int ct_fit_workspace_size(const ct_problem* p, uint32_t n_trees, const ct_fit_options* opt,
+                          size_t* bytes);
+int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint32_t n_trees,
+           const ct_fit_options* opt, const ct_tree_buffers* trees, void* workspace,
+           size_t workspace_bytes, void* stream);
+
+/* Host-side: renumber one raw tree (host arrays) into breadth-first order,
+ * left child before right.  Output arrays hold n_nodes entries. */
+int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature,
+                         const float* threshold, const uint32_t* value, uint32_t n_nodes,
+                         uint32_t* out_left, uint32_t* out_right, uint16_t* out_feature,
+                         float* out_threshold, uint32_t* out_value);
+
+/* ----------------------------------------------------------- predict --- */
+/* Packed forest: node i of the flat array is {threshold, feature, left, value}
+ * with children left and left+1 inside the tree (breadth-first order);
+ * tree_offset[t] is the first node of tree t.  Replaces BaseTree.gpu_predict +
+ * predict.cu (base_tree.py:44-81, predict.cu:12-69) and the host vote
+ * (random_forest.py:339-377).  x [n_rows][n_features] float32 row-major;
+ * votes [n_rows][n_classes] uint32 (may be NULL); pred [n_rows] uint32 class
+ * ids (may be NULL).  All device pointers. */
+typedef struct ct_packed_node {
+  float threshold;
+  uint32_t feature;
+  uint32_t left;   /* 0 = leaf; else index (within the tree) of the left child */
+  uint32_t value;  /* leaf class id                                           */
+} ct_packed_node;
+
+int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees,
+               const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
+               uint32_t* votes, uint32_t* pred, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUDATREE_B200_H */

@@ -1,0 +1,125 @@
+"""CPU-side checks of the C ABI: the library loads, exports every symbol the
+header declares, validates arguments without touching a GPU, and the
+host-side canonical renumbering matches a breadth-first walk."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cudatree_b200 import _lib
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "cudatree_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ct_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_loads_and_exports_header_symbols():
+    lib = _lib.load()
+    names = declared_functions()
+    assert len(names) >= 14
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(_lib.PROTOTYPES), "ctypes prototypes missing for some exports"
+    assert "sm_100a" in _lib.version()
+
+
+def test_struct_layouts_match_header_sizes():
+    assert C.sizeof(_lib.Node) == 32
+    assert C.sizeof(_lib.SplitResult) == 32
+    assert C.sizeof(_lib.PackedNode) == 16
+    assert np.dtype(_lib.NODE_DTYPE_FIELDS).itemsize == 32
+    assert np.dtype(_lib.SPLIT_DTYPE_FIELDS).itemsize == 32
+
+
+def test_argument_errors_are_reported_without_gpu():
+    lib = _lib.load()
+    st = lib.ct_predict(None, None, 0, None, 0, 0, 0, None, None, None)
+    assert st == 1
+    assert "NULL" in _lib.last_error()
+    prob = _lib.Problem(1, 1, 1, 10, 4, 3, 3, 1, 9, 1, 0, 0)  # uint16 index width is 2 or 4 only
+    ws = C.c_size_t()
+    st = lib.ct_fit(C.byref(prob), None, 0, 1, None, None, None, 0, None)
+    assert st != 0
+    with pytest.raises(_lib.CudaTreeError):
+        _lib.check(st)
+
+
+def test_workspace_size_queries_are_host_only():
+    prob = _lib.Problem(1, 1, 1, 581012, 54, 7, 4, 1, 7, 1, 1, 0)
+    ws = C.c_size_t()
+    for mode in (_lib.CT_FIT_PLAIN, _lib.CT_FIT_BATCHED):
+        opts = _lib.FitOptions(mode, 0, 0, 0)
+        _lib.call("ct_fit_workspace_size", C.byref(prob), 8, C.byref(opts), C.byref(ws))
+        assert ws.value > 0
+    _lib.call("ct_split_workspace_size", C.byref(prob), 100, 1 << 20, C.byref(ws))
+    assert ws.value > 0
+    _lib.call("ct_presort_workspace_size", 1000, 10, C.byref(ws))
+    assert ws.value >= 4 * 4 * 1000 * 10
+
+
+def _random_raw_tree(rng, n_inner):
+    # grow a random binary tree with ids in random allocation order
+    n = 2 * n_inner + 1
+    perm = np.concatenate([[0], 1 + rng.permutation(n - 1)])
+    left = np.zeros(n, np.uint32)
+    right = np.zeros(n, np.uint32)
+    feat = np.zeros(n, np.uint32)
+    thr = np.zeros(n, np.float32)
+    val = rng.integers(0, 5, n).astype(np.uint32)
+    leaves = [0]
+    nxt = 1
+    for _ in range(n_inner):
+        k = int(rng.integers(0, len(leaves)))
+        v = leaves.pop(k)
+        a, b = perm[nxt], perm[nxt + 1]
+        nxt += 2
+        left[perm[v] if False else v] = a
+        right[v] = b
+        feat[v] = rng.integers(0, 50)
+        thr[v] = rng.normal()
+        val[v] = 0
+        leaves += [a, b]
+    return left, right, feat, thr, val
+
+
+def test_canonicalize_is_breadth_first():
+    rng = np.random.default_rng(0)
+    left, right, feat, thr, val = _random_raw_tree(rng, 200)
+    n = left.shape[0]
+    out = [np.empty(n, np.uint32), np.empty(n, np.uint32), np.empty(n, np.uint16), np.empty(n, np.float32),
+           np.empty(n, np.uint32)]
+    _lib.call("ct_tree_canonicalize", left.ctypes.data, right.ctypes.data, feat.ctypes.data, thr.ctypes.data,
+              val.ctypes.data, n, *[o.ctypes.data for o in out])
+    ol, orr, of, ot, ov = out
+    # Python BFS
+    order, q = [], [0]
+    while q:
+        r = q.pop(0)
+        order.append(r)
+        if left[r] and right[r]:
+            q += [int(left[r]), int(right[r])]
+    new = {r: i for i, r in enumerate(order)}
+    for i, r in enumerate(order):
+        inner = left[r] != 0
+        assert ol[i] == (new[int(left[r])] if inner else 0)
+        assert orr[i] == (new[int(right[r])] if inner else 0)
+        assert of[i] == feat[r] and ot[i] == thr[r] and ov[i] == val[r]
+    inner = ol != 0
+    assert np.all(orr[inner] == ol[inner] + 1)
+
+
+def test_canonicalize_rejects_unreachable_nodes():
+    left = np.array([1, 0, 0, 0], np.uint32)
+    right = np.array([2, 0, 0, 0], np.uint32)
+    z = np.zeros(4, np.uint32)
+    out = [np.empty(4, t) for t in (np.uint32, np.uint32, np.uint16, np.float32, np.uint32)]
+    st = _lib.load().ct_tree_canonicalize(left.ctypes.data, right.ctypes.data, z.ctypes.data,
+                                         np.zeros(4, np.float32).ctypes.data, z.ctypes.data, 4,
+                                         *[o.ctypes.data for o in out])
+    assert st == 6 and "unreachable" in _lib.last_error()

@@ -1,0 +1,73 @@
+"""Whole-forest parity: plain and batched fits against the oracle, tree for
+tree and node for node, plus predict votes and the reference's memorize KATs."""
+import numpy as np
+import pytest
+from sklearn.datasets import load_diabetes, load_digits, load_iris
+
+from cudatree_b200 import RandomForestClassifier
+from oracle import cudatree_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _assert_same_trees(gpu_trees, oracle_trees):
+    assert len(gpu_trees) == len(oracle_trees)
+    for i, (a, b) in enumerate(zip(gpu_trees, oracle_trees)):
+        assert a.n_nodes == b.n_nodes, f"tree {i}: {a.n_nodes} vs {b.n_nodes} nodes"
+        np.testing.assert_array_equal(a.left_children, b.left, err_msg=f"tree {i} left")
+        np.testing.assert_array_equal(a.right_children, b.right, err_msg=f"tree {i} right")
+        np.testing.assert_array_equal(a.feature_idx_array, b.feature, err_msg=f"tree {i} feature")
+        np.testing.assert_array_equal(a.feature_threshold_array, b.threshold, err_msg=f"tree {i} thr")
+        np.testing.assert_array_equal(a.values_array.astype(np.int64), b.value, err_msg=f"tree {i} value")
+
+
+def _synthetic(n, f, c, seed):
+    rng = np.random.default_rng(seed)
+    y = rng.integers(0, c, size=n)
+    means = rng.normal(scale=1.5, size=(c, f))
+    x = (rng.normal(size=(n, f)) + means[y]).astype(np.float32)
+    x[:, ::3] = np.round(x[:, ::3])  # ties
+    return x, y
+
+
+DATASETS = {
+    "iris": lambda: (load_iris().data, load_iris().target),
+    "digits": lambda: (load_digits().data, load_digits().target),
+    "synthetic7": lambda: _synthetic(3000, 9, 7, 5),
+}
+
+
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+@pytest.mark.parametrize("name,bootstrap", [("iris", False), ("digits", True), ("synthetic7", True)])
+def test_fit_matches_oracle(cuda_device, name, bootstrap, mode):
+    x, y = DATASETS[name]()
+    forest = RandomForestClassifier(n_estimators=3, bootstrap=bootstrap, seed=123, fit_mode=mode)
+    forest.fit(x, y, bfs_threshold=500)
+    ref = O.fit_forest(x, y, n_estimators=3, bootstrap=bootstrap, seed=123)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
+    np.testing.assert_array_equal(forest.predict_proba(x), O.predict_proba(ref, x))
+
+
+def test_plain_equals_batched_large(cuda_device):
+    x, y = _synthetic(70000, 12, 5, 9)  # uint32 indices
+    a = RandomForestClassifier(n_estimators=4, seed=7, fit_mode="plain").fit(x, y)
+    b = RandomForestClassifier(n_estimators=4, seed=7, fit_mode="batched").fit(x, y)
+    for ta, tb in zip(a._trees, b._trees):
+        np.testing.assert_array_equal(ta.left_children, tb.left_children)
+        np.testing.assert_array_equal(ta.feature_idx_array, tb.feature_idx_array)
+        np.testing.assert_array_equal(ta.feature_threshold_array, tb.feature_threshold_array)
+        np.testing.assert_array_equal(ta.values_array, tb.values_array)
+
+
+@pytest.mark.parametrize("name", ["iris", "digits", "diabetes"])
+def test_memorize(cuda_device, name):
+    """Reference known-answer tests: test_iris.py:7-14, test_digits.py:10-17,
+    test_diabetes_classify.py:7-14 (bootstrap=False, zero training errors)."""
+    if name == "diabetes":
+        x, y = load_diabetes().data, load_diabetes().target > 140
+    else:
+        x, y = DATASETS[name]()
+    forest = RandomForestClassifier(n_estimators=6, bootstrap=False, seed=3)
+    forest.fit(x, y)
+    assert int((forest.predict(x) != y).sum()) == 0
