@@ -73,6 +73,22 @@ class PackedNode(C.Structure):
                 ("value", C.c_uint32)]
 
 
+class KernelStats(C.Structure):
+    _fields_ = [("launches", C.c_uint64 * 8), ("ms", C.c_double * 8), ("bytes", C.c_double * 8),
+                ("steps", C.c_uint64), ("total_launches", C.c_uint64)]
+
+
+KERNEL_GROUPS = ["select", "scan", "reduce", "mark", "partition", "children", "bootstrap", "subtree"]
+
+
+def fit_stats() -> dict:
+    """Per-kernel-group statistics of the last ct_fit on this thread."""
+    st = KernelStats()
+    call("ct_fit_stats", C.byref(st))
+    return {"launches": list(st.launches), "ms": list(st.ms), "bytes": list(st.bytes),
+            "steps": int(st.steps), "total_launches": int(st.total_launches)}
+
+
 NODE_DTYPE_FIELDS = [("slot", "<u4"), ("start", "<u4"), ("n", "<u4"), ("raw_id", "<u4"),
                      ("key", "<u8"), ("impurity", "<f4"), ("buf", "<u4")]
 SPLIT_DTYPE_FIELDS = [("score", "<f8"), ("feature", "<u4"), ("pos", "<u4"), ("imp_left", "<f4"),
@@ -99,6 +115,7 @@ PROTOTYPES = {
                                         C.POINTER(C.c_size_t)]),
     "ct_fit": (C.c_int, [C.POINTER(Problem), C.POINTER(Lists), C.c_uint32, C.c_uint32,
                          C.POINTER(FitOptions), C.POINTER(TreeBuffers), P, C.c_size_t, P]),
+    "ct_fit_stats": (C.c_int, [C.c_void_p]),
     "ct_tree_canonicalize": (C.c_int, [P, P, P, P, P, C.c_uint32, P, P, P, P, P]),
     "ct_predict": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
 }

@@ -27,6 +27,7 @@ SOURCES = [
     "ct_boot.cu",
     "ct_predict.cu",
     "ct_presort.cu",
+    "ct_partition.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -12,7 +12,7 @@ namespace ct {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
-size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features);
+size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots);
 int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
                       uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
 size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
@@ -68,7 +68,7 @@ int ct_presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t
 
 int ct_bootstrap_workspace_size(const ct_problem* p, size_t* bytes) {
   CT_ARG_CHECK(p && bytes, "NULL argument");
-  *bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features);
+  *bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, 1);
   return CT_OK;
 }
 
@@ -78,8 +78,20 @@ int ct_bootstrap_compact(const ct_problem* p, const ct_lists* lists, uint32_t sl
     CT_TRY(check_problem(p));
     CT_ARG_CHECK(lists && lists->si0 && lists->mark && n_in_dev, "NULL argument");
     if (p->bootstrap) CT_ARG_CHECK(workspace, "workspace is NULL");
-    if (workspace) CT_CUDA_TRY(cudaMemsetAsync(workspace, 0, 16, (cudaStream_t)stream));
-    return bootstrap_compact(p, lists, slot, tree, n_in_dev, workspace, workspace_bytes, (cudaStream_t)stream);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (workspace) CT_CUDA_TRY(cudaMemsetAsync(workspace, 0, 16, st));
+    CT_TRY(bootstrap_compact(p, lists, slot, tree, n_in_dev, workspace, workspace_bytes, st));
+    if (p->bootstrap) {
+      uint32_t words[2];
+      words[1] = 0;
+      CT_CUDA_TRY(cudaMemcpyAsync(words, workspace, sizeof(words), cudaMemcpyDeviceToHost, st));
+      CT_CUDA_TRY(cudaStreamSynchronize(st));
+      if (words[1]) {
+        set_last_error("bootstrap compaction look-back wait gave up");
+        return CT_ERR_TIMEOUT;
+      }
+    }
+    return CT_OK;
   })
 }
 
@@ -193,6 +205,12 @@ int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint
            void* stream) {
   CT_GUARD(return fit(p, lists, first_tree, n_trees, opt, trees, workspace, workspace_bytes,
                       (cudaStream_t)stream);)
+}
+
+int ct_fit_stats(ct_kernel_stats* out) {
+  CT_ARG_CHECK(out, "NULL argument");
+  *out = current_prof()->stats;
+  return CT_OK;
 }
 
 int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature,

@@ -1,188 +1,176 @@
-// Bootstrap: in-bag row set of a tree and the stable compaction of every
+// Bootstrap: in-bag row set of each tree and the stable compaction of every
 // presorted feature row onto it (reference _get_sorted_indices +
 // bootstrap_fill.cu + bootstrap_reshuffle.cu, random_forest.py:113-144).
 //
 // The reference draws N rows with np.random.randint and keeps np.unique of
 // them (random_forest.py:123-124); here draw i of tree t is
 // boot_draw(boot_key(tree_key(seed, t)), i, N), and the unique set is the
-// set of marked rows.  Compaction keeps the presorted order (stable), one
-// warp per (piece, feature) with a decoupled look-back across pieces.
+// set of marked rows.  The compaction is the tiled stable partition of
+// ct_partition.cu with the right (out-of-bag) part dropped; all slots of a
+// call are compacted by one launch.
 #include "ct_internal.cuh"
 
 namespace ct {
 
 namespace {
 
-constexpr uint64_t ST_AGG = 1ull << 62;
-constexpr uint64_t ST_INC = 2ull << 62;
-constexpr uint64_t ST_FLAG = 3ull << 62;
-constexpr uint64_t ST_VAL = (1ull << 62) - 1;
-constexpr uint32_t SPIN_LIMIT = 1u << 20;
-
-__global__ void k_boot_mark(uint8_t* mark, uint64_t bk, uint32_t n) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    mark[boot_draw(bk, i, n)] = 1;
+__global__ void k_boot_mark(uint8_t* mark, uint64_t seed, uint32_t tree_lo, uint32_t n) {
+  const uint32_t slot = blockIdx.y;
+  const uint64_t bk = boot_key(tree_key(seed, tree_lo + slot));
+  uint8_t* mk = mark + (size_t)slot * n;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    mk[boot_draw(bk, i, n)] = 1;
 }
 
 __global__ void k_count_marks(const uint8_t* mark, uint32_t n, uint32_t* out) {
+  const uint32_t slot = blockIdx.y;
+  const uint8_t* mk = mark + (size_t)slot * n;
   uint32_t c = 0;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    c += mark[i] ? 1u : 0u;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    c += mk[i] ? 1u : 0u;
   c = warp_sum_u32(c);
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(out + slot, c);
 }
 
-__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
+__global__ void k_set_u32(uint32_t* p, uint32_t v, uint32_t count) {
+  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) p[i] = v;
+}
 
-struct CompactArgs {
+struct BootPlan {
   const void* presort;
-  void* out;
-  const uint8_t* mark;
-  uint64_t* status;      // [n_features][pieces]
-  uint32_t* ticket;
-  uint32_t* error;
+  char* si0;              // slot 0 of buffer 0
+  const uint8_t* mark;    // slot 0 mark table
+  PartSeg* segs;
+  PartTile* tiles;
+  size_t slot_bytes;      // bytes between slots in si0
   uint32_t n_rows;
-  uint32_t n_features;
-  uint32_t pieces;
-  uint32_t out_stride;
+  uint32_t stride;
+  uint32_t tiles_per_slot;
 };
 
-template <typename IdxT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_compact(CompactArgs a) {
-  const uint32_t lane = lane_id();
-  uint32_t ticket = 0;
-  if (lane == 0) ticket = atomicAdd(a.ticket, 1u);
-  ticket = __shfl_sync(FULL, ticket, 0);
-  if ((uint64_t)ticket >= (uint64_t)a.pieces * a.n_features) return;
-  const uint32_t f = ticket / a.pieces;
-  const uint32_t j = ticket - f * a.pieces;
-  const IdxT* in = reinterpret_cast<const IdxT*>(a.presort) + (size_t)f * a.n_rows;
-  IdxT* out = reinterpret_cast<IdxT*>(a.out) + (size_t)f * a.out_stride;
-  const uint32_t lo = j * PART_PIECE;
-  uint32_t rows[PART_ROUNDS];
-  unsigned kmask[PART_ROUNDS];
-  uint32_t local = 0;
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    const uint32_t p = lo + r * 32 + lane;
-    rows[r] = p < a.n_rows ? (uint32_t)in[p] : 0u;
+__global__ void k_boot_plan(BootPlan b) {
+  const uint32_t slot = blockIdx.x;
+  if (threadIdx.x == 0) {
+    PartSeg sg;
+    sg.in = b.presort;
+    sg.out = b.si0 + slot * b.slot_bytes;
+    sg.mark = b.mark + (size_t)slot * b.n_rows;
+    sg.in_fstride = b.n_rows;
+    sg.out_fstride = b.stride;
+    sg.n = b.n_rows;
+    sg.nl = 0;
+    sg.keep_right = 0;
+    sg.status = slot * b.tiles_per_slot;
+    b.segs[slot] = sg;
   }
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    const uint32_t p = lo + r * 32 + lane;
-    kmask[r] = __ballot_sync(FULL, p < a.n_rows && a.mark[rows[r]] != 0);
-    local += __popc(kmask[r]);
+  for (uint32_t j = threadIdx.x; j < b.tiles_per_slot; j += blockDim.x) {
+    PartTile tl;
+    tl.seg = slot;
+    tl.j = j;
+    tl.ntiles = b.tiles_per_slot;
+    tl.pad = 0;
+    b.tiles[(size_t)slot * b.tiles_per_slot + j] = tl;
   }
-  uint64_t* col = a.status + (size_t)f * a.pieces;
-  uint32_t carry = 0;
-  if (lane == 0) {
-    if (j == 0) {
-      cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(col[0]).store(ST_INC | local,
-                                                                          cuda::memory_order_release);
-    } else {
-      cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(col[j]).store(ST_AGG | local,
-                                                                          cuda::memory_order_release);
-      uint64_t acc = 0;
-      uint32_t k = j - 1;
-      uint32_t spins = 0;
-      while (true) {
-        const uint64_t w =
-            cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(col[k]).load(cuda::memory_order_acquire);
-        const uint64_t flag = w & ST_FLAG;
-        if (flag == 0) {
-          if (++spins > SPIN_LIMIT || *reinterpret_cast<volatile uint32_t*>(a.error) != 0) {
-            atomicOr(a.error, DEV_ERR_TIMEOUT);
-            acc = 0;
-            break;
-          }
-          __nanosleep(64);
-          continue;
-        }
-        acc += w & ST_VAL;
-        if (flag == ST_INC || k == 0) break;
-        --k;
-      }
-      carry = (uint32_t)acc;
-      cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(col[j]).store(
-          ST_INC | (uint64_t)(carry + local), cuda::memory_order_release);
-    }
-  }
-  carry = __shfl_sync(FULL, carry, 0);
-  uint32_t run = carry;
-  const unsigned lt = lanemask_lt();
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    if ((kmask[r] >> lane) & 1u) {
-      const uint32_t dst = run + __popc(kmask[r] & lt);
-      if (dst < a.out_stride) out[dst] = (IdxT)rows[r];
-    }
-    run += __popc(kmask[r]);
-  }
+}
+
+struct BootLayout {
+  uint32_t* words;        // [0] ticket, [1] error, [2] n_big, [3] n_tiles, [4] n_small
+  PartSeg* segs;
+  PartTile* tiles;
+  uint64_t* status;
+  size_t bytes;
+};
+
+bool boot_layout(uint32_t n_rows, uint32_t n_features, uint32_t n_slots, void* ws, size_t wsb, BootLayout* L) {
+  Arena a{reinterpret_cast<char*>(ws), wsb, 0};
+  const size_t tiles = (size_t)ceil_div(n_rows, TILE_ELEMS) * n_slots;
+  L->words = a.take<uint32_t>(8);
+  L->segs = a.take<PartSeg>(n_slots);
+  L->tiles = a.take<PartTile>(tiles);
+  L->status = a.take<uint64_t>(tiles * n_features);
+  L->bytes = a.used + 256;
+  return ws != nullptr && a.ok();
 }
 
 }  // namespace
 
-size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features) {
-  const size_t pieces = ceil_div(n_rows, PART_PIECE);
-  return 512 + pieces * n_features * sizeof(uint64_t) + 256;
+size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots) {
+  BootLayout L;
+  boot_layout(n_rows, n_features, n_slots, nullptr, 0, &L);
+  return L.bytes;
 }
 
-int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
-                      uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st) {
+// Compacts slots [slot_lo, slot_lo + n_slots) for trees tree_lo.., one launch
+// per phase.  Error bits accumulate in the workspace's word [1]; the caller
+// zeroes it once and reads it after.
+int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
+                   uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st) {
   const uint32_t N = p->n_rows, F = p->n_features;
-  CT_ARG_CHECK(slot < l->n_slots, "slot out of range");
+  CT_ARG_CHECK(n_slots >= 1 && slot_lo + n_slots <= l->n_slots, "slot out of range");
   CT_ARG_CHECK(l->stride >= N, "list stride smaller than n_rows");
   CT_ARG_CHECK(p->presort != nullptr, "presort is NULL");
   const size_t ib = p->index_bytes;
-  char* dst = reinterpret_cast<char*>(l->si0) + (size_t)slot * F * l->stride * ib;
+  const size_t slot_bytes = (size_t)F * l->stride * ib;
+  char* dst = reinterpret_cast<char*>(l->si0) + slot_lo * slot_bytes;
   if (!p->bootstrap) {
-    CT_CUDA_TRY(cudaMemcpy2DAsync(dst, (size_t)l->stride * ib, p->presort, (size_t)N * ib, (size_t)N * ib, F,
-                                  cudaMemcpyDeviceToDevice, st));
-    k_set_u32<<<1, 1, 0, st>>>(n_in_dev + slot, N);
+    for (uint32_t s = 0; s < n_slots; ++s)
+      CT_CUDA_TRY(cudaMemcpy2DAsync(dst + s * slot_bytes, (size_t)l->stride * ib, p->presort, (size_t)N * ib,
+                                    (size_t)N * ib, F, cudaMemcpyDeviceToDevice, st));
+    k_set_u32<<<1, 256, 0, st>>>(n_in_dev + slot_lo, N, n_slots);
     CT_CUDA_TRY(cudaGetLastError());
     return CT_OK;
   }
-  Arena a{reinterpret_cast<char*>(ws), wsb, 0};
-  uint32_t* ctr = a.take<uint32_t>(4);  // ticket, error
-  const uint32_t pieces = ceil_div(N, PART_PIECE);
-  uint64_t* status = a.take<uint64_t>((size_t)pieces * F);
-  if (!ctr || !status) {
+  BootLayout L;
+  if (!boot_layout(N, F, n_slots, ws, wsb, &L)) {
     set_last_error("bootstrap workspace too small");
     return CT_ERR_OOM;
   }
-  uint8_t* mark = l->mark + (size_t)slot * N;
-  CT_CUDA_TRY(cudaMemsetAsync(mark, 0, N, st));
-  CT_CUDA_TRY(cudaMemsetAsync(ctr, 0, 4 * sizeof(uint32_t), st));
-  CT_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)pieces * F * sizeof(uint64_t), st));
-  CT_CUDA_TRY(cudaMemsetAsync(n_in_dev + slot, 0, sizeof(uint32_t), st));
-  const uint64_t bk = boot_key(tree_key(p->seed, tree));
-  const uint32_t grid = min(ceil_div(N, 256), 148u * 16u);
-  k_boot_mark<<<grid, 256, 0, st>>>(mark, bk, N);
-  k_count_marks<<<grid, 256, 0, st>>>(mark, N, n_in_dev + slot);
-  CompactArgs ca;
-  ca.presort = p->presort;
-  ca.out = dst;
-  ca.mark = mark;
-  ca.status = status;
-  ca.ticket = ctr;
-  ca.error = ctr + 1;
-  ca.n_rows = N;
-  ca.n_features = F;
-  ca.pieces = pieces;
-  ca.out_stride = l->stride;
-  const uint64_t warps = (uint64_t)pieces * F;
-  const uint32_t blocks = (uint32_t)((warps + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK);
-  if (ib == 2)
-    k_compact<uint16_t><<<blocks, THREADS_PER_BLOCK, 0, st>>>(ca);
-  else
-    k_compact<uint32_t><<<blocks, THREADS_PER_BLOCK, 0, st>>>(ca);
+  const uint32_t tiles_per = ceil_div(N, TILE_ELEMS);
+  uint8_t* mark = l->mark + (size_t)slot_lo * N;
+  CT_CUDA_TRY(cudaMemsetAsync(mark, 0, (size_t)n_slots * N, st));
+  CT_CUDA_TRY(cudaMemsetAsync(L.words, 0, sizeof(uint32_t), st));  // ticket (error word kept)
+  CT_CUDA_TRY(cudaMemsetAsync(L.status, 0, (size_t)tiles_per * n_slots * F * sizeof(uint64_t), st));
+  CT_CUDA_TRY(cudaMemsetAsync(n_in_dev + slot_lo, 0, n_slots * sizeof(uint32_t), st));
+  uint32_t counts[3] = {n_slots, tiles_per * n_slots, 0};
+  k_set_u32<<<1, 32, 0, st>>>(L.words + 2, counts[0], 1);
+  k_set_u32<<<1, 32, 0, st>>>(L.words + 3, counts[1], 1);
+  k_set_u32<<<1, 32, 0, st>>>(L.words + 4, 0, 1);
+  const dim3 grid(std::min<uint32_t>(ceil_div(N, 256), 1024), n_slots);
+  k_boot_mark<<<grid, 256, 0, st>>>(mark, p->seed, tree_lo, N);
+  k_count_marks<<<grid, 256, 0, st>>>(mark, N, n_in_dev + slot_lo);
+  BootPlan b;
+  b.presort = p->presort;
+  b.si0 = dst;
+  b.mark = mark;
+  b.segs = L.segs;
+  b.tiles = L.tiles;
+  b.slot_bytes = slot_bytes;
+  b.n_rows = N;
+  b.stride = l->stride;
+  b.tiles_per_slot = tiles_per;
+  k_boot_plan<<<n_slots, 128, 0, st>>>(b);
   CT_CUDA_TRY(cudaGetLastError());
-  return CT_OK;
+  PartWork w;
+  w.small = nullptr;
+  w.n_small = L.words + 4;
+  w.cap_small = 0;
+  w.big = L.segs;
+  w.n_big = L.words + 2;
+  w.cap_big = n_slots;
+  w.tiles = L.tiles;
+  w.n_tiles = L.words + 3;
+  w.cap_tiles = tiles_per * n_slots;
+  w.status = L.status;
+  w.cap_status = tiles_per * n_slots;
+  w.ticket = L.words;
+  w.error = L.words + 1;
+  w.n_features = F;
+  return launch_seg_partition((uint32_t)ib, w, 0, (uint64_t)tiles_per * n_slots, st);
 }
 
-// Error word of the last bootstrap_compact call (ticket at [0], error at [1]).
-uint32_t* bootstrap_error_word(void* ws) { return reinterpret_cast<uint32_t*>(ws) + 1; }
+int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree, uint32_t* n_in_dev,
+                      void* ws, size_t wsb, cudaStream_t st) {
+  return bootstrap_many(p, l, slot, 1, tree, n_in_dev, ws, wsb, st);
+}
 
 }  // namespace ct

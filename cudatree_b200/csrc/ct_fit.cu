@@ -19,26 +19,43 @@
 
 namespace ct {
 
-size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features);
-int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
-                      uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
+size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots);
+int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
+                   uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
 
 namespace {
 
 constexpr uint32_t CHUNK_NODES_MAX = 1u << 20;
 
+// Class histogram of every slot's in-bag rows: grid (blocks, slots), one
+// shared-memory histogram per block flushed with global atomics.
 template <typename IdxT, typename LabT>
-__global__ void k_root(View v, const uint32_t* n_in, uint32_t slot, uint64_t seed, uint32_t tree,
-                       TreeView tv, ct_node* out, uint32_t* out_tot, uint32_t cap, Counters* ctr) {
+__global__ void k_root_hist(View v, const uint32_t* n_in, uint32_t slot_lo, uint32_t* hist_out) {
   extern __shared__ uint32_t hist[];
-  __shared__ uint32_t s_idx;
+  const uint32_t slot = slot_lo + blockIdx.y;
   const uint32_t C = v.n_classes;
   for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) hist[c] = 0;
   __syncthreads();
   const uint32_t n = n_in[slot];
   const IdxT* lst = list_ptr<IdxT>(v, 0, slot, 0);
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&hist[label_of<LabT>(v, lst[i])], 1u);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(&hist[label_of<LabT>(v, lst[i])], 1u);
   __syncthreads();
+  for (uint32_t c = threadIdx.x; c < C; c += blockDim.x)
+    if (hist[c]) atomicAdd(&hist_out[(size_t)blockIdx.y * C + c], hist[c]);
+}
+
+// Root record of each slot (block per slot): a leaf if it holds fewer than
+// min_samples_split rows, else appended to the first level's list.
+template <typename IdxT, typename LabT>
+__global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t seed, uint32_t tree_lo,
+                       TreeView tv, const uint32_t* hist_in, ct_node* out, uint32_t* out_tot, uint32_t cap,
+                       Counters* ctr) {
+  __shared__ uint32_t s_idx;
+  const uint32_t slot = slot_lo + blockIdx.x;
+  const uint32_t C = v.n_classes;
+  const uint32_t n = n_in[slot];
+  const IdxT* lst = list_ptr<IdxT>(v, 0, slot, 0);
   if (threadIdx.x == 0) {
     const uint32_t ts = slot + tv.slot_base;
     tv.n_nodes[ts] = 1;
@@ -47,7 +64,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot, uint64_t see
     nd.start = 0;
     nd.n = n;
     nd.raw_id = 0;
-    nd.key = root_key(tree_key(seed, tree));
+    nd.key = root_key(tree_key(seed, tree_lo + blockIdx.x));
     nd.impurity = 1.0f;
     nd.buf = 0;
     s_idx = NONE;
@@ -71,7 +88,8 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot, uint64_t see
   }
   __syncthreads();
   if (s_idx != NONE)
-    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x) out_tot[(size_t)s_idx * C + c] = hist[c];
+    for (uint32_t c = threadIdx.x; c < C; c += blockDim.x)
+      out_tot[(size_t)s_idx * C + c] = hist_in[(size_t)blockIdx.x * C + c];
 }
 
 __global__ void k_begin_level(Counters* c) {
@@ -79,6 +97,23 @@ __global__ void k_begin_level(Counters* c) {
   c->n_small = 0;
   c->next_total = 0;
   c->small_total = 0;
+  c->split_total = 0;
+  c->scan_elems = 0;
+}
+
+void begin_level(Counters* c, cudaStream_t st) {
+  k_begin_level<<<1, 1, 0, st>>>(c);
+  current_prof()->launched(CT_K_CHILDREN);
+}
+
+// Algorithmic bytes of one level, from the device counters of the level.
+void account_level(const ct_problem* p, const Counters& h) {
+  Prof* pf = current_prof();
+  const double w = p->index_bytes, l = p->label_bytes, v = sizeof(float);
+  pf->stats.bytes[CT_K_SCAN] += (double)h.scan_elems * (w + l + v);
+  pf->stats.bytes[CT_K_MARK] += (double)h.split_total * (w + 1.0);
+  pf->stats.bytes[CT_K_PARTITION] += (double)h.split_total * p->n_features * (2.0 * w + 1.0);
+  pf->stats.steps += 1;
 }
 
 struct FitLayout {
@@ -111,7 +146,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
     L->list[i] = a.take<ct_node>(L->cap_list);
     L->tot[i] = a.take<uint32_t>((size_t)L->cap_list * p->n_classes);
   }
-  L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features);
+  L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, slots);
   L->boot_ws = a.take<char>(L->boot_bytes);
   LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
   carve_level_scratch(a, v, caps, &L->s);
@@ -152,23 +187,40 @@ int check_boot_error(const FitLayout& L, cudaStream_t st) {
   return CT_OK;
 }
 
+void account_bootstrap(const ct_problem* p) {
+  Prof* pf = current_prof();
+  const double w = p->index_bytes, n = p->n_rows, f = p->n_features;
+  // read presort + gather mark, write the in-bag part (about 0.632 n per feature)
+  pf->stats.bytes[CT_K_BOOTSTRAP] += n * f * (w + 1.0) + (p->bootstrap ? 0.632 : 1.0) * n * f * w;
+  pf->launched(CT_K_BOOTSTRAP, p->bootstrap ? 3 : 1);
+}
+
 template <typename IdxT, typename LabT>
-int launch_root(const View& v, const FitLayout& L, uint32_t slot, uint64_t seed, uint32_t tree,
-                const TreeView& tv, int cur, cudaStream_t st) {
-  k_root<IdxT, LabT><<<1, 256, v.n_classes * sizeof(uint32_t), st>>>(v, L.n_in, slot, seed, tree, tv,
-                                                                     L.list[cur], L.tot[cur], L.cap_list,
-                                                                     L.s.ctr);
+int launch_root(const View& v, const FitLayout& L, uint32_t slot_lo, uint32_t n_slots, uint64_t seed,
+                uint32_t tree_lo, const TreeView& tv, int cur, cudaStream_t st) {
+  const size_t C = v.n_classes;
+  // the histograms go to the tail of the next list's totals, which the root step does not use
+  uint32_t* hist = L.tot[1 - cur];
+  CT_CUDA_TRY(cudaMemsetAsync(hist, 0, n_slots * C * sizeof(uint32_t), st));
+  const uint32_t blocks = std::min<uint32_t>(ceil_div(v.n_rows, 256 * 8), 256);
+  k_root_hist<IdxT, LabT><<<dim3(blocks, n_slots), 256, C * sizeof(uint32_t), st>>>(v, L.n_in, slot_lo, hist);
+  k_root<IdxT, LabT><<<n_slots, 128, 0, st>>>(v, L.n_in, slot_lo, seed, tree_lo, tv, hist, L.list[cur],
+                                                L.tot[cur], L.cap_list, L.s.ctr);
+  current_prof()->launched(CT_K_CHILDREN, 2);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
 
-int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot, uint32_t tree,
-         const TreeView& tv, int cur, cudaStream_t st) {
+int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot_lo, uint32_t n_slots,
+         uint32_t tree_lo, const TreeView& tv, int cur, cudaStream_t st) {
   const uint32_t ib = p->index_bytes, lb = p->label_bytes;
-  if (ib == 2 && lb == 1) return launch_root<uint16_t, uint8_t>(v, L, slot, p->seed, tree, tv, cur, st);
-  if (ib == 2 && lb == 2) return launch_root<uint16_t, uint16_t>(v, L, slot, p->seed, tree, tv, cur, st);
-  if (ib == 4 && lb == 1) return launch_root<uint32_t, uint8_t>(v, L, slot, p->seed, tree, tv, cur, st);
-  return launch_root<uint32_t, uint16_t>(v, L, slot, p->seed, tree, tv, cur, st);
+  if (ib == 2 && lb == 1)
+    return launch_root<uint16_t, uint8_t>(v, L, slot_lo, n_slots, p->seed, tree_lo, tv, cur, st);
+  if (ib == 2 && lb == 2)
+    return launch_root<uint16_t, uint16_t>(v, L, slot_lo, n_slots, p->seed, tree_lo, tv, cur, st);
+  if (ib == 4 && lb == 1)
+    return launch_root<uint32_t, uint8_t>(v, L, slot_lo, n_slots, p->seed, tree_lo, tv, cur, st);
+  return launch_root<uint32_t, uint16_t>(v, L, slot_lo, n_slots, p->seed, tree_lo, tv, cur, st);
 }
 
 // One step over list[cur][0..n) -> children appended to list[1-cur].
@@ -193,10 +245,11 @@ int level_loop(const ct_problem* p, const View& v, const FitLayout& L, const Tre
                uint32_t n, uint64_t total, cudaStream_t st) {
   Counters h;
   while (n > 0) {
-    k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+    begin_level(L.s.ctr, st);
     CT_CUDA_TRY(cudaGetLastError());
     CT_TRY(step(p, v, L, tv, cur, n, total, st));
     CT_TRY(read_counters(L, &h, st));
+    account_level(p, h);
     n = h.n_next;
     total = h.next_total;
     cur = 1 - cur;
@@ -233,11 +286,13 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
   TreeView tv = tree_view(trees, 0);
   CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
   CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
-  for (uint32_t s = 0; s < n_trees; ++s)
-    CT_TRY(bootstrap_compact(p, l, s, first_tree + s, L.n_in, L.boot_ws, L.boot_bytes, st));
+  current_prof()->begin(CT_K_BOOTSTRAP);
+  CT_TRY(bootstrap_many(p, l, 0, n_trees, first_tree, L.n_in, L.boot_ws, L.boot_bytes, st));
+  current_prof()->end();
+  for (uint32_t s = 0; s < n_trees; ++s) account_bootstrap(p);
   CT_TRY(check_boot_error(L, st));
-  k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
-  for (uint32_t s = 0; s < n_trees; ++s) CT_TRY(root(p, v, L, s, first_tree + s, tv, 0, st));
+  begin_level(L.s.ctr, st);
+  CT_TRY(root(p, v, L, 0, n_trees, first_tree, tv, 0, st));
   Counters h;
   CT_TRY(read_counters(L, &h, st));
   return level_loop(p, v, L, tv, 0, h.n_next, h.next_total, st);
@@ -257,10 +312,13 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
   for (uint32_t t = 0; t < n_trees; ++t) {
     TreeView tv = tree_view(trees, t);
     CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
-    CT_TRY(bootstrap_compact(p, l, 0, first_tree + t, L.n_in, L.boot_ws, L.boot_bytes, st));
+    current_prof()->begin(CT_K_BOOTSTRAP);
+    CT_TRY(bootstrap_many(p, l, 0, 1, first_tree + t, L.n_in, L.boot_ws, L.boot_bytes, st));
+    current_prof()->end();
+    account_bootstrap(p);
     CT_TRY(check_boot_error(L, st));
-    k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
-    CT_TRY(root(p, v, L, 0, first_tree + t, tv, 0, st));
+    begin_level(L.s.ctr, st);
+    CT_TRY(root(p, v, L, 0, 1, first_tree + t, tv, 0, st));
     Counters h;
     CT_TRY(read_counters(L, &h, st));
     if (h.n_next == 0) continue;
@@ -280,9 +338,10 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
       }
       CT_CUDA_TRY(cudaMemcpyAsync(L.list[0], &cur.nd, sizeof(ct_node), cudaMemcpyHostToDevice, st));
       CT_CUDA_TRY(cudaMemcpyAsync(L.tot[0], cur.tot.data(), C * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-      k_begin_level<<<1, 1, 0, st>>>(L.s.ctr);
+      begin_level(L.s.ctr, st);
       CT_TRY(step(p, v, L, tv, 0, 1, cur.nd.n, st));
       CT_TRY(read_counters(L, &h, st));
+      account_level(p, h);
       std::vector<ct_node> kids(h.n_next);
       std::vector<uint32_t> ktot((size_t)h.n_next * C);
       if (h.n_next) {
@@ -352,8 +411,16 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
     set_last_error("fit workspace too small");
     return CT_ERR_OOM;
   }
-  if (o->mode == CT_FIT_PLAIN) return fit_plain(p, l, first_tree, n_trees, o, L, trees, st);
-  return fit_batched(p, l, first_tree, n_trees, L, trees, st);
+  Prof* pf = current_prof();
+  pf->finish();
+  pf->stats = ct_kernel_stats{};
+  pf->timing = (o->reserved[0] & 1u) != 0;
+  pf->st = st;
+  const int rc = (o->mode == CT_FIT_PLAIN) ? fit_plain(p, l, first_tree, n_trees, o, L, trees, st)
+                                           : fit_batched(p, l, first_tree, n_trees, L, trees, st);
+  pf->finish();
+  pf->timing = false;
+  return rc;
 }
 
 // ---------------------------------------------------------------------------

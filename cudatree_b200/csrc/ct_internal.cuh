@@ -4,6 +4,8 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include <cuda/atomic>
 
@@ -71,15 +73,55 @@ struct Counters {
   uint32_t n_scan_pieces;
   uint32_t n_carry;
   uint32_t n_splits;
-  uint32_t n_part_pieces;
+  uint32_t n_part_pieces; // mark-table pieces
   uint32_t n_status;
   uint32_t ticket;
   uint32_t error;
   uint32_t n_next;        // nodes appended to the next list
   uint32_t n_small;       // nodes appended to the subtree list
-  uint32_t pad[2];
+  uint32_t n_small_segs;  // partition segments of small splits
+  uint32_t n_big_segs;
+  uint32_t n_tiles;       // partition tiles of big splits
+  uint32_t pad[3];
   unsigned long long next_total;
   unsigned long long small_total;
+  unsigned long long split_total;  // samples in nodes partitioned this level
+  unsigned long long scan_elems;   // (node, feature) elements scanned this level
+};
+
+// One stable-partition segment: a node range in every feature list.
+struct PartSeg {
+  const void* in;         // element 0 of feature 0
+  void* out;
+  const uint8_t* mark;    // per-row left flag of the segment's tree
+  uint32_t in_fstride;    // elements between consecutive features
+  uint32_t out_fstride;
+  uint32_t n;
+  uint32_t nl;            // number of left rows
+  uint32_t keep_right;    // 0: right rows are dropped (compaction)
+  uint32_t status;        // first status slot (tiled segments)
+};
+struct PartTile {
+  uint32_t seg;
+  uint32_t j;
+  uint32_t ntiles;
+  uint32_t pad;
+};
+struct PartWork {
+  PartSeg* small;
+  uint32_t* n_small;
+  uint32_t cap_small;
+  PartSeg* big;
+  uint32_t* n_big;
+  uint32_t cap_big;
+  PartTile* tiles;
+  uint32_t* n_tiles;
+  uint32_t cap_tiles;
+  uint64_t* status;       // [n_features][cap_status]
+  uint32_t cap_status;
+  uint32_t* ticket;
+  uint32_t* error;
+  uint32_t n_features;
 };
 
 // View of the problem + lists passed by value to kernels.
@@ -138,10 +180,55 @@ struct LevelScratch {
   ct_split_result* result;// [cap_nodes]
   SplitRec* splits;       // [cap_nodes]
   uint32_t* split_left;   // [cap_nodes][n_classes]
-  PartPiece* part;        // [cap_part]
+  PartPiece* part;        // [cap_part] mark-table pieces
+  PartSeg* small_segs;    // [cap_nodes]
+  PartSeg* big_segs;      // [cap_nodes]
+  PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
 };
+
+// Per-kernel-group launch counts and CUDA-event timing of one fit.
+struct Prof {
+  bool timing = false;
+  cudaStream_t st = nullptr;
+  ct_kernel_stats stats{};
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ranges;
+  int open_kernel = -1;
+  cudaEvent_t open_ev = nullptr;
+  void begin(int k) {
+    if (!timing) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, st);
+    open_kernel = k;
+    open_ev = e;
+  }
+  void end() {
+    if (!timing || open_kernel < 0) return;
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, st);
+    ranges.push_back({open_kernel, {open_ev, e}});
+    open_kernel = -1;
+  }
+  void launched(int k, uint64_t n = 1) {
+    stats.launches[k] += n;
+    stats.total_launches += n;
+  }
+  void finish() {
+    if (!ranges.empty()) cudaStreamSynchronize(st);
+    for (auto& r : ranges) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.second.first, r.second.second);
+      stats.ms[r.first] += ms;
+      cudaEventDestroy(r.second.first);
+      cudaEventDestroy(r.second.second);
+    }
+    ranges.clear();
+  }
+};
+Prof* current_prof();  // profile of the fit running on this thread (never NULL)
 
 // Bump allocator over a caller workspace (256-byte aligned carving).
 struct Arena {
@@ -163,6 +250,8 @@ struct Arena {
 constexpr uint32_t DEFAULT_SCAN_PIECE = 2048;   // elements per split-scan work item
 constexpr uint32_t PART_ROUNDS = 16;            // rounds of 32 held in registers
 constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
+constexpr uint32_t TILE_ELEMS = 4096;           // partition tile of big segments
+constexpr uint32_t SMALL_SEG = 32 * PART_ROUNDS; // segments up to this size: one warp
 constexpr int WARPS_PER_BLOCK = 4;
 constexpr int THREADS_PER_BLOCK = 32 * WARPS_PER_BLOCK;
 
@@ -190,6 +279,11 @@ int launch_children(const View& v, uint32_t index_bytes, uint32_t label_bytes, c
                     const uint32_t* tot, const LevelScratch& s, LevelBounds b, const TreeView& tv,
                     ct_node* next, uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut,
                     ct_node* small, uint32_t cap_small, cudaStream_t st);
+// Stable partition of segments (ct_partition.cu).
+int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
+                         cudaStream_t st);
+PartWork level_part_work(const View& v, const LevelScratch& s);
+
 // Counter resets between steps (device-side, stream ordered).
 int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
 

@@ -25,26 +25,12 @@ namespace ct {
 
 namespace {
 
-constexpr uint64_t ST_AGG = 1ull << 62;
-constexpr uint64_t ST_INC = 2ull << 62;
-constexpr uint64_t ST_FLAG = 3ull << 62;
-constexpr uint64_t ST_VAL = (1ull << 62) - 1;
-constexpr uint32_t SPIN_LIMIT = 1u << 20;
-
 __device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
 __device__ __forceinline__ uint32_t global_warp() {
   return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
 }
 
-__device__ __forceinline__ void publish(uint64_t* p, uint64_t v) {
-  cuda::atomic_ref<uint64_t, cuda::thread_scope_device> a(*p);
-  a.store(v, cuda::memory_order_release);
-}
-__device__ __forceinline__ uint64_t poll(uint64_t* p) {
-  cuda::atomic_ref<uint64_t, cuda::thread_scope_device> a(*p);
-  return a.load(cuda::memory_order_acquire);
-}
 __device__ __forceinline__ uint32_t read_error(const Counters* c) {
   return *reinterpret_cast<const volatile uint32_t*>(&c->error);
 }
@@ -102,6 +88,7 @@ k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t sca
   uint32_t npieces = taken * pps;
   uint32_t base = 0, cbase = 0;
   if (lane == 0) {
+    if (taken) atomicAdd(&s.ctr->scan_elems, (unsigned long long)taken * nd.n);
     if (npieces) base = atomicAdd(&s.ctr->n_scan_pieces, npieces);
     if (npieces && pps > 1) cbase = atomicAdd(&s.ctr->n_carry, npieces);
     const bool overflow = (base + (uint64_t)npieces > s.cap_scan) ||
@@ -362,13 +349,21 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
   children = __shfl_sync(FULL, children, 0);
   if (!split) return;
   const uint32_t npp = ceil_div(nd.n, PART_PIECE);
-  uint32_t sidx = 0, pbase = 0, sbase = 0, ok = 1;
+  const bool big = nd.n > SMALL_SEG;
+  const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
+  uint32_t sidx = 0, pbase = 0, tbase = 0, gidx = 0, ok = 1;
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
+    atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
-    if (npp > 1) sbase = atomicAdd(&s.ctr->n_status, npp);
-    if (sidx >= s.cap_nodes || pbase + (uint64_t)npp > s.cap_part ||
-        (npp > 1 && sbase + (uint64_t)npp > s.cap_status)) {
+    if (big) {
+      gidx = atomicAdd(&s.ctr->n_big_segs, 1u);
+      tbase = atomicAdd(&s.ctr->n_tiles, ntiles);
+    } else {
+      gidx = atomicAdd(&s.ctr->n_small_segs, 1u);
+    }
+    if (sidx >= s.cap_nodes || gidx >= s.cap_nodes || pbase + (uint64_t)npp > s.cap_part ||
+        (big && tbase + (uint64_t)ntiles > s.cap_status)) {
       atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
       ok = 0;
     } else {
@@ -378,21 +373,41 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       sr.pos = r.pos;
       sr.children = children;
       s.splits[sidx] = sr;
+      PartSeg sg;
+      sg.in = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+      sg.out = list_ptr<IdxT>(v, nd.buf ^ 1u, nd.slot, 0) + nd.start;
+      sg.mark = v.mark + (size_t)nd.slot * v.n_rows;
+      sg.in_fstride = v.stride;
+      sg.out_fstride = v.stride;
+      sg.n = nd.n;
+      sg.nl = r.pos + 1;
+      sg.keep_right = 1;
+      sg.status = tbase;
+      (big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
   ok = __shfl_sync(FULL, ok, 0);
   if (!ok) return;
   sidx = __shfl_sync(FULL, sidx, 0);
   pbase = __shfl_sync(FULL, pbase, 0);
-  sbase = __shfl_sync(FULL, sbase, 0);
+  tbase = __shfl_sync(FULL, tbase, 0);
+  gidx = __shfl_sync(FULL, gidx, 0);
   for (uint32_t c = lane; c < v.n_classes; c += 32) s.split_left[(size_t)sidx * v.n_classes + c] = 0;
   for (uint32_t j = lane; j < npp; j += 32) {
     PartPiece pp;
     pp.split = sidx;
     pp.j = j;
     pp.npieces = npp;
-    pp.status = sbase + j;
+    pp.status = 0;
     s.part[pbase + j] = pp;
+  }
+  for (uint32_t j = lane; j < ntiles; j += 32) {
+    PartTile tl;
+    tl.seg = gidx;
+    tl.j = j;
+    tl.ntiles = ntiles;
+    tl.pad = 0;
+    s.tiles[tbase + j] = tl;
   }
 }
 
@@ -431,93 +446,6 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
   uint32_t* out = s.split_left + (size_t)pp.split * C;
   for (uint32_t c = lane; c < C; c += 32)
     if (cnt[c]) atomicAdd(&out[c], cnt[c]);
-}
-
-// ------------------------------------------------------------------------
-template <typename IdxT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_partition(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
-  const uint32_t lane = lane_id();
-  uint32_t ticket = 0;
-  if (lane == 0) ticket = atomicAdd(&s.ctr->ticket, 1u);
-  ticket = __shfl_sync(FULL, ticket, 0);
-  const uint32_t npp = live_count(s, s.ctr->n_part_pieces, s.cap_part);
-  if ((uint64_t)ticket >= (uint64_t)npp * v.n_features) return;
-  const uint32_t f = ticket / npp;
-  const uint32_t pi = ticket - f * npp;
-  const PartPiece pp = s.part[pi];
-  const SplitRec sr = s.splits[pp.split];
-  const ct_node nd = nodes[sr.node];
-  const IdxT* in = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
-  IdxT* out = list_ptr<IdxT>(v, nd.buf ^ 1u, nd.slot, f) + nd.start;
-  const uint8_t* mk = v.mark + (size_t)nd.slot * v.n_rows;
-  const uint32_t n = nd.n;
-  const uint32_t nl = sr.pos + 1;
-  const uint32_t lo = pp.j * PART_PIECE;
-
-  uint32_t rows[PART_ROUNDS];
-  unsigned lmask[PART_ROUNDS];
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    const uint32_t p = lo + r * 32 + lane;
-    rows[r] = p < n ? (uint32_t)in[p] : 0u;
-  }
-  uint32_t local = 0;
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    const uint32_t p = lo + r * 32 + lane;
-    const bool left = p < n && mk[rows[r]] != 0;
-    lmask[r] = __ballot_sync(FULL, left);
-    local += __popc(lmask[r]);
-  }
-
-  uint32_t carry = 0;
-  if (pp.npieces > 1) {
-    uint64_t* col = s.status + (size_t)f * s.cap_status + (pp.status - pp.j);
-    if (lane == 0) {
-      if (pp.j == 0) {
-        publish(col, ST_INC | local);
-      } else {
-        publish(col + pp.j, ST_AGG | local);
-        uint64_t acc = 0;
-        uint32_t k = pp.j - 1;
-        uint32_t spins = 0;
-        while (true) {
-          const uint64_t word = poll(col + k);
-          const uint64_t flag = word & ST_FLAG;
-          if (flag == 0) {
-            if (++spins > SPIN_LIMIT || read_error(s.ctr) != 0) {
-              atomicOr(&s.ctr->error, DEV_ERR_TIMEOUT);
-              acc = 0;
-              break;
-            }
-            __nanosleep(64);
-            continue;
-          }
-          acc += word & ST_VAL;
-          if (flag == ST_INC || k == 0) break;
-          --k;
-        }
-        carry = (uint32_t)acc;
-        publish(col + pp.j, ST_INC | (uint64_t)(carry + local));
-      }
-    }
-    carry = __shfl_sync(FULL, carry, 0);
-  }
-
-  uint32_t run = carry;
-  const unsigned lt = lanemask_lt();
-#pragma unroll
-  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-    const uint32_t p = lo + r * 32 + lane;
-    if (p < n) {
-      const bool left = (lmask[r] >> lane) & 1u;
-      const uint32_t rl = run + __popc(lmask[r] & lt);
-      const uint32_t dst = left ? rl : nl + (p - rl);
-      if (dst < n) out[dst] = (IdxT)rows[r];
-    }
-    run += __popc(lmask[r]);
-  }
 }
 
 // ------------------------------------------------------------------------
@@ -595,6 +523,9 @@ __global__ void k_reset_step(Counters* c, uint32_t n_nodes) {
   c->n_part_pieces = 0;
   c->n_status = 0;
   c->ticket = 0;
+  c->n_small_segs = 0;
+  c->n_big_segs = 0;
+  c->n_tiles = 0;
 }
 
 inline uint32_t blocks_for_warps(uint64_t warps) {
@@ -607,26 +538,44 @@ inline uint32_t clamp32(uint64_t x) { return x > 0xffffffffull ? 0xffffffffu : (
 template <typename IdxT, typename LabT>
 void split_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const LevelScratch& s,
                 const LevelCaps& caps, uint32_t scan_piece, cudaStream_t st) {
+  Prof* pf = current_prof();
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
+  pf->begin(CT_K_SELECT);
   k_select<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, scan_piece);
-  if (caps.carry > 0) {
-    k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
-                                                                                         scan_piece);
-    k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
-  }
+  pf->end();
+  pf->launched(CT_K_SELECT);
+  pf->begin(CT_K_SCAN);
+  k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
+                                                                                       scan_piece);
+  k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
   k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 2 * sm1, st>>>(
       v, nodes, tot, s, scan_piece);
+  pf->end();
+  pf->launched(CT_K_SCAN, 3);
+  pf->begin(CT_K_REDUCE);
   k_split_reduce<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s);
+  pf->end();
+  pf->launched(CT_K_REDUCE);
 }
 
 template <typename IdxT, typename LabT>
-void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s, const LevelCaps& caps,
+void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s_all, const LevelCaps& caps,
                     const TreeView& tv, cudaStream_t st) {
+  Prof* pf = current_prof();
+  // tile/status capacity of this step: its status words are zeroed, its stride is the column stride
+  LevelScratch s = s_all;
+  s.cap_status = caps.status;
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
+  pf->begin(CT_K_MARK);
   k_plan<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, tv);
   k_fill_mark<IdxT, LabT><<<blocks_for_warps(caps.part), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s);
-  k_partition<IdxT><<<blocks_for_warps((uint64_t)caps.part * v.n_features), THREADS_PER_BLOCK, 0, st>>>(
-      v, nodes, s);
+  pf->end();
+  pf->launched(CT_K_MARK, 2);
+  pf->begin(CT_K_PARTITION);
+  const PartWork w = level_part_work(v, s);
+  launch_seg_partition(sizeof(IdxT), w, caps.nodes, caps.status, st);
+  pf->end();
+  pf->launched(CT_K_PARTITION, 2);
 }
 
 template <typename IdxT, typename LabT>
@@ -634,8 +583,12 @@ void children_impl(const View& v, const ct_node* nodes, const uint32_t* tot, con
                    const LevelCaps& caps, const TreeView& tv, ct_node* next, uint32_t* next_tot,
                    uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small,
                    cudaStream_t st) {
+  Prof* pf = current_prof();
+  pf->begin(CT_K_CHILDREN);
   k_children<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(
       v, nodes, tot, s, tv, next, next_tot, cap_next, small_cut, small, cap_small);
+  pf->end();
+  pf->launched(CT_K_CHILDREN);
 }
 
 }  // namespace
@@ -648,7 +601,7 @@ LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b) {
   c.scan = clamp32(m * (b.samples / scan_piece + b.nodes) + 1);
   c.carry = clamp32(m * (2 * b.samples / scan_piece) + 1);
   c.part = clamp32(b.samples / PART_PIECE + b.nodes + 1);
-  c.status = clamp32(2 * b.samples / PART_PIECE + 1);
+  c.status = clamp32(b.samples / TILE_ELEMS + b.samples / (SMALL_SEG + 1) + 1);  // tiles of big splits
   return c;
 }
 
@@ -672,6 +625,9 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.splits = a.take<SplitRec>(c.nodes);
   t.split_left = a.take<uint32_t>((size_t)c.nodes * C);
   t.part = a.take<PartPiece>(c.part);
+  t.small_segs = a.take<PartSeg>(c.nodes);
+  t.big_segs = a.take<PartSeg>(c.nodes);
+  t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   if (s) *s = t;
   return a.used;
@@ -712,7 +668,7 @@ int launch_partition(const View& v, uint32_t ib, uint32_t lb, const ct_node* nod
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
   caps.part = min(caps.part, s.cap_part);
   caps.status = min(caps.status, s.cap_status);
-  CT_CUDA_TRY(cudaMemsetAsync(s.status, 0, (size_t)s.cap_status * v.n_features * sizeof(uint64_t), st));
+  CT_CUDA_TRY(cudaMemsetAsync(s.status, 0, (size_t)caps.status * v.n_features * sizeof(uint64_t), st));
 #define CALL(I, L) partition_impl<I, L>(v, nodes, s, caps, tv, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
@@ -735,8 +691,33 @@ int launch_children(const View& v, uint32_t ib, uint32_t lb, const ct_node* node
 
 int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st) {
   k_reset_step<<<1, 1, 0, st>>>(ctr, n_nodes);
+  current_prof()->launched(CT_K_CHILDREN);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
+}
+
+PartWork level_part_work(const View& v, const LevelScratch& s) {
+  PartWork w;
+  w.small = s.small_segs;
+  w.n_small = &s.ctr->n_small_segs;
+  w.cap_small = s.cap_nodes;
+  w.big = s.big_segs;
+  w.n_big = &s.ctr->n_big_segs;
+  w.cap_big = s.cap_nodes;
+  w.tiles = s.tiles;
+  w.n_tiles = &s.ctr->n_tiles;
+  w.cap_tiles = s.cap_status;
+  w.status = s.status;
+  w.cap_status = s.cap_status;
+  w.ticket = &s.ctr->ticket;
+  w.error = &s.ctr->error;
+  w.n_features = v.n_features;
+  return w;
+}
+
+Prof* current_prof() {
+  static thread_local Prof prof;
+  return &prof;
 }
 
 View make_view(const ct_problem* p, const ct_lists* l) {

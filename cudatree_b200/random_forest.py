@@ -132,6 +132,8 @@ class RandomForestClassifier:
         self._trees = []
         self._packed = None
         self.last_fit_timing = {}
+        self.last_fit_stats = None
+        self.profile = False  # record CUDA-event time per kernel group
 
     # ------------------------------------------------------------ pickling
     def _params(self):
@@ -146,8 +148,9 @@ class RandomForestClassifier:
     # ------------------------------------------------------------- fitting
     def fit_init(self, samples, target):
         """Validate, compact labels, upload and presort (random_forest.py:215-266)."""
-        x = np.asarray(samples)
-        y = np.asarray(target)
+        x_src = samples if isinstance(samples, torch.Tensor) else None
+        x = samples.numpy() if isinstance(samples, torch.Tensor) else np.asarray(samples)
+        y = target.numpy() if isinstance(target, torch.Tensor) else np.asarray(target)
         if x.ndim != 2:
             raise ValueError("samples must be a 2-D array [n_samples, n_features]")
         if y.ndim != 1 or y.shape[0] != x.shape[0]:
@@ -179,7 +182,10 @@ class RandomForestClassifier:
         self._seed = int(np.random.randint(0, 2**62)) if self.seed is None else int(self.seed)
         dev = _device()
         t0 = time.perf_counter()
-        xd = torch.from_numpy(x32).to(dev)
+        if x_src is not None and x_src.dtype == torch.float32 and x_src.is_contiguous():
+            xd = x_src.to(dev, non_blocking=True)  # pinned host tensors copy asynchronously
+        else:
+            xd = torch.from_numpy(x32).to(dev)
         self._x_fm = xd.t().contiguous()
         self._labels = _to_dev(y_c.astype(self.dtype_labels), dev)
         self._presort = _dev_bytes(self.n_features * self.n_samples * self.index_bytes, dev)
@@ -240,17 +246,28 @@ class RandomForestClassifier:
         tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
                               _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
         opts = _lib.FitOptions(mode_id, int(bfs_threshold), 0, 0)
+        opts.reserved[0] = 1 if self.profile else 0
         ws = C.c_size_t()
         _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))
         work = _dev_bytes(ws.value, dev)
         trees = []
+        stats = None
         for t0 in range(first, first + count, per_call):
             kk = min(per_call, first + count - t0)
             _lib.call("ct_fit", C.byref(prob), C.byref(lists), t0, kk, C.byref(opts), C.byref(tb),
                       _ptr(work), ws.value, _stream())
+            st = _lib.fit_stats()
+            if stats is None:
+                stats = st
+            else:
+                for key in ("launches", "ms", "bytes"):
+                    stats[key] = [a + b for a, b in zip(stats[key], st[key])]
+                stats["steps"] += st["steps"]
+                stats["total_launches"] += st["total_launches"]
             counts = n_nodes[:kk].cpu().numpy().astype(np.int64)
             for s in range(kk):
                 trees.append(self._canonical_tree(raw, s * cap, int(counts[s])))
+        self.last_fit_stats = stats
         return trees
 
     def _canonical_tree(self, raw, off, n_nodes):

@@ -167,6 +167,24 @@ int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint
            const ct_fit_options* opt, const ct_tree_buffers* trees, void* workspace,
            size_t workspace_bytes, void* stream);
 
+/* Per-kernel-group statistics of the last ct_fit on the calling thread.
+ * Launch counts and algorithmic bytes are always recorded; ms[] is filled
+ * when ct_fit_options.reserved[0] has bit 0 set (CUDA events recorded on
+ * the fit's stream around each kernel group). */
+enum {
+  CT_K_SELECT = 0, CT_K_SCAN = 1, CT_K_REDUCE = 2, CT_K_MARK = 3,
+  CT_K_PARTITION = 4, CT_K_CHILDREN = 5, CT_K_BOOTSTRAP = 6, CT_K_SUBTREE = 7,
+  CT_NUM_KERNEL_GROUPS = 8
+};
+typedef struct ct_kernel_stats {
+  uint64_t launches[8];  /* kernel launches per group                      */
+  double ms[8];          /* summed event time per group (profiling on)      */
+  double bytes[8];       /* algorithmic bytes per group                    */
+  uint64_t steps;        /* level steps (node batches) run                 */
+  uint64_t total_launches;
+} ct_kernel_stats;
+int ct_fit_stats(ct_kernel_stats* out);
+
 /* Host-side: renumber one raw tree (host arrays) into breadth-first order,
  * left child before right.  Output arrays hold n_nodes entries. */
 int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature,
