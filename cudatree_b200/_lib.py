@@ -107,6 +107,8 @@ PROTOTYPES = {
                                           C.POINTER(C.c_size_t)]),
     "ct_split_nodes": (C.c_int, [C.POINTER(Problem), C.POINTER(Lists), P, P, C.c_uint32, P, P, P,
                                  C.c_size_t, P]),
+    "ct_split_nodes_noalloc": (C.c_int, [C.POINTER(Problem), C.POINTER(Lists), P, P, C.c_uint32, C.c_uint64,
+                                         P, P]),
     "ct_partition_workspace_size": (C.c_int, [C.POINTER(Problem), C.c_uint32, C.c_uint64,
                                               C.POINTER(C.c_size_t)]),
     "ct_partition_nodes": (C.c_int, [C.POINTER(Problem), C.POINTER(Lists), P, P, C.c_uint32, P,

@@ -28,6 +28,7 @@ SOURCES = [
     "ct_predict.cu",
     "ct_presort.cu",
     "ct_partition.cu",
+    "ct_noalloc.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

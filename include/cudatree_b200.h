@@ -148,6 +148,20 @@ int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* no
                    const uint32_t* totals, uint32_t n_nodes, ct_split_result* out,
                    uint32_t* selected, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free variant of ct_split_nodes; no counterpart in the
+ * reference.  For callers that cannot allocate device memory (a process
+ * whose device memory is held by another allocator's pool, a latency-bound
+ * loop that must not call cudaMalloc/cudaFree, a C FFI host without device
+ * buffers of its own): the scratch is a static 16 MiB array per device
+ * instead of a caller workspace.  total_samples must be >= the sum of the
+ * nodes' n; batches whose scratch exceeds 16 MiB are rejected with
+ * CT_ERR_ARG.  The first call on a device looks up the array's device
+ * address and should come before any stream capture; calls that overlap on
+ * the same device race on the shared array and must be serialized. */
+int ct_split_nodes_noalloc(const ct_problem* p, const ct_lists* lists, const ct_node* nodes,
+                           const uint32_t* totals, uint32_t n_nodes, uint64_t total_samples,
+                           ct_split_result* out, void* stream);
+
 /* Mark table + stable partition of every feature's node range into the
  * other buffer for each node whose split has a feature (replaces fill_table +
  * scan_reshuffle, dfs_module.cu:210-307, bfs_module.cu:238-377). */
