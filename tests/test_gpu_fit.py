@@ -71,3 +71,21 @@ def test_memorize(cuda_device, name):
     forest = RandomForestClassifier(n_estimators=6, bootstrap=False, seed=3)
     forest.fit(x, y)
     assert int((forest.predict(x) != y).sum()) == 0
+
+
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+def test_golden_forests(cuda_device, mode):
+    """Committed canonical forests (tests/golden/oracle_forests.npz) node for node."""
+    from pathlib import Path
+    from tests.golden.make_golden import FOREST_CASES
+    g = np.load(Path(__file__).resolve().parent / "golden" / "oracle_forests.npz")
+    for name, (make, t, bs, m, seed) in FOREST_CASES.items():
+        x, y = make()
+        forest = RandomForestClassifier(n_estimators=t, bootstrap=bs, max_features=m, seed=seed, fit_mode=mode)
+        forest.fit(x, y)
+        for i, tr in enumerate(forest._trees):
+            np.testing.assert_array_equal(tr.left_children, g[f"{name}/{i}/left"])
+            np.testing.assert_array_equal(tr.right_children, g[f"{name}/{i}/right"])
+            np.testing.assert_array_equal(tr.feature_idx_array, g[f"{name}/{i}/feature"])
+            np.testing.assert_array_equal(tr.feature_threshold_array, g[f"{name}/{i}/threshold"])
+            np.testing.assert_array_equal(tr.values_array.astype(np.int64), g[f"{name}/{i}/value"])
