@@ -25,6 +25,8 @@ namespace ct {
 
 namespace {
 
+constexpr uint32_t SCAN_BATCH = 4;  // rounds of 32 whose loads are issued together
+
 __device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
 __device__ __forceinline__ uint32_t global_warp() {
@@ -135,13 +137,22 @@ k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t 
   __syncwarp();
   const uint32_t lo = pc.j * scan_piece;
   const uint32_t hi = min(lo + scan_piece, nd.n);
-  for (uint32_t base = lo; base < hi; base += 32) {
-    const uint32_t p = base + lane;
-    const bool valid = p < hi;
-    const uint32_t c = valid ? label_of<LabT>(v, lst[p]) : NONE;
-    const unsigned grp = __match_any_sync(FULL, c);
-    if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
-    __syncwarp();
+  for (uint32_t base = lo; base < hi; base += 32 * SCAN_BATCH) {
+    uint32_t rows[SCAN_BATCH], cs[SCAN_BATCH];
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const uint32_t p = base + r * 32 + lane;
+      rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r)
+      cs[r] = (base + r * 32 + lane < hi) ? label_of<LabT>(v, rows[r]) : NONE;
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const unsigned grp = __match_any_sync(FULL, cs[r]);
+      if (cs[r] != NONE && (grp >> lane) == 1u) cnt[cs[r]] += __popc(grp);
+      __syncwarp();
+    }
   }
   uint32_t* out = s.carry + (size_t)pc.carry * C;
   for (uint32_t c = lane; c < C; c += 32) out[c] = cnt[c];
@@ -203,47 +214,65 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   double best = dinf();
   uint32_t bpos = NONE;
   float bil = 0.f, bir = 0.f;
-  for (uint32_t base = lo; base < hi; base += 32) {
-    const uint32_t p = base + lane;
-    const bool valid = p < hi;
-    uint32_t c = NONE;
-    float x = 0.f;
-    if (valid) {
-      const uint32_t row = lst[p];
-      c = label_of<LabT>(v, row);
-      x = xf[row];
+  const unsigned lt = lanemask_lt();
+  for (uint32_t base = lo; base < hi; base += 32 * SCAN_BATCH) {
+    // loads of the whole batch first: index, then label and value
+    uint32_t rows[SCAN_BATCH], cs[SCAN_BATCH];
+    float xs[SCAN_BATCH];
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const uint32_t p = base + r * 32 + lane;
+      rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
     }
-    float xn = __shfl_down_sync(FULL, x, 1);
-    if (valid && (lane == 31 || p + 1 == hi) && p + 1 < n) xn = xf[lst[p + 1]];
-    const unsigned grp = __match_any_sync(FULL, c);
-    uint32_t k = 0;
-    int64_t tc = 0;
-    if (valid) {
-      k = cnt[c] + __popc(grp & lanemask_lt());
-      tc = T[c];
+    const uint32_t pe = base + 32 * SCAN_BATCH;  // first position after the batch
+    const uint32_t row_e = (lane == 31 && pe < hi) ? (uint32_t)lst[pe] : 0u;
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const bool valid = base + r * 32 + lane < hi;
+      cs[r] = valid ? label_of<LabT>(v, rows[r]) : NONE;
+      xs[r] = valid ? xf[rows[r]] : 0.f;
     }
-    __syncwarp();
-    if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
-    __syncwarp();
-    const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
-    const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
-    const int64_t il = warp_incl_scan_i64(dl);
-    const int64_t ir = warp_incl_scan_i64(dr);
-    const int64_t SL = sl + il;
-    const int64_t SR = sr + ir;
-    sl += __shfl_sync(FULL, il, 31);
-    sr += __shfl_sync(FULL, ir, 31);
-    if (valid && p + 1 < n && is_candidate(x, xn)) {
-      const double nl = (double)(p + 1);
-      const double nr = __dsub_rn(nn, nl);
-      const double gl = gini_part(SL, nl, nn);
-      const double gr = gini_part(SR, nr, nn);
-      const double sc = __dadd_rn(gl, gr);
-      if (sc < best) {
-        best = sc;
-        bpos = p;
-        bil = __double2float_rn(gl);
-        bir = __double2float_rn(gr);
+    const float x_e = (lane == 31 && pe < hi) ? xf[row_e] : 0.f;
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const uint32_t p = base + r * 32 + lane;
+      const bool valid = p < hi;
+      const uint32_t c = cs[r];
+      const float x = xs[r];
+      float xn = __shfl_down_sync(FULL, x, 1);
+      const float first_next = (r + 1 < SCAN_BATCH) ? __shfl_sync(FULL, xs[r + 1 < SCAN_BATCH ? r + 1 : r], 0) : x_e;
+      if (lane == 31) xn = first_next;
+      if (valid && p + 1 == hi && p + 1 < n) xn = xf[lst[p + 1]];  // next piece's first element
+      const unsigned grp = __match_any_sync(FULL, c);
+      uint32_t k = 0;
+      int64_t tc = 0;
+      if (valid) {
+        k = cnt[c] + __popc(grp & lt);
+        tc = T[c];
+      }
+      __syncwarp();
+      if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
+      __syncwarp();
+      const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
+      const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
+      const int64_t il = warp_incl_scan_i64(dl);
+      const int64_t ir = warp_incl_scan_i64(dr);
+      const int64_t SL = sl + il;
+      const int64_t SR = sr + ir;
+      sl += __shfl_sync(FULL, il, 31);
+      sr += __shfl_sync(FULL, ir, 31);
+      if (valid && p + 1 < n && is_candidate(x, xn)) {
+        const double nl = (double)(p + 1);
+        const double nr = __dsub_rn(nn, nl);
+        const double gl = gini_part(SL, nl, nn);
+        const double gr = gini_part(SR, nr, nn);
+        const double sc = __dadd_rn(gl, gr);
+        if (sc < best) {
+          best = sc;
+          bpos = p;
+          bil = __double2float_rn(gl);
+          bir = __double2float_rn(gr);
+        }
       }
     }
   }

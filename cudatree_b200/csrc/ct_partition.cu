@@ -176,41 +176,159 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
   }
 }
 
+// ---- TMA bulk copies (cp.async.bulk, 1-D) with mbarrier completion --------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+// Global -> shared bulk copy; src 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// One claimed (tile, feature) work item of k_part_big.
+struct TileJob {
+  const void* src16;      // 16-byte aligned start of the copied range
+  void* out;              // feature f's output base of the segment
+  const uint8_t* mark;
+  uint64_t* col;          // status column of (segment, feature)
+  uint32_t bytes;         // copied bytes (multiple of 16)
+  uint32_t off;           // element offset of the tile inside the copied range
+  uint32_t lo;            // first segment position of the tile
+  uint32_t cnt;           // elements in the tile
+  uint32_t n, nl, j, ntiles, keep_right, valid;
+};
+
 template <typename IdxT>
-__global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
-  __shared__ uint32_t s_ticket, s_carry;
+__device__ __forceinline__ void claim_tile(const PartWork& w, uint32_t ntiles, uint64_t tasks, TileJob* jb) {
+  const uint32_t t = atomicAdd(w.ticket, 1u);
+  if ((uint64_t)t >= tasks) {
+    jb->valid = 0;
+    return;
+  }
+  // tile-major: the predecessor (k-1, f) of a tile was issued n_features
+  // tickets earlier, so its status is usually published by the time we look
+  const uint32_t k = t / w.n_features;
+  const uint32_t f = t - k * w.n_features;
+  const PartTile tl = w.tiles[k];
+  const PartSeg sg = w.big[tl.seg];
+  const uint32_t lo = tl.j * TILE_ELEMS;
+  const uint32_t cnt = min(TILE_ELEMS, sg.n - lo);
+  const IdxT* src = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride + lo;
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uintptr_t a0 = a & ~uintptr_t(15);
+  const uintptr_t e1 = (a + (uintptr_t)cnt * sizeof(IdxT) + 15) & ~uintptr_t(15);
+  jb->src16 = reinterpret_cast<const void*>(a0);
+  jb->bytes = (uint32_t)(e1 - a0);
+  jb->off = (uint32_t)((a - a0) / sizeof(IdxT));
+  jb->out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
+  jb->mark = sg.mark;
+  jb->col = w.status + (size_t)f * w.cap_status + sg.status;
+  jb->lo = lo;
+  jb->cnt = cnt;
+  jb->n = sg.n;
+  jb->nl = sg.nl;
+  jb->j = tl.j;
+  jb->ntiles = tl.ntiles;
+  jb->keep_right = sg.keep_right;
+  jb->valid = 1;
+}
+
+// Persistent CTAs; the index tile of the next ticket is brought into shared
+// memory by a TMA bulk copy while the current tile gathers its marks, looks
+// back for its carry and stores.  Copies read up to 15 bytes past a tile's
+// last element (16-byte rounding); list buffers carry that padding.
+template <typename IdxT>
+__global__ void __launch_bounds__(BIG_THREADS) k_part_big(PartWork w) {
+  constexpr uint32_t BUF = TILE_ELEMS * sizeof(IdxT) + 32;
+  __shared__ alignas(128) unsigned char sbuf[2][BUF];
+  __shared__ alignas(8) uint64_t bars[2];
+  __shared__ TileJob jobs[2];
+  __shared__ uint32_t s_carry;
   __shared__ uint32_t s_wcnt[BIG_WARPS], s_woff[BIG_WARPS];
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
   const uint32_t ntiles = live(w, w.n_tiles, w.cap_tiles);
   const uint64_t tasks = (uint64_t)ntiles * w.n_features;
-  while (true) {
-    if (threadIdx.x == 0) s_ticket = atomicAdd(w.ticket, 1u);
-    __syncthreads();
-    const uint32_t t = s_ticket;
-    if ((uint64_t)t >= tasks) break;
-    // tile-major: the predecessor (k-1, f) of a tile was issued n_features
-    // tickets earlier, so its status is usually published by the time we look
-    const uint32_t k = t / w.n_features;
-    const uint32_t f = t - k * w.n_features;
-    const PartTile tl = w.tiles[k];
-    const PartSeg sg = w.big[tl.seg];
-    const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
-    IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
-    const uint32_t n = sg.n;
-    const uint32_t lo = tl.j * TILE_ELEMS + warp * (32 * PART_ROUNDS);
-    uint32_t rows[PART_ROUNDS];
-    unsigned lmask[PART_ROUNDS];
-#pragma unroll
-    for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-      const uint32_t p = lo + r * 32 + lane;
-      rows[r] = p < n ? (uint32_t)in[p] : 0u;
+  if (threadIdx.x == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+    claim_tile<IdxT>(w, ntiles, tasks, &jobs[0]);
+    if (jobs[0].valid) {
+      mbar_expect_tx(&bars[0], jobs[0].bytes);
+      bulk_g2s(sbuf[0], jobs[0].src16, jobs[0].bytes, &bars[0]);
     }
+  }
+  __syncthreads();
+  uint32_t phase[2] = {0u, 0u};
+  for (uint32_t it = 0;; ++it) {
+    const uint32_t b = it & 1u;
+    if (!jobs[b].valid) break;
+    if (threadIdx.x == 0) {  // prefetch the next work item into the other buffer
+      claim_tile<IdxT>(w, ntiles, tasks, &jobs[b ^ 1u]);
+      if (jobs[b ^ 1u].valid) {
+        mbar_expect_tx(&bars[b ^ 1u], jobs[b ^ 1u].bytes);
+        bulk_g2s(sbuf[b ^ 1u], jobs[b ^ 1u].src16, jobs[b ^ 1u].bytes, &bars[b ^ 1u]);
+      }
+    }
+    // wait for this tile's indices (bounded; a copy of at most 16 KiB)
+    bool ok = true;
+    {
+      uint32_t spins = 0;
+      while (!mbar_try_wait(&bars[b], phase[b])) {
+        if (++spins > (SPIN_LIMIT << 2)) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    if (!__syncthreads_and(ok)) {
+      // never read a tile that did not arrive: flag, drain both buffers' copies (bounded), leave
+      if (threadIdx.x == 0) atomicOr(w.error, DEV_ERR_TIMEOUT);
+      uint32_t spins = 0;
+      while (!mbar_try_wait(&bars[b], phase[b]) && ++spins < (SPIN_LIMIT << 4)) {
+      }
+      if (jobs[b ^ 1u].valid) {
+        spins = 0;
+        while (!mbar_try_wait(&bars[b ^ 1u], phase[b ^ 1u]) && ++spins < (SPIN_LIMIT << 4)) {
+        }
+      }
+      return;
+    }
+    phase[b] ^= 1u;
+    const TileJob jb = jobs[b];
+    const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + jb.off;
+    const uint32_t wlo = warp * (32 * PART_ROUNDS);
+    unsigned lmask[PART_ROUNDS];
     uint32_t cnt = 0;
 #pragma unroll
     for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-      const uint32_t p = lo + r * 32 + lane;
-      lmask[r] = __ballot_sync(FULL, p < n && sg.mark[rows[r]] != 0);
+      const uint32_t q = wlo + r * 32 + lane;
+      const bool left = q < jb.cnt && jb.mark[(uint32_t)rows[q < jb.cnt ? q : 0]] != 0;
+      lmask[r] = __ballot_sync(FULL, left);
       cnt += __popc(lmask[r]);
     }
     if (lane == 0) s_wcnt[warp] = cnt;
@@ -219,35 +337,36 @@ __global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
       const uint32_t c = lane < BIG_WARPS ? s_wcnt[lane] : 0u;
       uint32_t inc = c;
 #pragma unroll
-      for (int s = 1; s < BIG_WARPS; s <<= 1) {
-        const uint32_t o = __shfl_up_sync(FULL, inc, s);
-        if (lane >= (uint32_t)s) inc += o;
+      for (int sft = 1; sft < BIG_WARPS; sft <<= 1) {
+        const uint32_t o = __shfl_up_sync(FULL, inc, sft);
+        if (lane >= (uint32_t)sft) inc += o;
       }
       if (lane < BIG_WARPS) s_woff[lane] = inc - c;
       const uint32_t total = __shfl_sync(FULL, inc, BIG_WARPS - 1);
       uint32_t carry = 0;
-      if (tl.ntiles > 1) {
-        uint64_t* col = w.status + (size_t)f * w.cap_status + sg.status;
-        if (tl.j == 0) {
-          if (lane == 0) publish(col, ST_INC | total);
+      if (jb.ntiles > 1) {
+        if (jb.j == 0) {
+          if (lane == 0) publish(jb.col, ST_INC | total);
         } else {
-          if (lane == 0) publish(col + tl.j, ST_AGG | total);
-          carry = window_lookback(col, tl.j, w.error);
-          if (lane == 0) publish(col + tl.j, ST_INC | (uint64_t)(carry + total));
+          if (lane == 0) publish(jb.col + jb.j, ST_AGG | total);
+          carry = window_lookback(jb.col, jb.j, w.error);
+          if (lane == 0) publish(jb.col + jb.j, ST_INC | (uint64_t)(carry + total));
         }
       }
       if (lane == 0) s_carry = carry;
     }
     __syncthreads();
     uint32_t run = s_carry + s_woff[warp];
+    IdxT* out = reinterpret_cast<IdxT*>(jb.out);
 #pragma unroll
     for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-      const uint32_t p = lo + r * 32 + lane;
+      const uint32_t q = wlo + r * 32 + lane;
       const bool left = (lmask[r] >> lane) & 1u;
       const uint32_t rl = run + __popc(lmask[r] & lt);
-      if (p < n && (left || sg.keep_right)) {
-        const uint32_t dst = left ? rl : sg.nl + (p - rl);
-        if (dst < n) out[dst] = (IdxT)rows[r];
+      if (q < jb.cnt && (left || jb.keep_right)) {
+        const uint32_t p = jb.lo + q;
+        const uint32_t dst = left ? rl : jb.nl + (p - rl);
+        if (dst < jb.n) out[dst] = rows[q];
       }
       run += __popc(lmask[r]);
     }

@@ -55,8 +55,11 @@ def _device() -> torch.device:
     return torch.device("cuda", torch.cuda.current_device())
 
 
+PAD_BYTES = 64  # index buffers are read up to 15 bytes past their end by 16-byte bulk copies
+
+
 def _dev_bytes(nbytes: int, dev) -> torch.Tensor:
-    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device=dev)
+    return torch.empty(max(int(nbytes), 1) + PAD_BYTES, dtype=torch.uint8, device=dev)
 
 
 def _to_dev(a: np.ndarray, dev) -> torch.Tensor:

@@ -61,6 +61,10 @@ typedef struct ct_problem {
  * sorted_indices_gpu_, random_tree.py:466-467).  Slot s, buffer b, feature f
  * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark is
  * [n_slots][n_rows] bytes (reference mark_table, random_forest.py:168). */
+/* The partition and compaction kernels copy index tiles with 16-byte TMA
+ * bulk copies and may read up to 15 bytes past the last element of the
+ * si0/si1 buffers and of the presort: allocate them with >= 16 bytes of
+ * readable padding. */
 typedef struct ct_lists {
   void* si0;
   void* si1;

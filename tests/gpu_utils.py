@@ -20,7 +20,8 @@ def to_dev(a: np.ndarray) -> torch.Tensor:
 
 
 def dev_bytes(n: int) -> torch.Tensor:
-    return torch.zeros(max(int(n), 1), dtype=torch.uint8, device=dev())
+    # +64: index buffers are read up to 15 bytes past their end by 16-byte bulk copies
+    return torch.zeros(max(int(n), 1) + 64, dtype=torch.uint8, device=dev())
 
 
 def from_dev(t: torch.Tensor, dtype, shape=None) -> np.ndarray:
@@ -59,7 +60,8 @@ class GpuProblem:
                                  min_samples_split, int(bootstrap), seed)
 
     def presort_np(self) -> np.ndarray:
-        return from_dev(self.presort, self.idx_dtype, (self.f, self.n)).astype(np.int64)
+        nb = self.f * self.n * self.ib
+        return from_dev(self.presort[:nb], self.idx_dtype, (self.f, self.n)).astype(np.int64)
 
 
 class GpuLists:
@@ -74,14 +76,16 @@ class GpuLists:
 
     def get(self, buf: int, slot: int = 0) -> np.ndarray:
         gp = self.gp
-        a = from_dev(self.si[buf], gp.idx_dtype, (self.slots, gp.f, gp.n))
+        nb = self.slots * gp.f * gp.n * gp.ib
+        a = from_dev(self.si[buf][:nb], gp.idx_dtype, (self.slots, gp.f, gp.n))
         return a[slot].astype(np.int64)
 
     def put(self, buf: int, lists: np.ndarray, slot: int = 0) -> None:
         gp = self.gp
-        a = from_dev(self.si[buf], gp.idx_dtype, (self.slots, gp.f, gp.n)).copy()
+        nb = self.slots * gp.f * gp.n * gp.ib
+        a = from_dev(self.si[buf][:nb], gp.idx_dtype, (self.slots, gp.f, gp.n)).copy()
         a[slot] = lists.astype(gp.idx_dtype)
-        self.si[buf].copy_(to_dev(a))
+        self.si[buf][:nb].copy_(to_dev(a))
 
 
 def node_array(nodes: list[dict]) -> np.ndarray:
@@ -105,8 +109,8 @@ def split_nodes(gp: GpuProblem, gl: GpuLists, nodes: np.ndarray, totals: np.ndar
     sel = dev_bytes(nn * gp.prob.max_features * 4)
     _lib.call("ct_split_nodes", C.byref(gp.prob), C.byref(gl.lists), nd.data_ptr(), td.data_ptr(), nn,
               out.data_ptr(), sel.data_ptr(), work.data_ptr(), ws.value, stream())
-    res = from_dev(out, np.dtype(_lib.SPLIT_DTYPE_FIELDS))
-    sel_np = from_dev(sel, np.uint32, (nn, gp.prob.max_features))
+    res = from_dev(out[:nn * 32], np.dtype(_lib.SPLIT_DTYPE_FIELDS))
+    sel_np = from_dev(sel[:nn * gp.prob.max_features * 4], np.uint32, (nn, gp.prob.max_features))
     return res, sel_np, out
 
 

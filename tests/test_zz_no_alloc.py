@@ -35,7 +35,7 @@ def _noalloc(gp, gl, nodes, totals):
     out = G.dev_bytes(nn * 32)
     _lib.call("ct_split_nodes_noalloc", C.byref(gp.prob), C.byref(gl.lists), nd.data_ptr(), td.data_ptr(), nn,
               int(nodes["n"].sum()), out.data_ptr(), G.stream())
-    return G.from_dev(out, np.dtype(_lib.SPLIT_DTYPE_FIELDS))
+    return G.from_dev(out[:nn * 32], np.dtype(_lib.SPLIT_DTYPE_FIELDS))
 
 
 def test_noalloc_matches_workspace_split_twice_in_a_row(cuda_device):
