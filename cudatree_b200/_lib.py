@@ -98,6 +98,7 @@ P = C.c_void_p
 PROTOTYPES = {
     "ct_version": (C.c_char_p, []),
     "ct_last_error": (C.c_int, [C.c_char_p, C.c_size_t]),
+    "ct_mark_bytes": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t)]),
     "ct_presort_workspace_size": (C.c_int, [C.c_uint32, C.c_uint32, C.POINTER(C.c_size_t)]),
     "ct_presort": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, C.c_size_t, P]),
     "ct_bootstrap_workspace_size": (C.c_int, [C.POINTER(Problem), C.POINTER(C.c_size_t)]),
@@ -157,6 +158,12 @@ def check(status: int) -> None:
 
 def call(name: str, *args) -> None:
     check(getattr(load(), name)(*args))
+
+
+def mark_bytes(n_rows: int, n_slots: int) -> int:
+    out = C.c_size_t()
+    call("ct_mark_bytes", n_rows, n_slots, C.byref(out))
+    return out.value
 
 
 def version() -> str:

@@ -54,6 +54,12 @@ int ct_last_error(char* buf, size_t len) {
   return (int)s.size();
 }
 
+int ct_mark_bytes(uint32_t n_rows, uint32_t n_slots, size_t* bytes) {
+  CT_ARG_CHECK(bytes, "bytes is NULL");
+  *bytes = mark_bits_offset(n_rows, n_slots) + (size_t)n_slots * mark_bit_words(n_rows) * sizeof(uint32_t) + 64;
+  return CT_OK;
+}
+
 int ct_presort_workspace_size(uint32_t n_rows, uint32_t n_features, size_t* bytes) {
   CT_ARG_CHECK(bytes, "bytes is NULL");
   *bytes = presort_workspace_bytes(n_rows, n_features);

@@ -39,7 +39,7 @@ __global__ void k_set_u32(uint32_t* p, uint32_t v, uint32_t count) {
 struct BootPlan {
   const void* presort;
   char* si0;              // slot 0 of buffer 0
-  const uint8_t* mark;    // slot 0 mark table
+  const uint32_t* bits;   // slot 0 packed mark table
   PartSeg* segs;
   PartTile* tiles;
   size_t slot_bytes;      // bytes between slots in si0
@@ -54,7 +54,7 @@ __global__ void k_boot_plan(BootPlan b) {
     PartSeg sg;
     sg.in = b.presort;
     sg.out = b.si0 + slot * b.slot_bytes;
-    sg.mark = b.mark + (size_t)slot * b.n_rows;
+    sg.bits = b.bits + (size_t)slot * mark_bit_words(b.n_rows);
     sg.in_fstride = b.n_rows;
     sg.out_fstride = b.stride;
     sg.n = b.n_rows;
@@ -129,7 +129,6 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
   uint8_t* mark = l->mark + (size_t)slot_lo * N;
   CT_CUDA_TRY(cudaMemsetAsync(mark, 0, (size_t)n_slots * N, st));
   CT_CUDA_TRY(cudaMemsetAsync(L.words, 0, sizeof(uint32_t), st));  // ticket (error word kept)
-  CT_CUDA_TRY(cudaMemsetAsync(L.status, 0, (size_t)tiles_per * n_slots * F * sizeof(uint64_t), st));
   CT_CUDA_TRY(cudaMemsetAsync(n_in_dev + slot_lo, 0, n_slots * sizeof(uint32_t), st));
   uint32_t counts[3] = {n_slots, tiles_per * n_slots, 0};
   k_set_u32<<<1, 32, 0, st>>>(L.words + 2, counts[0], 1);
@@ -138,10 +137,13 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
   const dim3 grid(std::min<uint32_t>(ceil_div(N, 256), 1024), n_slots);
   k_boot_mark<<<grid, 256, 0, st>>>(mark, p->seed, tree_lo, N);
   k_count_marks<<<grid, 256, 0, st>>>(mark, N, n_in_dev + slot_lo);
+  uint32_t* bits = reinterpret_cast<uint32_t*>(l->mark + mark_bits_offset(N, l->n_slots)) +
+                   (size_t)slot_lo * mark_bit_words(N);
+  launch_pack_marks(mark, bits, N, n_slots, st);
   BootPlan b;
   b.presort = p->presort;
   b.si0 = dst;
-  b.mark = mark;
+  b.bits = bits;
   b.segs = L.segs;
   b.tiles = L.tiles;
   b.slot_bytes = slot_bytes;

@@ -93,7 +93,7 @@ struct Counters {
 struct PartSeg {
   const void* in;         // element 0 of feature 0
   void* out;
-  const uint8_t* mark;    // per-row left flag of the segment's tree
+  const uint32_t* bits;   // per-row left bit of the segment's tree
   uint32_t in_fstride;    // elements between consecutive features
   uint32_t out_fstride;
   uint32_t n;
@@ -130,7 +130,10 @@ struct View {
   const void* labels;
   void* si0;
   void* si1;
-  uint8_t* mark;
+  uint8_t* mark;          // [n_slots][n_rows] bytes
+  uint32_t* bits;         // [n_slots][bit_words] packed copy of mark
+  uint32_t bit_words;
+  uint32_t n_slots;
   uint32_t stride;
   uint32_t n_rows;
   uint32_t n_features;
@@ -139,6 +142,19 @@ struct View {
   uint32_t mss;
   int feistel_h;
 };
+
+// Packed mark table: bit r of a slot's words is row r's left flag.  The
+// words of one tree (N/8 bytes) fit in an SM's L1, unlike the byte table.
+__host__ __device__ __forceinline__ uint32_t mark_bit_words(uint32_t n_rows) {
+  return ((n_rows + 31) / 32 + 3) & ~3u;
+}
+__host__ __device__ __forceinline__ size_t mark_bits_offset(uint32_t n_rows, uint32_t n_slots) {
+  return ((size_t)n_slots * n_rows + 255) & ~size_t(255);
+}
+__device__ __forceinline__ bool left_bit(const uint32_t* bits, uint32_t row) {
+  return (__ldg(bits + (row >> 5)) >> (row & 31)) & 1u;
+}
+void launch_pack_marks(const uint8_t* mark, uint32_t* bits, uint32_t n_rows, uint32_t n_slots, cudaStream_t st);
 
 template <typename IdxT>
 __device__ __forceinline__ IdxT* list_ptr(const View& v, uint32_t buf, uint32_t slot, uint32_t f) {

@@ -405,7 +405,7 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       PartSeg sg;
       sg.in = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
       sg.out = list_ptr<IdxT>(v, nd.buf ^ 1u, nd.slot, 0) + nd.start;
-      sg.mark = v.mark + (size_t)nd.slot * v.n_rows;
+      sg.bits = v.bits + (size_t)nd.slot * v.bit_words;
       sg.in_fstride = v.stride;
       sg.out_fstride = v.stride;
       sg.n = nd.n;
@@ -598,8 +598,10 @@ void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s_a
   pf->begin(CT_K_MARK);
   k_plan<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, tv);
   k_fill_mark<IdxT, LabT><<<blocks_for_warps(caps.part), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s);
-  pf->end();
   pf->launched(CT_K_MARK, 2);
+  launch_pack_marks(v.mark, v.bits, v.n_rows, v.n_slots, st);
+  pf->launched(CT_K_MARK);
+  pf->end();
   pf->begin(CT_K_PARTITION);
   const PartWork w = level_part_work(v, s);
   launch_seg_partition(sizeof(IdxT), w, caps.nodes, caps.status, st);
@@ -697,7 +699,6 @@ int launch_partition(const View& v, uint32_t ib, uint32_t lb, const ct_node* nod
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
   caps.part = min(caps.part, s.cap_part);
   caps.status = min(caps.status, s.cap_status);
-  CT_CUDA_TRY(cudaMemsetAsync(s.status, 0, (size_t)caps.status * v.n_features * sizeof(uint64_t), st));
 #define CALL(I, L) partition_impl<I, L>(v, nodes, s, caps, tv, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
@@ -756,6 +757,9 @@ View make_view(const ct_problem* p, const ct_lists* l) {
   v.si0 = l ? l->si0 : nullptr;
   v.si1 = l ? l->si1 : nullptr;
   v.mark = l ? l->mark : nullptr;
+  v.n_slots = l ? l->n_slots : 0;
+  v.bit_words = mark_bit_words(p->n_rows);
+  v.bits = l && l->mark ? reinterpret_cast<uint32_t*>(l->mark + mark_bits_offset(p->n_rows, l->n_slots)) : nullptr;
   v.stride = l ? l->stride : 0;
   v.n_rows = p->n_rows;
   v.n_features = p->n_features;

@@ -11,23 +11,19 @@
 //                 features; ranks are popc of a ballot.  For n <= 16 a warp
 //                 packs 32/g features per round in lane groups of width
 //                 g = next_pow2(n), so tiny nodes keep the lanes busy.
-//   k_part_big    n > SMALL_SEG: persistent CTAs take (feature, tile) work
-//                 items of TILE elements from a ticket counter (feature-major,
-//                 so a segment's tiles are consecutive tickets).  Warp counts
-//                 are scanned in shared memory and the tile's carry comes from
-//                 a decoupled look-back over its predecessors' status words,
-//                 read 32 at a time by one warp.  Every wait is bounded: on
-//                 expiry the kernel sets an error bit and returns.
+//   k_part_big    n > SMALL_SEG: persistent CTAs claim whole (segment,
+//                 feature) chains from a ticket counter and stream the chain's
+//                 tiles of TILE elements in order through a ring of shared-
+//                 memory buffers filled by TMA bulk copies; the running left
+//                 count is a register, so no CTA waits for another.  Every
+//                 wait on a copy is bounded: on expiry the kernel sets an
+//                 error bit, drains its copies and returns.
 #include "ct_internal.cuh"
 
 namespace ct {
 
 namespace {
 
-constexpr uint64_t ST_AGG = 1ull << 62;
-constexpr uint64_t ST_INC = 2ull << 62;
-constexpr uint64_t ST_FLAG = 3ull << 62;
-constexpr uint64_t ST_VAL = (1ull << 62) - 1;
 constexpr uint32_t SPIN_LIMIT = 1u << 20;
 constexpr int BIG_WARPS = TILE_ELEMS / (32 * PART_ROUNDS);
 constexpr int BIG_THREADS = BIG_WARPS * 32;
@@ -39,47 +35,6 @@ __device__ __forceinline__ uint32_t read_word(const uint32_t* p) {
 }
 __device__ __forceinline__ uint32_t live(const PartWork& w, const uint32_t* count, uint32_t cap) {
   return read_word(w.error) ? 0u : min(read_word(count), cap);
-}
-__device__ __forceinline__ void publish(uint64_t* p, uint64_t v) {
-  cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_release);
-}
-__device__ __forceinline__ uint64_t poll(uint64_t* p) {
-  return cuda::atomic_ref<uint64_t, cuda::thread_scope_device>(*p).load(cuda::memory_order_acquire);
-}
-__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t v) {
-#pragma unroll
-  for (int s = 16; s > 0; s >>= 1) v += __shfl_xor_sync(FULL, v, s);
-  return v;
-}
-
-// Sum of the counts of tiles [0, j) of one segment column: warp-collective
-// look-back over windows of 32 predecessors.  Returns 0 and flags an error
-// if a predecessor never publishes.
-__device__ uint32_t window_lookback(uint64_t* col, uint32_t j, uint32_t* error) {
-  const uint32_t lane = lane_id();
-  uint64_t acc = 0;
-  int64_t hi = (int64_t)j - 1;
-  uint32_t spins = 0;
-  while (true) {
-    const int64_t k = hi - (int64_t)lane;
-    const uint64_t word = k >= 0 ? poll(col + k) : ST_INC;
-    const uint64_t flag = word & ST_FLAG;
-    const unsigned inc = __ballot_sync(FULL, flag == ST_INC);
-    const unsigned not_ready = __ballot_sync(FULL, flag == 0);
-    const unsigned upto = inc ? (((inc & (0u - inc)) << 1) - 1u) : FULL;
-    if (not_ready & upto) {
-      if (++spins > SPIN_LIMIT || read_word(error) != 0) {
-        if (lane == 0) atomicOr(error, DEV_ERR_TIMEOUT);
-        return 0;
-      }
-      __nanosleep(32);
-      continue;
-    }
-    acc += warp_sum_u64(((upto >> lane) & 1u) ? (word & ST_VAL) : 0ull);
-    if (inc) break;
-    hi -= 32;
-  }
-  return (uint32_t)acc;
 }
 
 // One warp per (segment, block of FEAT_BLOCK features).  Segments of up to
@@ -122,7 +77,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < R; ++r) {
         if (f_lo + r * per >= f_hi) break;
         const uint32_t f = f_lo + r * per + sub;
-        const bool left = valid[r] && sg.mark[rows[r]] != 0;
+        const bool left = valid[r] && left_bit(sg.bits, rows[r]);
         const unsigned lm = __ballot_sync(FULL, left) & gmask;
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (p - rl);
@@ -141,7 +96,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const uint32_t f = f_lo + r;
         if (f >= f_hi) break;
         const bool valid = lane < n;
-        const bool left = valid && sg.mark[rows[r]] != 0;
+        const bool left = valid && left_bit(sg.bits, rows[r]);
         const unsigned lm = __ballot_sync(FULL, left);
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (lane - rl);
@@ -164,7 +119,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
           if (r >= rounds) break;
           const uint32_t p = r * 32 + lane;
           const bool valid = p < n;
-          const bool left = valid && sg.mark[rows[r]] != 0;
+          const bool left = valid && left_bit(sg.bits, rows[r]);
           const unsigned lm = __ballot_sync(FULL, left);
           const uint32_t rl = run + __popc(lm & lt);
           const uint32_t dst = left ? rl : nl + (p - rl);
@@ -208,174 +163,156 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// One claimed (tile, feature) work item of k_part_big.
-struct TileJob {
-  const void* src16;      // 16-byte aligned start of the copied range
-  void* out;              // feature f's output base of the segment
-  const uint8_t* mark;
-  uint64_t* col;          // status column of (segment, feature)
-  uint32_t bytes;         // copied bytes (multiple of 16)
-  uint32_t off;           // element offset of the tile inside the copied range
-  uint32_t lo;            // first segment position of the tile
-  uint32_t cnt;           // elements in the tile
-  uint32_t n, nl, j, ntiles, keep_right, valid;
-};
+// Persistent CTAs; each claims a whole (segment, feature) chain from a
+// ticket counter and streams its tiles in order, so the running count of
+// left rows (the chain's carry) stays in a register and no CTA ever waits
+// for another.  Index tiles arrive by TMA bulk copies into a ring of
+// RING buffers, RING-1 tiles ahead of the one being partitioned.  Copies
+// are 16-byte aligned and rounded, so they read up to 15 bytes past a
+// tile's last element (list buffers carry that padding).
+constexpr uint32_t RING = 3;
 
 template <typename IdxT>
-__device__ __forceinline__ void claim_tile(const PartWork& w, uint32_t ntiles, uint64_t tasks, TileJob* jb) {
-  const uint32_t t = atomicAdd(w.ticket, 1u);
-  if ((uint64_t)t >= tasks) {
-    jb->valid = 0;
-    return;
-  }
-  // tile-major: the predecessor (k-1, f) of a tile was issued n_features
-  // tickets earlier, so its status is usually published by the time we look
-  const uint32_t k = t / w.n_features;
-  const uint32_t f = t - k * w.n_features;
-  const PartTile tl = w.tiles[k];
-  const PartSeg sg = w.big[tl.seg];
-  const uint32_t lo = tl.j * TILE_ELEMS;
-  const uint32_t cnt = min(TILE_ELEMS, sg.n - lo);
-  const IdxT* src = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride + lo;
-  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+__device__ __forceinline__ void issue_tile(const IdxT* seg_in, uint32_t n, uint32_t j, unsigned char* buf,
+                                           uint64_t* bar, uint32_t* off_out) {
+  const uint32_t lo = j * TILE_ELEMS;
+  const uint32_t cnt = min(TILE_ELEMS, n - lo);
+  const uintptr_t a = reinterpret_cast<uintptr_t>(seg_in + lo);
   const uintptr_t a0 = a & ~uintptr_t(15);
   const uintptr_t e1 = (a + (uintptr_t)cnt * sizeof(IdxT) + 15) & ~uintptr_t(15);
-  jb->src16 = reinterpret_cast<const void*>(a0);
-  jb->bytes = (uint32_t)(e1 - a0);
-  jb->off = (uint32_t)((a - a0) / sizeof(IdxT));
-  jb->out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
-  jb->mark = sg.mark;
-  jb->col = w.status + (size_t)f * w.cap_status + sg.status;
-  jb->lo = lo;
-  jb->cnt = cnt;
-  jb->n = sg.n;
-  jb->nl = sg.nl;
-  jb->j = tl.j;
-  jb->ntiles = tl.ntiles;
-  jb->keep_right = sg.keep_right;
-  jb->valid = 1;
+  *off_out = (uint32_t)((a - a0) / sizeof(IdxT));
+  mbar_expect_tx(bar, (uint32_t)(e1 - a0));
+  bulk_g2s(buf, reinterpret_cast<const void*>(a0), (uint32_t)(e1 - a0), bar);
 }
 
-// Persistent CTAs; the index tile of the next ticket is brought into shared
-// memory by a TMA bulk copy while the current tile gathers its marks, looks
-// back for its carry and stores.  Copies read up to 15 bytes past a tile's
-// last element (16-byte rounding); list buffers carry that padding.
 template <typename IdxT>
-__global__ void __launch_bounds__(BIG_THREADS) k_part_big(PartWork w) {
-  constexpr uint32_t BUF = TILE_ELEMS * sizeof(IdxT) + 32;
-  __shared__ alignas(128) unsigned char sbuf[2][BUF];
-  __shared__ alignas(8) uint64_t bars[2];
-  __shared__ TileJob jobs[2];
-  __shared__ uint32_t s_carry;
-  __shared__ uint32_t s_wcnt[BIG_WARPS], s_woff[BIG_WARPS];
+constexpr uint32_t ring_buf_bytes() {
+  return TILE_ELEMS * sizeof(IdxT) + 128;
+}
+
+template <typename IdxT>
+__global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
+  constexpr uint32_t BUF = ring_buf_bytes<IdxT>();
+  extern __shared__ __align__(128) unsigned char ring_smem[];
+  unsigned char(*sbuf)[BUF] = reinterpret_cast<unsigned char(*)[BUF]>(ring_smem);
+  __shared__ alignas(8) uint64_t bars[RING];
+  __shared__ uint32_t s_off[RING];
+  __shared__ uint32_t s_chain;
+  __shared__ uint32_t s_wcnt[BIG_WARPS];
   const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
   const unsigned lt = lanemask_lt();
-  const uint32_t ntiles = live(w, w.n_tiles, w.cap_tiles);
-  const uint64_t tasks = (uint64_t)ntiles * w.n_features;
+  const uint32_t nbig = live(w, w.n_big, w.cap_big);
+  const uint64_t chains = (uint64_t)nbig * w.n_features;
   if (threadIdx.x == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
+    for (uint32_t i = 0; i < RING; ++i) mbar_init(&bars[i], 1);
     mbar_fence_init();
-    claim_tile<IdxT>(w, ntiles, tasks, &jobs[0]);
-    if (jobs[0].valid) {
-      mbar_expect_tx(&bars[0], jobs[0].bytes);
-      bulk_g2s(sbuf[0], jobs[0].src16, jobs[0].bytes, &bars[0]);
+  }
+  uint32_t uses[RING] = {0u, 0u, 0u};  // completed phases per ring buffer (uniform)
+  uint32_t g = 0;                      // tiles consumed by this CTA (ring position)
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_chain = atomicAdd(w.ticket, 1u);
+    __syncthreads();
+    const uint32_t c = s_chain;
+    if ((uint64_t)c >= chains) break;
+    // feature-fastest: the chains in flight share few segments (trees), so the
+    // mark bytes they gather stay hot in L2
+    const uint32_t si = c / w.n_features;
+    const uint32_t f = c - si * w.n_features;
+    const PartSeg sg = w.big[si];
+    const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
+    IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
+    const uint32_t n = sg.n;
+    const uint32_t ntiles = ceil_div(n, TILE_ELEMS);
+    if (threadIdx.x == 0)
+      for (uint32_t j = 0; j < RING - 1 && j < ntiles; ++j)
+        issue_tile<IdxT>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING]);
+    uint32_t carry = 0;
+    for (uint32_t j = 0; j < ntiles; ++j, ++g) {
+      const uint32_t b = g % RING;
+      if (threadIdx.x == 0 && j + RING - 1 < ntiles) {  // refill the buffer freed by tile j-1
+        const uint32_t bn = (g + RING - 1) % RING;
+        issue_tile<IdxT>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn]);
+      }
+      bool ok = true;
+      {
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&bars[b], uses[b] & 1u)) {
+          if (++spins > (SPIN_LIMIT << 2)) {
+            ok = false;
+            break;
+          }
+        }
+      }
+      if (!__syncthreads_and(ok)) {
+        // never read a tile that did not arrive: flag, drain the ring (bounded), leave
+        if (threadIdx.x == 0) atomicOr(w.error, DEV_ERR_TIMEOUT);
+        for (uint32_t k = 0; k < RING && j + k < ntiles; ++k) {  // tiles j .. j+RING-1 may be in flight
+          const uint32_t bb = (g + k) % RING;
+          uint32_t spins = 0;
+          while (!mbar_try_wait(&bars[bb], uses[bb] & 1u) && ++spins < (SPIN_LIMIT << 4)) {
+          }
+          uses[bb] += 1;
+        }
+        return;
+      }
+      uses[b] += 1;
+      const uint32_t lo = j * TILE_ELEMS;
+      const uint32_t cnt = min(TILE_ELEMS, n - lo);
+      const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
+      const uint32_t wlo = warp * (32 * PART_ROUNDS);
+      unsigned lmask[PART_ROUNDS];
+      uint32_t wc = 0;
+#pragma unroll
+      for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+        const uint32_t q = wlo + r * 32 + lane;
+        const bool left = q < cnt && left_bit(sg.bits, (uint32_t)rows[q < cnt ? q : 0]);
+        lmask[r] = __ballot_sync(FULL, left);
+        wc += __popc(lmask[r]);
+      }
+      if (lane == 0) s_wcnt[warp] = wc;
+      __syncthreads();
+      uint32_t woff = 0, total = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < (uint32_t)BIG_WARPS; ++k) {
+        const uint32_t v = s_wcnt[k];
+        woff += k < warp ? v : 0u;
+        total += v;
+      }
+      uint32_t run = carry + woff;
+#pragma unroll
+      for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+        const uint32_t q = wlo + r * 32 + lane;
+        const bool left = (lmask[r] >> lane) & 1u;
+        const uint32_t rl = run + __popc(lmask[r] & lt);
+        if (q < cnt && (left || sg.keep_right)) {
+          const uint32_t p = lo + q;
+          const uint32_t dst = left ? rl : sg.nl + (p - rl);
+          if (dst < n) out[dst] = rows[q];
+        }
+        run += __popc(lmask[r]);
+      }
+      carry += total;
+      __syncthreads();  // tile buffer and s_wcnt free for reuse
     }
   }
-  __syncthreads();
-  uint32_t phase[2] = {0u, 0u};
-  for (uint32_t it = 0;; ++it) {
-    const uint32_t b = it & 1u;
-    if (!jobs[b].valid) break;
-    if (threadIdx.x == 0) {  // prefetch the next work item into the other buffer
-      claim_tile<IdxT>(w, ntiles, tasks, &jobs[b ^ 1u]);
-      if (jobs[b ^ 1u].valid) {
-        mbar_expect_tx(&bars[b ^ 1u], jobs[b ^ 1u].bytes);
-        bulk_g2s(sbuf[b ^ 1u], jobs[b ^ 1u].src16, jobs[b ^ 1u].bytes, &bars[b ^ 1u]);
-      }
-    }
-    // wait for this tile's indices (bounded; a copy of at most 16 KiB)
-    bool ok = true;
-    {
-      uint32_t spins = 0;
-      while (!mbar_try_wait(&bars[b], phase[b])) {
-        if (++spins > (SPIN_LIMIT << 2)) {
-          ok = false;
-          break;
-        }
-      }
-    }
-    if (!__syncthreads_and(ok)) {
-      // never read a tile that did not arrive: flag, drain both buffers' copies (bounded), leave
-      if (threadIdx.x == 0) atomicOr(w.error, DEV_ERR_TIMEOUT);
-      uint32_t spins = 0;
-      while (!mbar_try_wait(&bars[b], phase[b]) && ++spins < (SPIN_LIMIT << 4)) {
-      }
-      if (jobs[b ^ 1u].valid) {
-        spins = 0;
-        while (!mbar_try_wait(&bars[b ^ 1u], phase[b ^ 1u]) && ++spins < (SPIN_LIMIT << 4)) {
-        }
-      }
-      return;
-    }
-    phase[b] ^= 1u;
-    const TileJob jb = jobs[b];
-    const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + jb.off;
-    const uint32_t wlo = warp * (32 * PART_ROUNDS);
-    unsigned lmask[PART_ROUNDS];
-    uint32_t cnt = 0;
-#pragma unroll
-    for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-      const uint32_t q = wlo + r * 32 + lane;
-      const bool left = q < jb.cnt && jb.mark[(uint32_t)rows[q < jb.cnt ? q : 0]] != 0;
-      lmask[r] = __ballot_sync(FULL, left);
-      cnt += __popc(lmask[r]);
-    }
-    if (lane == 0) s_wcnt[warp] = cnt;
-    __syncthreads();
-    if (warp == 0) {
-      const uint32_t c = lane < BIG_WARPS ? s_wcnt[lane] : 0u;
-      uint32_t inc = c;
-#pragma unroll
-      for (int sft = 1; sft < BIG_WARPS; sft <<= 1) {
-        const uint32_t o = __shfl_up_sync(FULL, inc, sft);
-        if (lane >= (uint32_t)sft) inc += o;
-      }
-      if (lane < BIG_WARPS) s_woff[lane] = inc - c;
-      const uint32_t total = __shfl_sync(FULL, inc, BIG_WARPS - 1);
-      uint32_t carry = 0;
-      if (jb.ntiles > 1) {
-        if (jb.j == 0) {
-          if (lane == 0) publish(jb.col, ST_INC | total);
-        } else {
-          if (lane == 0) publish(jb.col + jb.j, ST_AGG | total);
-          carry = window_lookback(jb.col, jb.j, w.error);
-          if (lane == 0) publish(jb.col + jb.j, ST_INC | (uint64_t)(carry + total));
-        }
-      }
-      if (lane == 0) s_carry = carry;
-    }
-    __syncthreads();
-    uint32_t run = s_carry + s_woff[warp];
-    IdxT* out = reinterpret_cast<IdxT*>(jb.out);
-#pragma unroll
-    for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-      const uint32_t q = wlo + r * 32 + lane;
-      const bool left = (lmask[r] >> lane) & 1u;
-      const uint32_t rl = run + __popc(lmask[r] & lt);
-      if (q < jb.cnt && (left || jb.keep_right)) {
-        const uint32_t p = jb.lo + q;
-        const uint32_t dst = left ? rl : jb.nl + (p - rl);
-        if (dst < jb.n) out[dst] = rows[q];
-      }
-      run += __popc(lmask[r]);
-    }
-    __syncthreads();
+}
+
+__global__ void k_pack_marks(const uint8_t* __restrict__ mark, uint32_t* __restrict__ bits, uint32_t n_rows,
+                             uint32_t words, uint32_t n_slots) {
+  const uint64_t total = (uint64_t)words * n_slots;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t slot = (uint32_t)(i / words), wd = (uint32_t)(i - (uint64_t)slot * words);
+    const uint8_t* m = mark + (size_t)slot * n_rows + (size_t)wd * 32;
+    const uint32_t lim = wd * 32 < n_rows ? min(32u, n_rows - wd * 32) : 0u;
+    uint32_t v = 0;
+    for (uint32_t k = 0; k < lim; ++k) v |= (m[k] ? 1u : 0u) << k;
+    bits[i] = v;
   }
 }
 
 template <typename K>
-int resident_blocks(K kernel, int threads) {
+int resident_blocks(K kernel, int threads, size_t dyn_smem = 0) {
   static int sms = 0;
   if (sms == 0) {
     int dev = 0;
@@ -384,11 +321,32 @@ int resident_blocks(K kernel, int threads) {
     if (sms <= 0) sms = 148;
   }
   int per = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, dyn_smem);
   return sms * (per > 0 ? per : 1);
 }
 
+template <typename IdxT>
+int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
+  const size_t smem = RING * ring_buf_bytes<IdxT>();
+  static bool configured = false;  // per instantiation; the attribute is per device function
+  if (!configured) {
+    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_big<IdxT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    configured = true;
+  }
+  const int cap = resident_blocks(k_part_big<IdxT>, BIG_THREADS, smem);
+  k_part_big<IdxT><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, smem, st>>>(w);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
 }  // namespace
+
+void launch_pack_marks(const uint8_t* mark, uint32_t* bits, uint32_t n_rows, uint32_t n_slots, cudaStream_t st) {
+  const uint32_t words = mark_bit_words(n_rows);
+  const uint64_t total = (uint64_t)words * n_slots;
+  const uint32_t blocks = (uint32_t)std::min<uint64_t>((total + 255) / 256, 148u * 16u);
+  k_pack_marks<<<blocks, 256, 0, st>>>(mark, bits, n_rows, words, n_slots);
+}
 
 int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
                          cudaStream_t st) {
@@ -404,14 +362,9 @@ int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound
     }
   }
   if (bound_tiles > 0) {
-    const uint64_t want = bound_tiles * w.n_features;
-    if (index_bytes == 2) {
-      const int cap = resident_blocks(k_part_big<uint16_t>, BIG_THREADS);
-      k_part_big<uint16_t><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, 0, st>>>(w);
-    } else {
-      const int cap = resident_blocks(k_part_big<uint32_t>, BIG_THREADS);
-      k_part_big<uint32_t><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, 0, st>>>(w);
-    }
+    const uint64_t want = bound_tiles * w.n_features;  // >= number of (big segment, feature) chains
+    if (index_bytes == 2) CT_TRY(launch_big<uint16_t>(w, want, st));
+    else CT_TRY(launch_big<uint32_t>(w, want, st));
   }
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;

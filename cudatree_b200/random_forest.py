@@ -240,7 +240,7 @@ class RandomForestClassifier:
         per_call = 1 if mode == "plain" else k
         si0 = _dev_bytes(slots * f * n * self.index_bytes, dev)
         si1 = _dev_bytes(slots * f * n * self.index_bytes, dev)
-        mark = _dev_bytes(slots * n, dev)
+        mark = _dev_bytes(_lib.mark_bytes(n, slots), dev)
         lists = _lib.Lists(_ptr(si0), _ptr(si1), _ptr(mark), n, slots)
         cap = 2 * n
         raw = {name: torch.empty(per_call * cap, dtype=torch.int32, device=dev)

@@ -59,8 +59,10 @@ typedef struct ct_problem {
 
 /* Double-buffered per-tree index lists (reference sorted_indices_gpu and
  * sorted_indices_gpu_, random_tree.py:466-467).  Slot s, buffer b, feature f
- * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark is
- * [n_slots][n_rows] bytes (reference mark_table, random_forest.py:168). */
+ * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark
+ * holds the [n_slots][n_rows] byte mark table (reference mark_table,
+ * random_forest.py:168) followed, at the next 256-byte boundary, by its
+ * packed [n_slots][bit_words] uint32 copy; ct_mark_bytes gives the size. */
 /* The partition and compaction kernels copy index tiles with 16-byte TMA
  * bulk copies and may read up to 15 bytes past the last element of the
  * si0/si1 buffers and of the presort: allocate them with >= 16 bytes of
@@ -118,6 +120,9 @@ typedef struct ct_fit_options {
   uint32_t scan_piece;      /* elements per split-scan work item (0 = default)      */
   uint32_t reserved[4];
 } ct_fit_options;
+
+/* Bytes of the ct_lists.mark buffer for n_slots tree slots. */
+int ct_mark_bytes(uint32_t n_rows, uint32_t n_slots, size_t* bytes);
 
 /* ---------------------------------------------------------------- info --- */
 const char* ct_version(void);

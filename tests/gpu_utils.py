@@ -70,7 +70,7 @@ class GpuLists:
         self.slots = slots
         nbytes = slots * gp.f * gp.n * gp.ib
         self.si = [dev_bytes(nbytes), dev_bytes(nbytes)]
-        self.mark = dev_bytes(slots * gp.n)
+        self.mark = dev_bytes(_lib.mark_bytes(gp.n, slots))
         self.lists = _lib.Lists(self.si[0].data_ptr(), self.si[1].data_ptr(), self.mark.data_ptr(), gp.n,
                                 slots)
 
