@@ -162,6 +162,112 @@ def run_reference(args, world, rank):
     return 0
 
 
+# ------------------------------------------------------------------ serving
+def run_serving(args, x_cov, y_cov, seed):
+    """Serving workload: a 500-tree covtype-shaped forest + 8 resident forests
+    (50-500 trees, 16-512 features), Poisson arrivals at args.rate req/s,
+    rows log-uniform in [1, 65536], 5 % small fit jobs (<= 20,000 rows, 10
+    trees); p50/p99 latency and rows/s from the engine, and a spot check that
+    served predictions equal the plain predict path."""
+    import torch
+
+    from cudatree_b200 import RandomForestClassifier
+    from cudatree_b200.serving import ForestServer, pinned
+
+    rng = np.random.default_rng(5)
+    forests, pools = [], []
+    big = RandomForestClassifier(args.serve_trees, max_features=MAX_FEATURES, seed=seed + 17).fit(x_cov, y_cov)
+    forests.append(big)
+    pools.append(x_cov[:65536])
+    feats = [16, 32, 64, 128, 192, 256, 384, 512]
+    for j, f in enumerate(feats):
+        n, c = 20000, int(rng.integers(2, 51))
+        yj = rng.integers(0, c, size=n)
+        means = rng.normal(0.0, 1.0, size=(c, f)).astype(np.float32)
+        xj = (rng.standard_normal((n, f)).astype(np.float32) + means[yj])
+        trees = int(rng.integers(50, 501))
+        forests.append(RandomForestClassifier(trees, seed=seed + j).fit(xj, yj))
+        pool = (rng.standard_normal((65536, f)).astype(np.float32) + means[rng.integers(0, c, 65536)])
+        pools.append(pool)
+    # plain-path throughput: one 65,536-row batch on the 500-tree forest
+    nodes, offs = big._device_forest()
+    from cudatree_b200 import _lib
+    xd = torch.from_numpy(pools[0]).cuda()
+    out = torch.empty(xd.shape[0], dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream()
+    for _ in range(2):
+        _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
+                  big.n_features, big.n_labels, None, out.data_ptr(), st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    reps = 5
+    for _ in range(reps):
+        _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
+                  big.n_features, big.n_labels, None, out.data_ptr(), st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    batch_rows_per_s = reps * xd.shape[0] / (e0.elapsed_time(e1) / 1000.0)
+
+    srv = ForestServer(max_features=512, fit_workers=2, max_fit_rows=20000, max_fit_trees=10)
+    ids = [srv.add_forest(f) for f in forests]
+    pinned_pools = [pinned(p) for p in pools]
+    fit_x, fit_y = pinned(pools[3][:20000]), pinned(rng.integers(0, 10, 20000).astype(np.uint32))
+    n_req = int(args.rate * args.serve_seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=n_req))
+    reqs, meta = [], []
+    rows_total = 0
+    plans = []
+    for i in range(n_req):
+        if rng.random() < 0.05:
+            n = int(np.exp(rng.uniform(np.log(500), np.log(20000))))
+            plans.append(("fit", n))
+        else:
+            k = int(rng.integers(0, len(forests)))
+            n = int(np.exp(rng.uniform(0.0, np.log(65536))))
+            plans.append(("predict", k, n, int(rng.integers(0, 65536 - n + 1))))
+            rows_total += n
+    outbuf = torch.zeros(rows_total, dtype=torch.int32).pin_memory()
+    pos = 0
+    for i, plan in enumerate(plans):
+        if plan[0] == "fit":
+            n = plan[1]
+            r = srv.fit_request(fit_x[:n], fit_y[:n], n_classes=10, n_trees=10, seed=i)
+            meta.append(None)
+        else:
+            _, k, n, lo = plan
+            xs = pinned_pools[k][lo:lo + n]
+            o = outbuf[pos:pos + n]
+            r = srv.predict_request(ids[k], xs, o)
+            meta.append((k, lo, n, pos))
+            pos += n
+        r.arrival_s = float(arrivals[i])
+        reqs.append(r)
+    stats = srv.replay(reqs, timeout_s=300.0)
+    # spot check: served predictions == plain predict path
+    same = True
+    checked = 0
+    for i in rng.permutation(len(reqs))[:40]:
+        if meta[i] is None or reqs[i].status != 0:
+            continue
+        k, lo, n, p0 = meta[i]
+        got = forests[k].compt_table[outbuf[p0:p0 + n].numpy().astype(np.int64)]
+        same &= bool(np.array_equal(got, forests[k].predict(pools[k][lo:lo + n])))
+        checked += 1
+    srv.close()
+    return {
+        "workload": f"{args.serve_trees}-tree covtype-shaped forest + 8 forests (50-500 trees, 16-512 features); "
+                    f"Poisson {args.rate:g} req/s for {args.serve_seconds:g} s, rows log-uniform [1, 65536], "
+                    "5% fit jobs (<= 20000 rows, 10 trees)",
+        "requests": int(stats["requests"]), "fit_jobs": int(stats["fit_jobs"]), "rejected": int(stats["rejected"]),
+        "rows_per_s": stats["rows_per_s"], "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"],
+        "p50_ms_le4096_rows": stats["p50_small_ms"], "p99_ms_le4096_rows": stats["p99_small_ms"],
+        "p50_fit_ms": stats["p50_fit_ms"], "p99_fit_ms": stats["p99_fit_ms"], "batches": int(stats["batches"]),
+        "hbm_used_gb": stats["hbm_used_bytes"] / 1e9,
+        "identical_to_plain_predict": bool(same), "checked_requests": checked,
+        "plain_predict_rows_per_s_500_trees": batch_rows_per_s,
+    }
+
+
 # --------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local):
     import torch
@@ -170,14 +276,15 @@ def run_ours(args, world, rank, local):
 
     x, y = synthetic.covtype_like()
     seed = 1000 + rank
-    forest = RandomForestClassifier(N_TREES, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
+    n_trees = args.trees
+    forest = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
     forest.fit_init(x, y)
     thr = forest.bfs_threshold
     stream = torch.cuda.current_stream()
 
     def step(mode="batched", profile=False):
         forest.profile = profile
-        return forest._fit_trees(0, N_TREES, mode, thr)
+        return forest._fit_trees(0, n_trees, mode, thr)
 
     for _ in range(args.warmup):
         step()
@@ -205,7 +312,7 @@ def run_ours(args, world, rank, local):
         forest._fit_trees(0, 1, "plain", thr)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        plain_trees = forest._fit_trees(0, N_TREES, "plain", thr)
+        plain_trees = forest._fit_trees(0, n_trees, "plain", thr)
         torch.cuda.synchronize()
         plain_s = time.perf_counter() - t0
         same = all(np.array_equal(a.left_children, b.left_children) and
@@ -214,20 +321,22 @@ def run_ours(args, world, rank, local):
     forest.fit_release()
 
     # end to end through the public API: pinned host arrays in, trees out
-    xp = torch.from_numpy(x).pin_memory()
+    xp = torch.from_numpy(x).pin_memory() if args.e2e_steps > 0 else None
     yp = torch.from_numpy(y)
     e2e_times = []
-    for i in range(1 + args.e2e_steps):
-        f2 = RandomForestClassifier(N_TREES, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
+    f2 = forest
+    for i in range(1 + args.e2e_steps if args.e2e_steps > 0 else 0):
+        f2 = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         f2.fit(xp, yp)
         torch.cuda.synchronize()
         if i > 0:
             e2e_times.append(time.perf_counter() - t0)
-    e2e_s = max_over_ranks(statistics.mean(e2e_times), world)
-    d2h = sum(t.n_nodes for t in f2._trees) * 20 + 4 * N_TREES
+    e2e_s = max_over_ranks(statistics.mean(e2e_times), world) if e2e_times else None
+    d2h = sum(t.n_nodes for t in trees) * 20 + 4 * n_trees
 
+    serving = None if args.skip_serving else run_serving(args, x, y, seed)
     if rank != 0:
         return 0
     peak, peak_kind = peaks()
@@ -277,6 +386,7 @@ def run_ours(args, world, rank, local):
         "scan_roofline": {"kernel": "k_split_scan (+hist/carry)",
                           "achieved": round(stats["bytes"][si] / (s_ms * 1e6), 1) if s_ms > 0 else None,
                           "peak": peak, "unit": "GB/s"},
+        "predict": serving,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(x.nbytes + y.shape[0]),
                 "d2h_bytes_per_step": int(d2h)},
@@ -293,10 +403,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2, help="0 skips the end-to-end measurement")
+    ap.add_argument("--trees", type=int, default=N_TREES, help="trees per forest (profiling runs use fewer)")
     ap.add_argument("--ref-trees", type=int, default=100)
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--serve-trees", type=int, default=500)
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--rate", type=float, default=2000.0)
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

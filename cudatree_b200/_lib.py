@@ -121,6 +121,13 @@ PROTOTYPES = {
     "ct_fit_stats": (C.c_int, [C.c_void_p]),
     "ct_tree_canonicalize": (C.c_int, [P, P, P, P, P, C.c_uint32, P, P, P, P, P]),
     "ct_predict": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
+    "ct_server_create": (C.c_int, [P, P]),
+    "ct_server_destroy": (C.c_int, [P]),
+    "ct_server_add_forest": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
+    "ct_server_submit": (C.c_int, [P, P]),
+    "ct_server_wait": (C.c_int, [P, P, C.c_double]),
+    "ct_server_replay": (C.c_int, [P, P, C.c_uint32, C.c_double, P]),
+    "ct_server_get_stats": (C.c_int, [P, P]),
 }
 
 _lib = None

@@ -29,6 +29,7 @@ SOURCES = [
     "ct_presort.cu",
     "ct_partition.cu",
     "ct_noalloc.cu",
+    "ct_server.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

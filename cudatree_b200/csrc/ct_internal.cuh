@@ -304,6 +304,24 @@ PartWork level_part_work(const View& v, const LevelScratch& s);
 int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
 
 View make_view(const ct_problem* p, const ct_lists* l);
+
+// One request of a multi-request predict launch (ct_predict.cu): blocks
+// [block0, block0 + ceil(n_rows / rows_per_block)) of the launch are its.
+struct BatchReq {
+  const ct_packed_node* nodes;
+  const uint32_t* tree_off;
+  const float* x;         // [n_rows][n_features] on the device
+  uint32_t* pred;         // [n_rows] on the device
+  uint32_t n_rows;
+  uint32_t n_features;
+  uint32_t n_classes;
+  uint32_t n_trees;
+  uint32_t block0;
+  uint32_t pad[3];
+};
+int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t rows_per_block,
+                  uint32_t max_classes, cudaStream_t st);
+int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st);
 int check_problem(const ct_problem* p);
 
 }  // namespace ct

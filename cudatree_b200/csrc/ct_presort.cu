@@ -147,6 +147,22 @@ __global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
 
 }  // namespace
 
+// Row-major [n_rows][n_cols] -> column-major [n_cols][n_rows] through a
+// 32x33 shared-memory tile (coalesced reads and writes).
+__global__ void k_transpose(const float* __restrict__ in, uint32_t n_rows, uint32_t n_cols, float* __restrict__ out) {
+  __shared__ float tile[32][33];
+  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t r = r0 + k, c = c0 + threadIdx.x;
+    if (r < n_rows && c < n_cols) tile[k][threadIdx.x] = in[(size_t)r * n_cols + c];
+  }
+  __syncthreads();
+  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+    const uint32_t c = c0 + k, r = r0 + threadIdx.x;
+    if (r < n_rows && c < n_cols) out[(size_t)c * n_rows + r] = tile[threadIdx.x][k];
+  }
+}
+
 size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features) {
   const size_t tiles = ceil_div(n_rows, RS_TILE);
   const size_t elems = (size_t)n_rows * n_features;
@@ -190,6 +206,16 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
     k_digit_scan<<<n_features, 1024, 0, st>>>(hist, tiles);
     k_digit_move<<<grid, RS_THREADS, 0, st>>>(a);
   }
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st) {
+  CT_ARG_CHECK(x_rm && x_cm, "transpose: NULL argument");
+  if (n_rows == 0 || n_cols == 0) return CT_OK;
+  const dim3 grid(ceil_div(n_cols, 32), ceil_div(n_rows, 32));
+  CT_ARG_CHECK(grid.y <= 65535u, "transpose: too many rows for one launch");
+  k_transpose<<<grid, dim3(32, 8), 0, st>>>(x_rm, n_rows, n_cols, x_cm);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

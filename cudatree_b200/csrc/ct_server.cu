@@ -1,0 +1,662 @@
+// Serving engine: resident forests, continuous batching of predict
+// requests, small fit jobs, admission by an HBM budget, latency percentiles.
+//
+// The reference has no serving path (its predict re-uploads X and every tree
+// per call, base_tree.py:57-62).  Here:
+//   * forests stay resident on the device as packed breadth-first nodes;
+//   * two predict lanes, each a worker thread with its own CUDA stream: small
+//     requests (<= small_rows rows) on a high-priority stream, larger ones on
+//     a low-priority stream, so a 65k-row request does not hold back 1-row
+//     requests;
+//   * a lane takes every request that has arrived (up to its staging
+//     capacity) into one multi-request predict launch; with two staging
+//     slots a lane launches the next batch while the previous one runs, and
+//     requests that arrive meanwhile join the next batch (continuous
+//     batching);
+//   * fit jobs (host arrays in, a new resident forest out) run on fit-worker
+//     threads with their own low-priority streams and device arenas, so
+//     their kernels overlap the predict batches;
+//   * every device allocation is made at creation or when a forest is added,
+//     against the byte budget; a request that does not fit is rejected with
+//     CT_ERR_OOM instead of allocating.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "ct_internal.cuh"
+
+namespace ct {
+
+size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
+int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees, const ct_fit_options* o,
+        const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
+int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
+                 const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
+                 uint32_t* ov);
+size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features);
+int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
+            size_t wsb, cudaStream_t st);
+
+namespace {
+
+constexpr uint32_t PRED_ROWS_PER_BLOCK = 8;
+
+double now_s() {
+  using namespace std::chrono;
+  return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct Forest {
+  ct_packed_node* nodes = nullptr;
+  uint32_t* off = nullptr;
+  uint32_t n_nodes = 0, n_trees = 0, n_features = 0, n_classes = 0;
+  size_t bytes = 0;
+};
+
+struct Job {
+  ct_request* req = nullptr;
+  double t_start = 0;
+  bool done = false;
+};
+
+struct Slot {
+  float* x_dev = nullptr;
+  uint32_t* pred_dev = nullptr;
+  BatchReq* req_dev = nullptr;
+  BatchReq* req_host = nullptr;  // pinned
+  cudaEvent_t ev = nullptr;
+  std::vector<Job*> jobs;
+  double launched = 0;
+};
+
+struct Lane {
+  cudaStream_t st = nullptr;
+  std::deque<Job*> q;
+  Slot slot[2];
+  std::thread th;
+  uint64_t cap_rows = 0, cap_floats = 0;
+};
+
+struct FitWorker {
+  cudaStream_t st = nullptr;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  std::thread th;
+};
+
+}  // namespace
+
+class Server {
+ public:
+  ct_server_config cfg{};
+  int device = 0;
+  size_t budget = 0, used = 0;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  std::vector<Forest> forests;
+  Lane lanes[2];
+  std::deque<Job*> fit_q;
+  std::vector<FitWorker> fit_workers;
+  // statistics
+  std::vector<double> lat_small, lat_large, lat_fit;
+  uint64_t n_req = 0, n_rows = 0, n_batches = 0, n_fit = 0, n_rejected = 0;
+  double t_first = 0, t_last = 0;
+  std::string error;
+
+  ~Server() { shutdown(); }
+
+  int take(size_t bytes, void** out) {
+    if (used + bytes > budget) {
+      set_last_error("server: HBM budget exhausted (" + std::to_string(used + bytes) + " > " +
+                     std::to_string(budget) + " bytes)");
+      return CT_ERR_OOM;
+    }
+    CT_CUDA_TRY(cudaMalloc(out, bytes));
+    used += bytes;
+    return CT_OK;
+  }
+
+  int init(const ct_server_config* c) {
+    cfg = *c;
+    if (!cfg.max_batch_rows) cfg.max_batch_rows = 131072;
+    if (!cfg.max_features) cfg.max_features = 512;
+    if (!cfg.small_rows) cfg.small_rows = 4096;
+    if (!cfg.max_fit_rows) cfg.max_fit_rows = 20000;
+    if (!cfg.max_fit_trees) cfg.max_fit_trees = 10;
+    CT_CUDA_TRY(cudaGetDevice(&device));
+    size_t free_b = 0, total_b = 0;
+    CT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    budget = cfg.hbm_budget_bytes ? cfg.hbm_budget_bytes : (size_t)(free_b * 0.8);
+    int prio_lo = 0, prio_hi = 0;
+    CT_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    for (int l = 0; l < 2; ++l) {
+      Lane& ln = lanes[l];
+      CT_CUDA_TRY(cudaStreamCreateWithPriority(&ln.st, cudaStreamNonBlocking, l == 0 ? prio_hi : prio_lo));
+      ln.cap_rows = l == 0 ? std::max<uint64_t>(cfg.small_rows * 8ull, 32768) : cfg.max_batch_rows;
+      ln.cap_floats = ln.cap_rows * cfg.max_features;
+      for (auto& s : ln.slot) {
+        CT_TRY(take(ln.cap_floats * sizeof(float), (void**)&s.x_dev));
+        CT_TRY(take(ln.cap_rows * sizeof(uint32_t), (void**)&s.pred_dev));
+        CT_TRY(take(4096 * sizeof(BatchReq), (void**)&s.req_dev));
+        CT_CUDA_TRY(cudaMallocHost((void**)&s.req_host, 4096 * sizeof(BatchReq)));
+        CT_CUDA_TRY(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
+      }
+    }
+    const uint32_t nfw = cfg.fit_workers;
+    fit_workers.resize(nfw);
+    const size_t arena = fit_arena_bytes();
+    for (auto& fw : fit_workers) {
+      CT_CUDA_TRY(cudaStreamCreateWithPriority(&fw.st, cudaStreamNonBlocking, prio_lo));
+      CT_TRY(take(arena, (void**)&fw.arena));
+      fw.arena_bytes = arena;
+    }
+    for (int l = 0; l < 2; ++l) lanes[l].th = std::thread([this, l] { lane_loop(l); });
+    for (auto& fw : fit_workers) fw.th = std::thread([this, &fw] { fit_loop(fw); });
+    return CT_OK;
+  }
+
+  // Device bytes of one fit job at the configured maximum size.
+  size_t fit_arena_bytes() const { return job_bytes(cfg.max_fit_rows, cfg.max_features, 255, cfg.max_fit_trees); }
+
+  static size_t job_bytes(uint32_t n, uint32_t f, uint32_t c, uint32_t t) {
+    ct_problem p{};
+    p.n_rows = n;
+    p.n_features = f;
+    p.n_classes = c;
+    p.index_bytes = n <= 0xFFFF ? 2 : 4;
+    p.label_bytes = c <= 255 ? 1 : 2;
+    p.max_features = 1;
+    p.min_samples_split = 1;
+    ct_fit_options o{};
+    o.mode = CT_FIT_BATCHED;
+    const size_t ib = p.index_bytes, nf = (size_t)n * f;
+    size_t mb = 0;
+    mb = (((size_t)t * n + 255) & ~size_t(255)) + (size_t)t * mark_bit_words(n) * 4 + 64;
+    size_t b = 0;
+    auto add = [&](size_t x) { b += (x + 511) & ~size_t(511); };
+    add(nf * 4);                       // x row-major
+    add(nf * 4);                       // x feature-major
+    add((size_t)n * 2);                // labels
+    add(nf * ib + 64);                 // presort
+    add(presort_workspace_bytes(n, f));
+    add((size_t)t * nf * ib + 64);     // si0
+    add((size_t)t * nf * ib + 64);     // si1
+    add(mb);                           // marks
+    add((size_t)t * 2 * n * 4 * 5);    // raw trees
+    add((size_t)t * 4);                // node counts
+    add(fit_workspace_bytes(&p, t, &o));
+    return b + 4096;
+  }
+
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (stop) return;
+      stop = true;
+    }
+    cv_work.notify_all();
+    for (auto& ln : lanes)
+      if (ln.th.joinable()) ln.th.join();
+    for (auto& fw : fit_workers)
+      if (fw.th.joinable()) fw.th.join();
+    cudaSetDevice(device);
+    for (auto& ln : lanes) {
+      for (auto& s : ln.slot) {
+        if (s.x_dev) cudaFree(s.x_dev);
+        if (s.pred_dev) cudaFree(s.pred_dev);
+        if (s.req_dev) cudaFree(s.req_dev);
+        if (s.req_host) cudaFreeHost(s.req_host);
+        if (s.ev) cudaEventDestroy(s.ev);
+      }
+      if (ln.st) cudaStreamDestroy(ln.st);
+    }
+    for (auto& fw : fit_workers) {
+      if (fw.arena) cudaFree(fw.arena);
+      if (fw.st) cudaStreamDestroy(fw.st);
+    }
+    for (auto& f : forests) {
+      if (f.nodes) cudaFree(f.nodes);
+      if (f.off) cudaFree(f.off);
+    }
+  }
+
+  int add_forest(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* off, uint32_t n_trees,
+                 uint32_t n_features, uint32_t n_classes, uint32_t* id) {
+    CT_ARG_CHECK(nodes && off && id && n_nodes && n_trees, "server: empty forest");
+    CT_ARG_CHECK(n_features <= cfg.max_features, "server: forest has more features than max_features");
+    CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "server: n_classes out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    Forest f;
+    f.n_nodes = n_nodes;
+    f.n_trees = n_trees;
+    f.n_features = n_features;
+    f.n_classes = n_classes;
+    f.bytes = (size_t)n_nodes * sizeof(ct_packed_node) + (size_t)n_trees * 4;
+    CT_CUDA_TRY(cudaSetDevice(device));
+    CT_TRY(take((size_t)n_nodes * sizeof(ct_packed_node), (void**)&f.nodes));
+    CT_TRY(take((size_t)n_trees * 4, (void**)&f.off));
+    CT_CUDA_TRY(cudaMemcpy(f.nodes, nodes, (size_t)n_nodes * sizeof(ct_packed_node), cudaMemcpyHostToDevice));
+    CT_CUDA_TRY(cudaMemcpy(f.off, off, (size_t)n_trees * 4, cudaMemcpyHostToDevice));
+    forests.push_back(f);
+    *id = (uint32_t)(forests.size() - 1);
+    return CT_OK;
+  }
+
+  int submit(ct_request* r) {
+    CT_ARG_CHECK(r && r->x && r->n_rows, "server: empty request");
+    std::unique_lock<std::mutex> lk(mu);
+    r->status = CT_OK;
+    r->latency_ms = -1.0;
+    auto* j = new Job();
+    j->req = r;
+    j->t_start = now_s();
+    if (t_first == 0) t_first = j->t_start;
+    if (r->kind == CT_REQ_FIT) {
+      if (fit_workers.empty()) {
+        delete j;
+        set_last_error("server: no fit workers");
+        return CT_ERR_ARG;
+      }
+      fit_q.push_back(j);
+    } else {
+      if (r->forest >= forests.size()) {
+        delete j;
+        set_last_error("server: unknown forest id");
+        return CT_ERR_ARG;
+      }
+      const Forest& f = forests[r->forest];
+      const int l = r->n_rows <= cfg.small_rows ? 0 : 1;
+      if ((uint64_t)r->n_rows * f.n_features > lanes[l].cap_floats || r->n_rows > lanes[l].cap_rows) {
+        // admission: a request larger than the lane's staging never fits
+        r->status = CT_ERR_OOM;
+        r->latency_ms = 0;
+        ++n_rejected;
+        delete j;
+        set_last_error("server: request larger than the staging capacity");
+        return CT_ERR_OOM;
+      }
+      lanes[l].q.push_back(j);
+    }
+    r->pending_ = j;
+    lk.unlock();
+    cv_work.notify_all();
+    return CT_OK;
+  }
+
+  int wait(ct_request* r, double timeout_s) {
+    std::unique_lock<std::mutex> lk(mu);
+    Job* j = reinterpret_cast<Job*>(r->pending_);
+    if (!j) return r->status;
+    const bool ok = cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), [&] { return j->done; });
+    if (!ok) {
+      set_last_error("server: wait timed out");
+      return CT_ERR_TIMEOUT;
+    }
+    r->pending_ = nullptr;
+    delete j;
+    return r->status;
+  }
+
+  void finish(Job* j, double t, int status) {
+    // caller holds mu
+    ct_request* r = j->req;
+    r->status = status;
+    r->latency_ms = (t - j->t_start) * 1000.0;
+    j->done = true;
+    t_last = std::max(t_last, t);
+    if (r->kind == CT_REQ_FIT) {
+      lat_fit.push_back(r->latency_ms);
+      ++n_fit;
+    } else if (status == CT_OK) {
+      (r->n_rows <= 4096 ? lat_small : lat_large).push_back(r->latency_ms);
+      ++n_req;
+      n_rows += r->n_rows;
+    }
+  }
+
+  void complete_slot(Slot& s) {
+    const double t = now_s();
+    std::lock_guard<std::mutex> lk(mu);
+    for (Job* j : s.jobs) finish(j, t, CT_OK);
+    s.jobs.clear();
+    cv_done.notify_all();
+  }
+
+  void lane_loop(int l) {
+    cudaSetDevice(device);
+    Lane& ln = lanes[l];
+    int next = 0;
+    while (true) {
+      // retire finished batches
+      for (auto& s : ln.slot)
+        if (!s.jobs.empty() && cudaEventQuery(s.ev) == cudaSuccess) complete_slot(s);
+      std::vector<Job*> batch;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        if (ln.q.empty()) {
+          Slot* oldest = nullptr;
+          for (auto& s : ln.slot)
+            if (!s.jobs.empty() && (!oldest || s.launched < oldest->launched)) oldest = &s;
+          if (oldest) {
+            lk.unlock();
+            cudaEventSynchronize(oldest->ev);
+            complete_slot(*oldest);
+            continue;
+          }
+          if (stop) break;
+          cv_work.wait(lk, [&] { return stop || !ln.q.empty(); });
+          if (ln.q.empty()) continue;
+        }
+        uint64_t rows = 0, floats = 0;
+        while (!ln.q.empty() && batch.size() < 4096) {
+          Job* j = ln.q.front();
+          const Forest& f = forests[j->req->forest];
+          const uint64_t fl = (uint64_t)j->req->n_rows * f.n_features;
+          if (!batch.empty() && (rows + j->req->n_rows > ln.cap_rows || floats + fl > ln.cap_floats)) break;
+          rows += j->req->n_rows;
+          floats += fl;
+          batch.push_back(j);
+          ln.q.pop_front();
+        }
+      }
+      Slot& s = ln.slot[next];
+      if (!s.jobs.empty()) {  // both slots busy: wait for this one
+        cudaEventSynchronize(s.ev);
+        complete_slot(s);
+      }
+      next ^= 1;
+      launch(ln, s, batch);
+    }
+  }
+
+  void launch(Lane& ln, Slot& s, std::vector<Job*>& batch) {
+    uint64_t xoff = 0, roff = 0;
+    uint32_t blocks = 0, max_c = 1;
+    std::vector<std::pair<Job*, uint64_t>> outs;
+    int err = 0;
+    for (size_t i = 0; i < batch.size(); ++i) {
+      ct_request* r = batch[i]->req;
+      Forest f;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        f = forests[r->forest];
+      }
+      BatchReq& br = s.req_host[i];
+      br.nodes = f.nodes;
+      br.tree_off = f.off;
+      br.x = s.x_dev + xoff;
+      br.pred = s.pred_dev + roff;
+      br.n_rows = r->n_rows;
+      br.n_features = f.n_features;
+      br.n_classes = f.n_classes;
+      br.n_trees = f.n_trees;
+      br.block0 = blocks;
+      blocks += ceil_div(r->n_rows, PRED_ROWS_PER_BLOCK);
+      max_c = std::max(max_c, f.n_classes);
+      if (cudaMemcpyAsync(s.x_dev + xoff, r->x, (size_t)r->n_rows * f.n_features * sizeof(float),
+                          cudaMemcpyHostToDevice, ln.st) != cudaSuccess)
+        err = 1;
+      outs.push_back({batch[i], roff});
+      xoff += (uint64_t)r->n_rows * f.n_features;
+      roff += r->n_rows;
+    }
+    if (cudaMemcpyAsync(s.req_dev, s.req_host, batch.size() * sizeof(BatchReq), cudaMemcpyHostToDevice, ln.st) !=
+        cudaSuccess)
+      err = 1;
+    if (predict_batch(s.req_dev, (uint32_t)batch.size(), blocks, PRED_ROWS_PER_BLOCK, max_c, ln.st) != CT_OK) err = 1;
+    for (auto& o : outs)
+      if (cudaMemcpyAsync(o.first->req->pred, s.pred_dev + o.second, (size_t)o.first->req->n_rows * 4,
+                          cudaMemcpyDeviceToHost, ln.st) != cudaSuccess)
+        err = 1;
+    cudaEventRecord(s.ev, ln.st);
+    s.launched = now_s();
+    s.jobs = batch;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      ++n_batches;
+    }
+    if (err) {
+      cudaEventSynchronize(s.ev);
+      std::lock_guard<std::mutex> lk(mu);
+      for (Job* j : s.jobs) finish(j, now_s(), CT_ERR_CUDA);
+      s.jobs.clear();
+      cv_done.notify_all();
+    }
+  }
+
+  void fit_loop(FitWorker& fw) {
+    cudaSetDevice(device);
+    while (true) {
+      Job* j = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv_work.wait(lk, [&] { return stop || !fit_q.empty(); });
+        if (fit_q.empty()) {
+          if (stop) break;
+          continue;
+        }
+        j = fit_q.front();
+        fit_q.pop_front();
+      }
+      uint32_t fid = NONE;
+      int st = run_fit(fw, j->req, &fid);
+      std::lock_guard<std::mutex> lk(mu);
+      j->req->result_forest = fid;
+      if (st == CT_ERR_OOM) ++n_rejected;
+      finish(j, now_s(), st);
+      cv_done.notify_all();
+    }
+  }
+
+  // Host arrays -> new resident forest, on the worker's stream and arena.
+  int run_fit(FitWorker& fw, ct_request* r, uint32_t* fid) {
+    const uint32_t n = r->n_rows, F = r->n_features, C = r->n_classes, T = r->n_trees;
+    CT_ARG_CHECK(r->y && n && F && C && T && C <= CT_MAX_CLASSES, "fit job: bad arguments");
+    CT_ARG_CHECK(F <= cfg.max_features, "fit job: more features than the server's max_features");
+    if (job_bytes(n, F, C, T) > fw.arena_bytes) {
+      set_last_error("fit job larger than the fit arena (admission)");
+      return CT_ERR_OOM;
+    }
+    cudaStream_t st = fw.st;
+    Arena a{fw.arena, fw.arena_bytes, 0};
+    const uint32_t ib = n <= 0xFFFF ? 2 : 4, lb = C <= 255 ? 1 : 2;
+    const size_t nf = (size_t)n * F;
+    float* x_rm = a.take<float>(nf);
+    float* x_fm = a.take<float>(nf);
+    char* labels = a.take<char>((size_t)n * 2);
+    char* pre = a.take<char>(nf * ib + 64);
+    const size_t pws_b = presort_workspace_bytes(n, F);
+    char* pws = a.take<char>(pws_b);
+    char* si0 = a.take<char>((size_t)T * nf * ib + 64);
+    char* si1 = a.take<char>((size_t)T * nf * ib + 64);
+    const size_t mb = mark_bits_offset(n, T) + (size_t)T * mark_bit_words(n) * 4 + 64;
+    uint8_t* mark = a.take<uint8_t>(mb);
+    const uint32_t cap = 2 * n;
+    uint32_t* raw = a.take<uint32_t>((size_t)T * cap * 5);
+    uint32_t* counts = a.take<uint32_t>(T);
+    ct_problem p{};
+    p.x_fm = x_fm;
+    p.labels = labels;
+    p.presort = pre;
+    p.n_rows = n;
+    p.n_features = F;
+    p.n_classes = C;
+    p.index_bytes = ib;
+    p.label_bytes = lb;
+    p.max_features = r->max_features ? std::min(r->max_features, F) : (uint32_t)std::ceil(std::sqrt((double)F));
+    p.min_samples_split = 1;
+    p.bootstrap = 1;
+    p.seed = r->seed;
+    ct_fit_options o{};
+    o.mode = CT_FIT_BATCHED;
+    const size_t wsb = fit_workspace_bytes(&p, T, &o);
+    char* ws = a.take<char>(wsb);
+    if (!ws || !a.ok()) {
+      set_last_error("fit job: arena carve failed");
+      return CT_ERR_OOM;
+    }
+    std::vector<uint8_t> lab_host((size_t)n * lb);
+    for (uint32_t i = 0; i < n; ++i) {
+      if (r->y[i] >= C) {
+        set_last_error("fit job: label out of range");
+        return CT_ERR_ARG;
+      }
+      if (lb == 1) lab_host[i] = (uint8_t)r->y[i];
+      else reinterpret_cast<uint16_t*>(lab_host.data())[i] = (uint16_t)r->y[i];
+    }
+    CT_CUDA_TRY(cudaMemcpyAsync(x_rm, r->x, nf * 4, cudaMemcpyHostToDevice, st));
+    CT_CUDA_TRY(cudaMemcpyAsync(labels, lab_host.data(), lab_host.size(), cudaMemcpyHostToDevice, st));
+    CT_TRY(transpose_rows(x_rm, n, F, x_fm, st));
+    CT_TRY(presort(x_fm, n, F, ib, pre, pws, pws_b, st));
+    ct_lists l{si0, si1, mark, n, T};
+    ct_tree_buffers tb{raw, raw + (size_t)T * cap, raw + 2 * (size_t)T * cap,
+                       reinterpret_cast<float*>(raw + 3 * (size_t)T * cap), raw + 4 * (size_t)T * cap, counts, cap};
+    CT_TRY(fit(&p, &l, 0, T, &o, &tb, ws, wsb, st));
+    std::vector<uint32_t> cnt(T);
+    CT_CUDA_TRY(cudaMemcpyAsync(cnt.data(), counts, T * 4, cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<ct_packed_node> packed;
+    std::vector<uint32_t> offs(T);
+    std::vector<uint32_t> h[5];
+    for (uint32_t t = 0; t < T; ++t) {
+      const uint32_t nn = cnt[t];
+      for (int k = 0; k < 5; ++k) {
+        h[k].resize(nn);
+        CT_CUDA_TRY(cudaMemcpyAsync(h[k].data(), raw + (size_t)k * T * cap + (size_t)t * cap, nn * 4,
+                                    cudaMemcpyDeviceToHost, st));
+      }
+      CT_CUDA_TRY(cudaStreamSynchronize(st));
+      std::vector<uint32_t> ol(nn), orr(nn), ov(nn);
+      std::vector<uint16_t> of(nn);
+      std::vector<float> ot(nn);
+      CT_TRY(canonicalize(h[0].data(), h[1].data(), h[2].data(), reinterpret_cast<const float*>(h[3].data()),
+                          h[4].data(), nn, ol.data(), orr.data(), of.data(), ot.data(), ov.data()));
+      offs[t] = (uint32_t)packed.size();
+      for (uint32_t i = 0; i < nn; ++i) packed.push_back(ct_packed_node{ot[i], of[i], ol[i], ov[i]});
+    }
+    return add_forest(packed.data(), (uint32_t)packed.size(), offs.data(), T, F, C, fid);
+  }
+
+  static double pct(std::vector<double> v, double q) {
+    if (v.empty()) return 0.0;
+    const size_t k = std::min(v.size() - 1, (size_t)std::ceil(q * v.size()) - (q > 0 ? 1 : 0));
+    std::nth_element(v.begin(), v.begin() + k, v.end());
+    return v[k];
+  }
+
+  void stats(ct_server_stats* out) {
+    std::lock_guard<std::mutex> lk(mu);
+    std::vector<double> all = lat_small;
+    all.insert(all.end(), lat_large.begin(), lat_large.end());
+    out->requests = n_req;
+    out->rows = n_rows;
+    out->batches = n_batches;
+    out->fit_jobs = n_fit;
+    out->rejected = n_rejected;
+    out->p50_ms = pct(all, 0.50);
+    out->p99_ms = pct(all, 0.99);
+    out->p50_small_ms = pct(lat_small, 0.50);
+    out->p99_small_ms = pct(lat_small, 0.99);
+    out->p50_fit_ms = pct(lat_fit, 0.50);
+    out->p99_fit_ms = pct(lat_fit, 0.99);
+    out->max_ms = all.empty() ? 0.0 : *std::max_element(all.begin(), all.end());
+    out->wall_s = t_last > t_first ? t_last - t_first : 0.0;
+    out->rows_per_s = out->wall_s > 0 ? n_rows / out->wall_s : 0.0;
+    out->hbm_used_bytes = used;
+    out->hbm_budget_bytes = budget;
+  }
+
+  void reset_stats() {
+    std::lock_guard<std::mutex> lk(mu);
+    lat_small.clear();
+    lat_large.clear();
+    lat_fit.clear();
+    n_req = n_rows = n_batches = n_fit = n_rejected = 0;
+    t_first = t_last = 0;
+  }
+};
+
+}  // namespace ct
+
+using namespace ct;
+
+extern "C" {
+
+int ct_server_create(const ct_server_config* cfg, void** handle) {
+  CT_ARG_CHECK(cfg && handle, "NULL argument");
+  try {
+    auto s = std::make_unique<Server>();
+    const int st = s->init(cfg);
+    if (st != CT_OK) return st;  // destructor frees what init allocated
+    *handle = s.release();
+    return CT_OK;
+  } catch (const std::exception& e) {
+    set_last_error(std::string("server create: ") + e.what());
+    return CT_ERR_INTERNAL;
+  }
+}
+
+int ct_server_destroy(void* handle) {
+  delete reinterpret_cast<Server*>(handle);
+  return CT_OK;
+}
+
+int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
+                         uint32_t n_trees, uint32_t n_features, uint32_t n_classes, uint32_t* forest_id) {
+  CT_ARG_CHECK(handle, "NULL server");
+  return reinterpret_cast<Server*>(handle)->add_forest(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes,
+                                                        forest_id);
+}
+
+int ct_server_submit(void* handle, ct_request* req) {
+  CT_ARG_CHECK(handle, "NULL server");
+  return reinterpret_cast<Server*>(handle)->submit(req);
+}
+
+int ct_server_wait(void* handle, ct_request* req, double timeout_s) {
+  CT_ARG_CHECK(handle && req, "NULL argument");
+  return reinterpret_cast<Server*>(handle)->wait(req, timeout_s);
+}
+
+int ct_server_replay(void* handle, ct_request* reqs, uint32_t n, double timeout_s, ct_server_stats* stats) {
+  CT_ARG_CHECK(handle && (reqs || n == 0), "NULL argument");
+  Server* s = reinterpret_cast<Server*>(handle);
+  s->reset_stats();
+  const double t0 = now_s();
+  for (uint32_t i = 0; i < n; ++i) {
+    const double due = t0 + reqs[i].arrival_s;
+    while (now_s() < due) {
+      const double left = due - now_s();
+      if (left > 200e-6) std::this_thread::sleep_for(std::chrono::duration<double>(left - 100e-6));
+    }
+    const int st = s->submit(&reqs[i]);
+    if (st != CT_OK && st != CT_ERR_OOM) return st;
+  }
+  int worst = CT_OK;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!reqs[i].pending_) continue;
+    const int st = s->wait(&reqs[i], timeout_s);
+    if (st == CT_ERR_TIMEOUT) return st;
+    if (st != CT_OK) worst = st;
+  }
+  if (stats) s->stats(stats);
+  (void)worst;
+  return CT_OK;
+}
+
+int ct_server_get_stats(void* handle, ct_server_stats* out) {
+  CT_ARG_CHECK(handle && out, "NULL argument");
+  reinterpret_cast<Server*>(handle)->stats(out);
+  return CT_OK;
+}
+
+}  // extern "C"

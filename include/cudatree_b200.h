@@ -234,6 +234,69 @@ int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_
                const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
                uint32_t* votes, uint32_t* pred, void* stream);
 
+/* ----------------------------------------------------------- serving --- */
+/* No counterpart in the reference (its predict re-uploads X and every tree
+ * per call, base_tree.py:57-62).  A server keeps forests resident, batches
+ * the predict requests that have arrived into one multi-request launch per
+ * lane (small requests on a high-priority stream, large ones on a
+ * low-priority stream), runs small fit jobs on worker streams, and holds all
+ * its device memory inside an HBM budget. */
+enum { CT_REQ_PREDICT = 0, CT_REQ_FIT = 1 };
+
+typedef struct ct_server_config {
+  uint32_t max_batch_rows;   /* rows per large-request batch (0 = 131072)            */
+  uint32_t max_features;     /* largest feature count served (0 = 512)                */
+  uint32_t small_rows;       /* <= this many rows: high-priority lane (0 = 4096)      */
+  uint32_t fit_workers;      /* fit-job worker threads (0: fit jobs rejected)         */
+  uint32_t max_fit_rows;     /* largest fit job (0 = 20000)                           */
+  uint32_t max_fit_trees;    /* trees per fit job (0 = 10)                            */
+  uint64_t hbm_budget_bytes; /* device bytes the server may hold (0 = 80% of free)    */
+} ct_server_config;
+
+typedef struct ct_request {
+  double arrival_s;          /* ct_server_replay: seconds after the replay starts    */
+  uint32_t kind;             /* CT_REQ_PREDICT or CT_REQ_FIT                          */
+  uint32_t forest;           /* predict: resident forest id                           */
+  const float* x;            /* host [n_rows][n_features] (pinned: async copies)      */
+  const uint32_t* y;         /* fit: host [n_rows] class ids < n_classes              */
+  uint32_t* pred;            /* predict: host [n_rows] class ids (output)             */
+  uint32_t n_rows;
+  uint32_t n_features;       /* fit */
+  uint32_t n_classes;        /* fit */
+  uint32_t n_trees;          /* fit */
+  uint32_t max_features;     /* fit (0 = ceil(sqrt(n_features)))                      */
+  uint32_t status;           /* out: CT_OK or an error status                        */
+  uint64_t seed;             /* fit */
+  double latency_ms;         /* out: submit to completion                            */
+  uint32_t result_forest;    /* out (fit): id of the new resident forest              */
+  uint32_t pad_;
+  void* pending_;            /* internal */
+} ct_request;
+
+typedef struct ct_server_stats {
+  uint64_t requests, rows, batches, fit_jobs, rejected;
+  double p50_ms, p99_ms;               /* all predict requests                 */
+  double p50_small_ms, p99_small_ms;   /* predict requests of <= 4096 rows     */
+  double p50_fit_ms, p99_fit_ms;       /* fit jobs                              */
+  double max_ms, wall_s, rows_per_s;
+  uint64_t hbm_used_bytes, hbm_budget_bytes;
+} ct_server_stats;
+
+int ct_server_create(const ct_server_config* cfg, void** handle);
+int ct_server_destroy(void* handle);
+/* Copies a packed forest (host arrays, layout of ct_predict) to the device. */
+int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes,
+                         const uint32_t* tree_offset, uint32_t n_trees, uint32_t n_features,
+                         uint32_t n_classes, uint32_t* forest_id);
+/* Queues a request now; its buffers must stay valid until ct_server_wait. */
+int ct_server_submit(void* handle, ct_request* req);
+int ct_server_wait(void* handle, ct_request* req, double timeout_s);
+/* Submits each request at its arrival_s (open loop), waits for all, and
+ * fills stats for this replay. */
+int ct_server_replay(void* handle, ct_request* reqs, uint32_t n, double timeout_s,
+                     ct_server_stats* stats);
+int ct_server_get_stats(void* handle, ct_server_stats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,92 @@
+"""Serving engine: each request's predictions equal the plain predict path,
+alone and inside a mixed replay of concurrent requests of different sizes and
+forests; a fit job through the server yields the same forest as the Python
+fit with the same seed; admission rejects work that does not fit."""
+import numpy as np
+import pytest
+import torch
+from sklearn.datasets import load_digits, load_iris
+
+from cudatree_b200 import CudaTreeError, RandomForestClassifier
+from cudatree_b200.serving import ForestServer, pinned
+
+pytestmark = pytest.mark.gpu
+
+
+def _blobs(n, f, c, seed):
+    rng = np.random.default_rng(seed)
+    y = rng.integers(0, c, size=n)
+    means = rng.normal(scale=1.5, size=(c, f))
+    return (rng.normal(size=(n, f)) + means[y]).astype(np.float32), y
+
+
+@pytest.fixture(scope="module")
+def served(cuda_device):
+    xa, ya = load_digits().data.astype(np.float32), load_digits().target
+    xb, yb = _blobs(4000, 37, 9, 3)
+    fa = RandomForestClassifier(n_estimators=40, seed=1).fit(xa, ya)
+    fb = RandomForestClassifier(n_estimators=25, seed=2).fit(xb, yb)
+    srv = ForestServer(max_features=64, fit_workers=1, max_fit_rows=5000, max_fit_trees=8)
+    ida, idb = srv.add_forest(fa), srv.add_forest(fb)
+    yield srv, [(ida, fa, xa), (idb, fb, xb)]
+    srv.close()
+
+
+def test_single_requests_match_plain_predict(served):
+    srv, forests = served
+    for fid, forest, x in forests:
+        for n in (1, 7, 300, x.shape[0]):
+            np.testing.assert_array_equal(srv.predict(fid, x[:n]), forest.predict(x[:n]))
+
+
+def test_mixed_replay_matches_plain_predict(served):
+    srv, forests = served
+    rng = np.random.default_rng(7)
+    reqs, keep = [], []
+    t = 0.0
+    for i in range(200):
+        fid, forest, x = forests[i % 2]
+        n = int(np.exp(rng.uniform(0, np.log(x.shape[0]))))
+        lo = int(rng.integers(0, x.shape[0] - n + 1))
+        xp = pinned(x[lo:lo + n])
+        out = torch.zeros(n, dtype=torch.int32).pin_memory()
+        r = srv.predict_request(fid, xp, out)
+        t += rng.exponential(1 / 4000.0)
+        r.arrival_s = t
+        reqs.append(r)
+        keep.append((forest, x[lo:lo + n], xp, out))
+    stats = srv.replay(reqs)
+    assert stats["requests"] == 200 and stats["rejected"] == 0
+    assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    for r, (forest, xs, xp, out) in zip(reqs, keep):
+        assert r.status == 0
+        got = forest.compt_table[out.numpy().astype(np.int64)]
+        np.testing.assert_array_equal(got, forest.predict(xs))
+
+
+def test_fit_job_matches_python_fit(served):
+    srv, _ = served
+    x, y = _blobs(3000, 20, 6, 11)
+    xp, yp = pinned(x), pinned(y.astype(np.uint32))
+    req = srv.fit_request(xp, yp, n_classes=6, n_trees=5, seed=99, max_features=4)
+    srv.submit(req)
+    assert srv.wait(req) == 0
+    ref = RandomForestClassifier(n_estimators=5, max_features=4, seed=99).fit(x, y)
+    np.testing.assert_array_equal(srv.predict(req.result_forest, x), ref.predict(x))
+
+
+def test_admission_rejects_oversize(served):
+    srv, forests = served
+    fid, forest, x = forests[1]
+    big = np.zeros((200000, forest.n_features), dtype=np.float32)
+    with pytest.raises(CudaTreeError):
+        srv.predict(fid, big)
+    x2, y2 = _blobs(20000, 64, 3, 5)  # 4x the rows the fit arena was sized for
+    req = srv.fit_request(pinned(x2), pinned(y2.astype(np.uint32)), n_classes=3, n_trees=8, seed=1)
+    srv.submit(req)
+    assert srv.wait(req) == 2  # CT_ERR_OOM
+
+
+def test_budget_too_small_fails_cleanly(cuda_device):
+    with pytest.raises(CudaTreeError):
+        ForestServer(hbm_budget_bytes=1 << 20)
