@@ -268,6 +268,40 @@ def run_serving(args, x_cov, y_cov, seed):
     }
 
 
+def run_predict_only(args):
+    """Plain predict throughput on a forest fit to the covtype-shaped data:
+    65,536-row batches through ct_predict, with and without the vote table
+    (the table lets the launch walk L2-sized tree groups)."""
+    import torch
+
+    from cudatree_b200 import RandomForestClassifier, _lib, synthetic
+    x, y = synthetic.covtype_like()
+    forest = RandomForestClassifier(args.serve_trees, max_features=MAX_FEATURES, seed=77).fit(x, y)
+    nodes, offs = forest._device_forest()
+    xd = torch.from_numpy(x[:65536]).cuda()
+    out = torch.empty(xd.shape[0], dtype=torch.int32, device="cuda")
+    votes = torch.empty((xd.shape[0], forest.n_labels), dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream()
+    res = {}
+    for name, vt in (("no_vote_table", None), ("tree_groups", votes)):
+        def call():
+            _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(forest._trees), xd.data_ptr(),
+                      xd.shape[0], forest.n_features, forest.n_labels, None if vt is None else vt.data_ptr(),
+                      out.data_ptr(), st.cuda_stream)
+        for _ in range(args.warmup):
+            call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(args.steps):
+            call()
+        e1.record(st)
+        torch.cuda.synchronize()
+        res[name] = args.steps * xd.shape[0] / (e0.elapsed_time(e1) / 1000.0)
+    print(json.dumps({"predict_rows_per_s": res, "trees": args.serve_trees,
+                      "nodes": int(sum(t.n_nodes for t in forest._trees))}), flush=True)
+    return 0
+
+
 # --------------------------------------------------------------------- ours
 def run_ours(args, world, rank, local):
     import torch
@@ -409,6 +443,7 @@ def main():
     ap.add_argument("--skip-plain", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
+    ap.add_argument("--predict-only", action="store_true", help="time plain predict only (profiling runs)")
     ap.add_argument("--serve-trees", type=int, default=500)
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--rate", type=float, default=2000.0)
@@ -416,6 +451,9 @@ def main():
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         return run_reference(args, int(os.environ.get("WORLD_SIZE", "1")), rank)
+    if args.predict_only:
+        dist_setup(1)
+        return run_predict_only(args)
     world, rank, local = dist_setup(args.gpus)
     try:
         return run_ours(args, world, rank, local)

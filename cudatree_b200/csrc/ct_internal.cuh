@@ -306,21 +306,28 @@ int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
 View make_view(const ct_problem* p, const ct_lists* l);
 
 // One request of a multi-request predict launch (ct_predict.cu): blocks
-// [block0, block0 + ceil(n_rows / rows_per_block)) of the launch are its.
+// [block0, block0 + tiles * ceil(n_trees / group)) of the launch are its,
+// group-major; rows [row0, row0 + n_rows) of the batch are its.
 struct BatchReq {
   const ct_packed_node* nodes;
   const uint32_t* tree_off;
   const float* x;         // [n_rows][n_features] on the device
   uint32_t* pred;         // [n_rows] on the device
+  uint32_t* votes;        // [n_rows][n_classes] zeroed table (grouped requests)
   uint32_t n_rows;
   uint32_t n_features;
   uint32_t n_classes;
   uint32_t n_trees;
   uint32_t block0;
-  uint32_t pad[3];
+  uint32_t tiles;
+  uint32_t group;         // trees per group (>= n_trees: one group, no vote table)
+  uint32_t row0;
+  uint32_t pad[2];
 };
-int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t rows_per_block,
-                  uint32_t max_classes, cudaStream_t st);
+uint32_t predict_rows_per_block(uint32_t n_classes);
+uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes);
+int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
+                  uint32_t rows_per_block, uint32_t max_classes, bool any_grouped, cudaStream_t st);
 int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st);
 int check_problem(const ct_problem* p);
 

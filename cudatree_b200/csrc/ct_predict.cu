@@ -3,11 +3,18 @@
 // Reference: predict.cu:12-69 walks one tree per launch with one active lane
 // per warp, and random_forest.py:339-362 stacks per-tree labels on the host
 // and votes row by row in Python.  Here one launch walks every tree of the
-// packed forest for a tile of rows: the rows are staged in shared memory,
-// each thread walks several (row, tree) pairs interleaved so their node
-// loads overlap, and votes accumulate in a shared-memory histogram.  The
-// winner is the class with most votes, lowest class id on ties
-// (np.argmax(np.bincount(...)), random_forest.py:358).
+// packed forest:
+//   * blocks cover (row tile, tree group); the trees are cut into groups whose
+//     nodes fit comfortably in L2, and blocks are numbered group-major, so the
+//     blocks in flight walk one group and its nodes come from DRAM about once
+//     per launch instead of once per walk;
+//   * walks inside a block are numbered row-fastest: with 32 rows per tile a
+//     lane keeps one row and a warp's lanes walk the same tree (shared loads
+//     of its top levels); each thread keeps PRED_ILP walks in flight;
+//   * votes go to a shared-memory histogram; with several groups the
+//     histograms are added into a global [rows][classes] table and a second
+//     kernel takes the majority, lowest class on ties
+//     (np.argmax(np.bincount(...)), random_forest.py:358).
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -15,161 +22,208 @@ namespace ct {
 namespace {
 
 constexpr int PRED_THREADS = 256;
-constexpr int PRED_ILP = 4;
+constexpr int PRED_ILP = 8;
+constexpr uint32_t X_SMEM_BYTES = 32 * 1024;     // rows of x staged per block when they fit
+constexpr uint32_t HIST_SMEM_BYTES = 64 * 1024;  // vote histogram [rows][classes]
+constexpr size_t GROUP_L2_BYTES = 32ull << 20;   // node bytes of one tree group
 
-__global__ void __launch_bounds__(PRED_THREADS)
-k_predict(const ct_packed_node* __restrict__ nodes, const uint32_t* __restrict__ tree_off, uint32_t n_trees,
-          const float* __restrict__ x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
-          uint32_t rows_per_block, uint32_t x_in_smem, uint32_t* __restrict__ votes,
-          uint32_t* __restrict__ pred) {
-  extern __shared__ uint32_t smem[];
-  uint32_t* hist = smem;                                            // [rows_per_block][C]
-  float* xs = reinterpret_cast<float*>(smem + rows_per_block * n_classes);  // [rows][F]
-  const uint32_t row0 = blockIdx.x * rows_per_block;
-  const uint32_t rows = min(rows_per_block, n_rows - row0);
-  for (uint32_t i = threadIdx.x; i < rows_per_block * n_classes; i += blockDim.x) hist[i] = 0;
-  if (x_in_smem)
-    for (uint32_t i = threadIdx.x; i < rows * n_features; i += blockDim.x)
-      xs[i] = x[(size_t)row0 * n_features + i];
-  __syncthreads();
-  const uint64_t work = (uint64_t)rows * n_trees;
-  for (uint64_t w0 = (uint64_t)threadIdx.x * PRED_ILP; w0 < work; w0 += (uint64_t)blockDim.x * PRED_ILP) {
-    uint32_t idx[PRED_ILP], base[PRED_ILP], r[PRED_ILP];
-    bool live[PRED_ILP];
+// Walk every (row, tree) pair of a tile for trees [t_lo, t_lo + n_t) and add
+// the leaf votes to hist[row][class].  x is the tile's rows (shared memory when
+// staged, else global).  Walks are numbered w = t * rpb + row (row-fastest);
+// rpb is a power of two dividing blockDim.x, so a thread's row is fixed
+// (threadIdx.x % rpb) and its tree index advances by blockDim.x / rpb per walk.
+// Each thread keeps PRED_ILP walks in flight; their node loads are issued
+// together, then each walk steps or, at a leaf, votes and starts the thread's
+// next tree.
+__device__ __forceinline__ void walk_tile(const ct_packed_node* __restrict__ nodes,
+                                          const uint32_t* __restrict__ tree_off, uint32_t t_lo, uint32_t n_t,
+                                          const float* x, uint32_t n_features, uint32_t rows, uint32_t rpb,
+                                          uint32_t n_classes, uint32_t* hist) {
+  const uint32_t r = threadIdx.x & (rpb - 1);
+  if (r >= rows) return;
+  const uint32_t t_step = blockDim.x / rpb;
+  const float* xr = x + (size_t)r * n_features;
+  uint32_t* hr = hist + r * n_classes;
+  uint32_t t_next = threadIdx.x / rpb;
+  uint32_t base[PRED_ILP], pos[PRED_ILP];  // pos: absolute node index, NONE when the slot is idle
 #pragma unroll
-    for (int k = 0; k < PRED_ILP; ++k) {
-      const uint64_t w = w0 + k;
-      live[k] = w < work;
-      r[k] = live[k] ? (uint32_t)(w / n_trees) : 0;
-      const uint32_t t = live[k] ? (uint32_t)(w - (uint64_t)r[k] * n_trees) : 0;
-      base[k] = tree_off[t];
-      idx[k] = 0;
-    }
-    bool any = true;
-    while (any) {
-      any = false;
-#pragma unroll
-      for (int k = 0; k < PRED_ILP; ++k) {
-        if (!live[k]) continue;
-        const ct_packed_node nd = nodes[base[k] + idx[k]];
-        if (nd.left == 0) {
-          atomicAdd(&hist[r[k] * n_classes + nd.value], 1u);
-          live[k] = false;
-          continue;
-        }
-        const float xv = x_in_smem ? xs[r[k] * n_features + nd.feature]
-                                   : x[(size_t)(row0 + r[k]) * n_features + nd.feature];
-        idx[k] = (xv < nd.threshold) ? nd.left : nd.left + 1;
-        any = true;
-      }
+  for (int k = 0; k < PRED_ILP; ++k) {
+    pos[k] = NONE;
+    base[k] = 0;
+    if (t_next < n_t) {
+      base[k] = __ldg(tree_off + t_lo + t_next);
+      pos[k] = base[k];
+      t_next += t_step;
     }
   }
-  __syncthreads();
-  // one warp per row: argmax with lowest class on ties
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t rr = warp; rr < rows; rr += blockDim.x >> 5) {
-    uint32_t best = 0, bc = NONE;
-    for (uint32_t c = lane; c < n_classes; c += 32) {
-      const uint32_t v = hist[rr * n_classes + c];
-      if (votes) votes[(size_t)(row0 + rr) * n_classes + c] = v;
-      if (bc == NONE || v > best) {
-        best = v;
-        bc = c;
-      }
-    }
+  bool any = pos[0] != NONE;
+  while (any) {
+    ct_packed_node nd[PRED_ILP];
 #pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-      const uint32_t ob = __shfl_xor_sync(FULL, best, s);
-      const uint32_t oc = __shfl_xor_sync(FULL, bc, s);
-      if (oc != NONE && (bc == NONE || ob > best || (ob == best && oc < bc))) {
-        best = ob;
-        bc = oc;
+    for (int k = 0; k < PRED_ILP; ++k)
+      if (pos[k] != NONE) nd[k] = nodes[pos[k]];
+    any = false;
+#pragma unroll
+    for (int k = 0; k < PRED_ILP; ++k) {
+      if (pos[k] == NONE) continue;
+      any = true;
+      if (nd[k].left != 0) {
+        pos[k] = base[k] + nd[k].left + (xr[nd[k].feature] < nd[k].threshold ? 0u : 1u);
+      } else {
+        atomicAdd(hr + nd[k].value, 1u);
+        pos[k] = NONE;
+        if (t_next < n_t) {
+          base[k] = __ldg(tree_off + t_lo + t_next);
+          pos[k] = base[k];
+          t_next += t_step;
+        }
       }
     }
-    if (lane == 0 && pred) pred[row0 + rr] = bc;
   }
 }
 
-// One request of a batched predict launch.
+// Majority of a row's votes, lowest class on ties; warp-collective.
+__device__ __forceinline__ uint32_t warp_argmax(const uint32_t* votes, uint32_t n_classes, uint32_t* votes_out) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint32_t best = 0, bc = NONE;
+  for (uint32_t c = lane; c < n_classes; c += 32) {
+    const uint32_t v = votes[c];
+    if (votes_out) votes_out[c] = v;
+    if (bc == NONE || v > best) {
+      best = v;
+      bc = c;
+    }
+  }
+#pragma unroll
+  for (int s = 16; s > 0; s >>= 1) {
+    const uint32_t ob = __shfl_xor_sync(FULL, best, s);
+    const uint32_t oc = __shfl_xor_sync(FULL, bc, s);
+    if (oc != NONE && (bc == NONE || ob > best || (ob == best && oc < bc))) {
+      best = ob;
+      bc = oc;
+    }
+  }
+  return bc;
+}
+
+__device__ __forceinline__ const float* stage_rows(const float* x, uint32_t rows, uint32_t n_features,
+                                                   float* xs, bool fits) {
+  if (!fits) return x;
+  for (uint32_t i = threadIdx.x; i < rows * n_features; i += blockDim.x) xs[i] = __ldg(x + i);
+  return xs;
+}
+
+// One tile of one tree group: walk, then either vote (single group) or add
+// the histogram into the global vote table.
+__device__ __forceinline__ void tile_work(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t t_lo,
+                                          uint32_t n_t, bool single_group, const float* x, uint32_t n_rows,
+                                          uint32_t n_features, uint32_t n_classes, uint32_t rpb, uint32_t row0,
+                                          uint32_t* votes, uint32_t* pred, uint32_t* smem) {
+  uint32_t* hist = smem;
+  float* xs = reinterpret_cast<float*>(smem + rpb * n_classes);
+  const uint32_t rows = min(rpb, n_rows - row0);
+  for (uint32_t i = threadIdx.x; i < rpb * n_classes; i += blockDim.x) hist[i] = 0;
+  const bool fits = (size_t)rpb * n_features * sizeof(float) <= X_SMEM_BYTES;
+  const float* xt = stage_rows(x + (size_t)row0 * n_features, rows, n_features, xs, fits);
+  __syncthreads();
+  walk_tile(nodes, tree_off, t_lo, n_t, xt, n_features, rows, rpb, n_classes, hist);
+  __syncthreads();
+  if (single_group) {
+    const uint32_t warp = threadIdx.x >> 5;
+    for (uint32_t rr = warp; rr < rows; rr += blockDim.x >> 5) {
+      const uint32_t c = warp_argmax(hist + rr * n_classes, n_classes,
+                                     votes ? votes + (size_t)(row0 + rr) * n_classes : nullptr);
+      if ((threadIdx.x & 31) == 0 && pred) pred[row0 + rr] = c;
+    }
+  } else {
+    for (uint32_t i = threadIdx.x; i < rows * n_classes; i += blockDim.x)
+      if (hist[i]) atomicAdd(votes + (size_t)row0 * n_classes + i, hist[i]);
+  }
+}
+
+__global__ void __launch_bounds__(PRED_THREADS, 4)
+k_predict(const ct_packed_node* __restrict__ nodes, const uint32_t* __restrict__ tree_off, uint32_t n_trees,
+          uint32_t group, uint32_t tiles, const float* __restrict__ x, uint32_t n_rows, uint32_t n_features,
+          uint32_t n_classes, uint32_t rpb, uint32_t* __restrict__ votes, uint32_t* __restrict__ pred) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t g = blockIdx.x / tiles, tile = blockIdx.x - g * tiles;  // group-major
+  const uint32_t t_lo = g * group;
+  tile_work(nodes, tree_off, t_lo, min(group, n_trees - t_lo), group >= n_trees, x, n_rows, n_features, n_classes,
+            rpb, tile * rpb, votes, pred, smem);
+}
+
+__global__ void k_vote_rows(const uint32_t* __restrict__ votes, uint32_t n_rows, uint32_t n_classes,
+                            uint32_t* __restrict__ pred) {
+  const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n_rows) return;
+  const uint32_t c = warp_argmax(votes + (size_t)row * n_classes, n_classes, nullptr);
+  if ((threadIdx.x & 31) == 0 && pred) pred[row] = c;
+}
+
+uint32_t group_size(uint32_t n_trees, uint64_t n_nodes) {
+  const uint64_t per_tree = (n_nodes * sizeof(ct_packed_node) + n_trees - 1) / n_trees;
+  uint64_t g = per_tree ? GROUP_L2_BYTES / per_tree : n_trees;
+  if (g < 1) g = 1;
+  return (uint32_t)std::min<uint64_t>(g, n_trees);
+}
+
 }  // namespace
 
-__global__ void __launch_bounds__(PRED_THREADS)
-k_predict_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, uint32_t rows_per_block) {
+// Rows per tile: 32 when the [rows][classes] histogram fits, fewer for many classes.
+uint32_t predict_rows_per_block(uint32_t n_classes) {
+  uint32_t r = 32;
+  while (r > 1 && (size_t)r * n_classes * sizeof(uint32_t) > HIST_SMEM_BYTES) r >>= 1;
+  return r;
+}
+
+uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes) { return group_size(n_trees, n_nodes); }
+
+__global__ void __launch_bounds__(PRED_THREADS, 4)
+k_predict_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, uint32_t rpb, uint32_t max_classes) {
   extern __shared__ uint32_t smem[];
-  // request of this block: the last request whose first block is <= blockIdx.x
-  uint32_t lo = 0, hi = n_req;
+  uint32_t lo = 0, hi = n_req;  // the last request whose first block is <= blockIdx.x
   while (hi - lo > 1) {
     const uint32_t mid = (lo + hi) / 2;
     if (reqs[mid].block0 <= blockIdx.x) lo = mid; else hi = mid;
   }
   const BatchReq rq = reqs[lo];
-  const uint32_t n_classes = rq.n_classes, n_features = rq.n_features, n_trees = rq.n_trees;
-  uint32_t* hist = smem;
-  const uint32_t row0 = (blockIdx.x - rq.block0) * rows_per_block;
-  const uint32_t rows = min(rows_per_block, rq.n_rows - row0);
-  for (uint32_t i = threadIdx.x; i < rows_per_block * n_classes; i += blockDim.x) hist[i] = 0;
-  __syncthreads();
-  const float* x = rq.x + (size_t)row0 * n_features;
-  const ct_packed_node* __restrict__ nodes = rq.nodes;
-  const uint64_t work = (uint64_t)rows * n_trees;
-  for (uint64_t w0 = (uint64_t)threadIdx.x * PRED_ILP; w0 < work; w0 += (uint64_t)blockDim.x * PRED_ILP) {
-    uint32_t idx[PRED_ILP], base[PRED_ILP], r[PRED_ILP];
-    bool live[PRED_ILP];
-#pragma unroll
-    for (int k = 0; k < PRED_ILP; ++k) {
-      const uint64_t w = w0 + k;
-      live[k] = w < work;
-      r[k] = live[k] ? (uint32_t)(w / n_trees) : 0;
-      const uint32_t t = live[k] ? (uint32_t)(w - (uint64_t)r[k] * n_trees) : 0;
-      base[k] = rq.tree_off[t];
-      idx[k] = 0;
-    }
-    bool any = true;
-    while (any) {
-      any = false;
-#pragma unroll
-      for (int k = 0; k < PRED_ILP; ++k) {
-        if (!live[k]) continue;
-        const ct_packed_node nd = nodes[base[k] + idx[k]];
-        if (nd.left == 0) {
-          atomicAdd(&hist[r[k] * n_classes + nd.value], 1u);
-          live[k] = false;
-          continue;
-        }
-        idx[k] = (__ldg(x + (size_t)r[k] * n_features + nd.feature) < nd.threshold) ? nd.left : nd.left + 1;
-        any = true;
-      }
-    }
-  }
-  __syncthreads();
-  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (uint32_t rr = warp; rr < rows; rr += blockDim.x >> 5) {
-    uint32_t best = 0, bc = NONE;
-    for (uint32_t c = lane; c < n_classes; c += 32) {
-      const uint32_t v = hist[rr * n_classes + c];
-      if (bc == NONE || v > best) {
-        best = v;
-        bc = c;
-      }
-    }
-#pragma unroll
-    for (int s2 = 16; s2 > 0; s2 >>= 1) {
-      const uint32_t ob = __shfl_xor_sync(FULL, best, s2);
-      const uint32_t oc = __shfl_xor_sync(FULL, bc, s2);
-      if (oc != NONE && (bc == NONE || ob > best || (ob == best && oc < bc))) {
-        best = ob;
-        bc = oc;
-      }
-    }
-    if (lane == 0) rq.pred[row0 + rr] = bc;
-  }
+  const uint32_t local = blockIdx.x - rq.block0;
+  const uint32_t g = local / rq.tiles, tile = local - g * rq.tiles;
+  const uint32_t t_lo = g * rq.group;
+  (void)max_classes;
+  tile_work(rq.nodes, rq.tree_off, t_lo, min(rq.group, rq.n_trees - t_lo), rq.group >= rq.n_trees, rq.x,
+            rq.n_rows, rq.n_features, rq.n_classes, rpb, tile * rpb, rq.votes, rq.pred, smem);
 }
 
-int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t rows_per_block,
-                  uint32_t max_classes, cudaStream_t st) {
+// Majority vote of the rows of requests whose trees were split into groups.
+__global__ void k_vote_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, uint32_t total_rows) {
+  const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= total_rows) return;
+  uint32_t lo = 0, hi = n_req;
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) / 2;
+    if (reqs[mid].row0 <= row) lo = mid; else hi = mid;
+  }
+  const BatchReq rq = reqs[lo];
+  if (rq.group >= rq.n_trees) return;  // voted in the walk kernel
+  const uint32_t r = row - rq.row0;
+  const uint32_t c = warp_argmax(rq.votes + (size_t)r * rq.n_classes, rq.n_classes, nullptr);
+  if ((threadIdx.x & 31) == 0) rq.pred[r] = c;
+}
+
+int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
+                  uint32_t rows_per_block, uint32_t max_classes, bool any_grouped, cudaStream_t st) {
   if (n_req == 0 || total_blocks == 0) return CT_OK;
-  const size_t smem = (size_t)rows_per_block * max_classes * sizeof(uint32_t);
-  k_predict_batch<<<total_blocks, PRED_THREADS, smem, st>>>(reqs_dev, n_req, rows_per_block);
+  // histogram for the batch's largest class count, then the staged rows of x
+  const size_t smem = (size_t)rows_per_block * max_classes * sizeof(uint32_t) + X_SMEM_BYTES;
+  static bool configured = false;
+  if (!configured) {
+    const int most = (int)(HIST_SMEM_BYTES + X_SMEM_BYTES);
+    CT_CUDA_TRY(cudaFuncSetAttribute(k_predict_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+    configured = true;
+  }
+  k_predict_batch<<<total_blocks, PRED_THREADS, smem, st>>>(reqs_dev, n_req, rows_per_block, max_classes);
+  if (any_grouped) k_vote_batch<<<ceil_div(total_rows, 8), 256, 0, st>>>(reqs_dev, n_req, total_rows);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
@@ -181,14 +235,32 @@ int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_tr
   CT_ARG_CHECK(n_trees >= 1 && n_features >= 1, "predict: empty forest or no features");
   CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "predict: n_classes out of range");
   if (n_rows == 0) return CT_OK;
-  uint32_t rpb = 8;
-  size_t hist_bytes = (size_t)rpb * n_classes * sizeof(uint32_t);
-  size_t x_bytes = (size_t)rpb * n_features * sizeof(float);
-  uint32_t x_in_smem = (hist_bytes + x_bytes) <= 48 * 1024 ? 1u : 0u;
-  const size_t smem = hist_bytes + (x_in_smem ? x_bytes : 0);
-  const uint32_t blocks = ceil_div(n_rows, rpb);
-  k_predict<<<blocks, PRED_THREADS, smem, st>>>(nodes, tree_off, n_trees, x, n_rows, n_features, n_classes, rpb,
-                                                x_in_smem, votes, pred);
+  const uint32_t rpb = predict_rows_per_block(n_classes);
+  const uint32_t tiles = ceil_div(n_rows, rpb);
+  // Tree groups need the vote table; without one every block walks all
+  // trees.  The forest's size is estimated from the last tree's offset (one
+  // 4-byte read, only for batches large enough to amortize it).
+  uint32_t group = n_trees;
+  if (votes && n_trees >= 16 && n_rows >= 1024) {
+    uint32_t last_off = 0;
+    CT_CUDA_TRY(cudaMemcpyAsync(&last_off, tree_off + n_trees - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    group = group_size(n_trees, (uint64_t)last_off * n_trees / (n_trees - 1));
+  }
+  const uint32_t groups = ceil_div(n_trees, group);
+  const size_t hist_bytes = (size_t)rpb * n_classes * sizeof(uint32_t);
+  const size_t x_bytes = (size_t)rpb * n_features * sizeof(float);
+  const size_t smem = hist_bytes + (x_bytes <= X_SMEM_BYTES ? x_bytes : 0);
+  static bool configured = false;
+  if (!configured) {
+    const int most = (int)(HIST_SMEM_BYTES + X_SMEM_BYTES);
+    CT_CUDA_TRY(cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
+    configured = true;
+  }
+  if (groups > 1) CT_CUDA_TRY(cudaMemsetAsync(votes, 0, (size_t)n_rows * n_classes * sizeof(uint32_t), st));
+  k_predict<<<tiles * groups, PRED_THREADS, smem, st>>>(nodes, tree_off, n_trees, group, tiles, x, n_rows,
+                                                         n_features, n_classes, rpb, votes, pred);
+  if (groups > 1) k_vote_rows<<<ceil_div(n_rows, 8), 256, 0, st>>>(votes, n_rows, n_classes, pred);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

@@ -47,7 +47,6 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
 
 namespace {
 
-constexpr uint32_t PRED_ROWS_PER_BLOCK = 8;
 
 double now_s() {
   using namespace std::chrono;
@@ -58,6 +57,7 @@ struct Forest {
   ct_packed_node* nodes = nullptr;
   uint32_t* off = nullptr;
   uint32_t n_nodes = 0, n_trees = 0, n_features = 0, n_classes = 0;
+  uint32_t group = 0;  // trees per L2-sized group
   size_t bytes = 0;
 };
 
@@ -70,6 +70,7 @@ struct Job {
 struct Slot {
   float* x_dev = nullptr;
   uint32_t* pred_dev = nullptr;
+  uint32_t* votes_dev = nullptr;  // [rows][classes] tables of grouped requests
   BatchReq* req_dev = nullptr;
   BatchReq* req_host = nullptr;  // pinned
   cudaEvent_t ev = nullptr;
@@ -132,6 +133,7 @@ class Server {
     if (!cfg.small_rows) cfg.small_rows = 4096;
     if (!cfg.max_fit_rows) cfg.max_fit_rows = 20000;
     if (!cfg.max_fit_trees) cfg.max_fit_trees = 10;
+    if (!cfg.max_classes) cfg.max_classes = 64;
     CT_CUDA_TRY(cudaGetDevice(&device));
     size_t free_b = 0, total_b = 0;
     CT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
@@ -146,6 +148,7 @@ class Server {
       for (auto& s : ln.slot) {
         CT_TRY(take(ln.cap_floats * sizeof(float), (void**)&s.x_dev));
         CT_TRY(take(ln.cap_rows * sizeof(uint32_t), (void**)&s.pred_dev));
+        CT_TRY(take(ln.cap_rows * cfg.max_classes * sizeof(uint32_t), (void**)&s.votes_dev));
         CT_TRY(take(4096 * sizeof(BatchReq), (void**)&s.req_dev));
         CT_CUDA_TRY(cudaMallocHost((void**)&s.req_host, 4096 * sizeof(BatchReq)));
         CT_CUDA_TRY(cudaEventCreateWithFlags(&s.ev, cudaEventDisableTiming));
@@ -213,6 +216,7 @@ class Server {
       for (auto& s : ln.slot) {
         if (s.x_dev) cudaFree(s.x_dev);
         if (s.pred_dev) cudaFree(s.pred_dev);
+        if (s.votes_dev) cudaFree(s.votes_dev);
         if (s.req_dev) cudaFree(s.req_dev);
         if (s.req_host) cudaFreeHost(s.req_host);
         if (s.ev) cudaEventDestroy(s.ev);
@@ -241,6 +245,7 @@ class Server {
     f.n_features = n_features;
     f.n_classes = n_classes;
     f.bytes = (size_t)n_nodes * sizeof(ct_packed_node) + (size_t)n_trees * 4;
+    f.group = n_classes <= cfg.max_classes ? predict_group_size(n_trees, n_nodes) : n_trees;
     CT_CUDA_TRY(cudaSetDevice(device));
     CT_TRY(take((size_t)n_nodes * sizeof(ct_packed_node), (void**)&f.nodes));
     CT_TRY(take((size_t)n_trees * 4, (void**)&f.off));
@@ -379,17 +384,22 @@ class Server {
   }
 
   void launch(Lane& ln, Slot& s, std::vector<Job*>& batch) {
-    uint64_t xoff = 0, roff = 0;
+    uint64_t xoff = 0, roff = 0, voff = 0;
     uint32_t blocks = 0, max_c = 1;
-    std::vector<std::pair<Job*, uint64_t>> outs;
+    bool grouped = false;
+    std::vector<Forest> fs(batch.size());
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      for (size_t i = 0; i < batch.size(); ++i) {
+        fs[i] = forests[batch[i]->req->forest];
+        max_c = std::max(max_c, fs[i].n_classes);
+      }
+    }
+    const uint32_t rpb = predict_rows_per_block(max_c);
     int err = 0;
     for (size_t i = 0; i < batch.size(); ++i) {
       ct_request* r = batch[i]->req;
-      Forest f;
-      {
-        std::lock_guard<std::mutex> lk(mu);
-        f = forests[r->forest];
-      }
+      const Forest& f = fs[i];
       BatchReq& br = s.req_host[i];
       br.nodes = f.nodes;
       br.tree_off = f.off;
@@ -400,23 +410,34 @@ class Server {
       br.n_classes = f.n_classes;
       br.n_trees = f.n_trees;
       br.block0 = blocks;
-      blocks += ceil_div(r->n_rows, PRED_ROWS_PER_BLOCK);
-      max_c = std::max(max_c, f.n_classes);
+      br.tiles = ceil_div(r->n_rows, rpb);
+      br.group = f.group;
+      br.row0 = (uint32_t)roff;
+      br.votes = nullptr;  // a single-group request votes directly and must not touch the table
+      if (f.group < f.n_trees) {
+        grouped = true;
+        br.votes = s.votes_dev + voff;
+        voff += (uint64_t)r->n_rows * f.n_classes;
+      }
+      blocks += br.tiles * ceil_div(f.n_trees, f.group);
       if (cudaMemcpyAsync(s.x_dev + xoff, r->x, (size_t)r->n_rows * f.n_features * sizeof(float),
                           cudaMemcpyHostToDevice, ln.st) != cudaSuccess)
         err = 1;
-      outs.push_back({batch[i], roff});
       xoff += (uint64_t)r->n_rows * f.n_features;
       roff += r->n_rows;
     }
+    if (voff && cudaMemsetAsync(s.votes_dev, 0, voff * sizeof(uint32_t), ln.st) != cudaSuccess) err = 1;
     if (cudaMemcpyAsync(s.req_dev, s.req_host, batch.size() * sizeof(BatchReq), cudaMemcpyHostToDevice, ln.st) !=
         cudaSuccess)
       err = 1;
-    if (predict_batch(s.req_dev, (uint32_t)batch.size(), blocks, PRED_ROWS_PER_BLOCK, max_c, ln.st) != CT_OK) err = 1;
-    for (auto& o : outs)
-      if (cudaMemcpyAsync(o.first->req->pred, s.pred_dev + o.second, (size_t)o.first->req->n_rows * 4,
-                          cudaMemcpyDeviceToHost, ln.st) != cudaSuccess)
+    if (predict_batch(s.req_dev, (uint32_t)batch.size(), blocks, (uint32_t)roff, rpb, max_c, grouped, ln.st) != CT_OK)
+      err = 1;
+    for (size_t i = 0; i < batch.size(); ++i) {
+      ct_request* r = batch[i]->req;
+      if (cudaMemcpyAsync(r->pred, s.pred_dev + s.req_host[i].row0, (size_t)r->n_rows * 4, cudaMemcpyDeviceToHost,
+                          ln.st) != cudaSuccess)
         err = 1;
+    }
     cudaEventRecord(s.ev, ln.st);
     s.launched = now_s();
     s.jobs = batch;

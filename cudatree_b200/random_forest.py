@@ -111,10 +111,11 @@ def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_vot
     nodes = packed if isinstance(packed, torch.Tensor) else _to_dev(packed, dev)
     offs = offsets if isinstance(offsets, torch.Tensor) else _to_dev(offsets.astype(np.uint32), dev)
     xd = torch.from_numpy(x).to(dev)
-    out = torch.empty((n, n_classes) if want_votes else (n,), dtype=torch.int32, device=dev)
+    votes = torch.empty((n, n_classes), dtype=torch.int32, device=dev)  # also the tree-group vote table
+    pred = torch.empty((n,), dtype=torch.int32, device=dev)
     _lib.call("ct_predict", _ptr(nodes), _ptr(offs), n_trees, _ptr(xd), n, n_features, n_classes,
-              _ptr(out) if want_votes else None, None if want_votes else _ptr(out), _stream())
-    return out.cpu().numpy().view(np.uint32)
+              _ptr(votes), _ptr(pred), _stream())
+    return (votes if want_votes else pred).cpu().numpy().view(np.uint32)
 
 
 class RandomForestClassifier:

@@ -22,7 +22,7 @@ CT_REQ_FIT = 1
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch_rows", C.c_uint32), ("max_features", C.c_uint32), ("small_rows", C.c_uint32),
                 ("fit_workers", C.c_uint32), ("max_fit_rows", C.c_uint32), ("max_fit_trees", C.c_uint32),
-                ("hbm_budget_bytes", C.c_uint64)]
+                ("max_classes", C.c_uint32), ("reserved", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
 
 
 class Request(C.Structure):
@@ -56,11 +56,11 @@ class ForestServer:
     """Resident forests + request loop on the current CUDA device."""
 
     def __init__(self, max_batch_rows=0, max_features=512, small_rows=4096, fit_workers=2,
-                 max_fit_rows=20000, max_fit_trees=10, hbm_budget_bytes=0):
+                 max_fit_rows=20000, max_fit_trees=10, hbm_budget_bytes=0, max_classes=64):
         _lib.load()
         torch.cuda.init()
         cfg = ServerConfig(max_batch_rows, max_features, small_rows, fit_workers, max_fit_rows,
-                           max_fit_trees, hbm_budget_bytes)
+                           max_fit_trees, max_classes, 0, hbm_budget_bytes)
         h = C.c_void_p()
         _lib.call("ct_server_create", C.byref(cfg), C.byref(h))
         self._h = h

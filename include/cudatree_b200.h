@@ -250,6 +250,9 @@ typedef struct ct_server_config {
   uint32_t fit_workers;      /* fit-job worker threads (0: fit jobs rejected)         */
   uint32_t max_fit_rows;     /* largest fit job (0 = 20000)                           */
   uint32_t max_fit_trees;    /* trees per fit job (0 = 10)                            */
+  uint32_t max_classes;      /* forests with more classes are walked in one tree group
+                                (0 = 64)                                              */
+  uint32_t reserved;
   uint64_t hbm_budget_bytes; /* device bytes the server may hold (0 = 80% of free)    */
 } ct_server_config;
 

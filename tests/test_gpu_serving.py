@@ -90,3 +90,40 @@ def test_admission_rejects_oversize(served):
 def test_budget_too_small_fails_cleanly(cuda_device):
     with pytest.raises(CudaTreeError):
         ForestServer(hbm_budget_bytes=1 << 20)
+
+
+def test_tree_groups_match_oracle_and_server(cuda_device):
+    """Large trees (noise labels, fully grown) split the forest into several
+    L2-sized tree groups; grouped votes must equal the oracle's votes, and
+    the server's batched path must equal the plain path."""
+    from oracle import cudatree_oracle as O
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=(200000, 8)).astype(np.float32)
+    y = rng.integers(0, 5, size=200000)
+    forest = RandomForestClassifier(n_estimators=40, seed=8).fit(x, y)
+    per_tree = sum(t.n_nodes for t in forest._trees) * 16 / 40
+    assert 32 * 2**20 / per_tree < 40, "test forest must need several tree groups"
+    xs = x[:3000]
+    ref = O.Forest(trees=[O.Tree(t.left_children, t.right_children, t.feature_idx_array,
+                                 t.feature_threshold_array, t.values_array.astype(np.int64))
+                          for t in forest._trees], classes=forest.compt_table, n_features=8)
+    np.testing.assert_array_equal(forest.predict(xs), O.predict(ref, xs))
+    np.testing.assert_array_equal(forest.predict_proba(xs), O.predict_proba(ref, xs))
+    srv = ForestServer(max_features=16, fit_workers=0)
+    fid = srv.add_forest(forest)
+    small = RandomForestClassifier(n_estimators=20, seed=9).fit(x[:5000], y[:5000])
+    sid = srv.add_forest(small)
+    reqs, keep = [], []
+    for i, n in enumerate([1, 2000, 37, 5000, 4096, 9000, 3]):
+        f, fi = (forest, fid) if i % 2 == 0 else (small, sid)
+        xp = pinned(x[i * 10000:i * 10000 + n])
+        out = torch.zeros(n, dtype=torch.int32).pin_memory()
+        r = srv.predict_request(fi, xp, out)
+        r.arrival_s = 0.0
+        reqs.append(r)
+        keep.append((f, x[i * 10000:i * 10000 + n], out, xp))  # buffers live until completion
+    srv.replay(reqs)
+    for r, (f, xs2, out, _) in zip(reqs, keep):
+        assert r.status == 0
+        np.testing.assert_array_equal(f.compt_table[out.numpy().astype(np.int64)], f.predict(xs2))
+    srv.close()
