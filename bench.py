@@ -218,7 +218,7 @@ def run_serving(args, x_cov, y_cov, seed):
     rows_total = 0
     plans = []
     for i in range(n_req):
-        if rng.random() < 0.05:
+        if rng.random() < args.fit_frac:
             n = int(np.exp(rng.uniform(np.log(500), np.log(20000))))
             plans.append(("fit", n))
         else:
@@ -257,7 +257,7 @@ def run_serving(args, x_cov, y_cov, seed):
     return {
         "workload": f"{args.serve_trees}-tree covtype-shaped forest + 8 forests (50-500 trees, 16-512 features); "
                     f"Poisson {args.rate:g} req/s for {args.serve_seconds:g} s, rows log-uniform [1, 65536], "
-                    "5% fit jobs (<= 20000 rows, 10 trees)",
+                    f"{100 * args.fit_frac:g}% fit jobs (<= 20000 rows, 10 trees)",
         "requests": int(stats["requests"]), "fit_jobs": int(stats["fit_jobs"]), "rejected": int(stats["rejected"]),
         "rows_per_s": stats["rows_per_s"], "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"],
         "p50_ms_le4096_rows": stats["p50_small_ms"], "p99_ms_le4096_rows": stats["p99_small_ms"],
@@ -447,6 +447,8 @@ def main():
     ap.add_argument("--serve-trees", type=int, default=500)
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--rate", type=float, default=2000.0)
+    ap.add_argument("--fit-frac", type=float, default=0.05, help="fraction of serving requests that are fit jobs")
+    ap.add_argument("--serving-only", action="store_true", help="run the serving workload alone (profiling runs)")
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
@@ -454,6 +456,12 @@ def main():
     if args.predict_only:
         dist_setup(1)
         return run_predict_only(args)
+    if args.serving_only:
+        dist_setup(1)
+        from cudatree_b200 import synthetic
+        x, y = synthetic.covtype_like()
+        print(json.dumps({"predict": run_serving(args, x, y, 1000)}), flush=True)
+        return 0
     world, rank, local = dist_setup(args.gpus)
     try:
         return run_ours(args, world, rank, local)

@@ -124,6 +124,7 @@ PROTOTYPES = {
     "ct_server_create": (C.c_int, [P, P]),
     "ct_server_destroy": (C.c_int, [P]),
     "ct_server_add_forest": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
+    "ct_server_remove_forest": (C.c_int, [P, C.c_uint32]),
     "ct_server_submit": (C.c_int, [P, P]),
     "ct_server_wait": (C.c_int, [P, P, C.c_double]),
     "ct_server_replay": (C.c_int, [P, P, C.c_uint32, C.c_double, P]),

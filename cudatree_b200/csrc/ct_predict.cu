@@ -28,8 +28,10 @@ constexpr uint32_t HIST_SMEM_BYTES = 64 * 1024;  // vote histogram [rows][classe
 constexpr size_t GROUP_L2_BYTES = 32ull << 20;   // node bytes of one tree group
 
 // Walk every (row, tree) pair of a tile for trees [t_lo, t_lo + n_t) and add
-// the leaf votes to hist[row][class].  x is the tile's rows (shared memory when
-// staged, else global).  Walks are numbered w = t * rpb + row (row-fastest);
+// the leaf votes to hist[row][class].  Feature f of tile row r is
+// x[r * row_stride + f * feat_stride]: the staged shared-memory tile is
+// feature-major (row_stride 1, feat_stride rpb), so the lanes of a warp, one
+// row each, read distinct banks; unstaged rows are read from global memory.  Walks are numbered w = t * rpb + row (row-fastest);
 // rpb is a power of two dividing blockDim.x, so a thread's row is fixed
 // (threadIdx.x % rpb) and its tree index advances by blockDim.x / rpb per walk.
 // Each thread keeps PRED_ILP walks in flight; their node loads are issued
@@ -37,12 +39,12 @@ constexpr size_t GROUP_L2_BYTES = 32ull << 20;   // node bytes of one tree group
 // next tree.
 __device__ __forceinline__ void walk_tile(const ct_packed_node* __restrict__ nodes,
                                           const uint32_t* __restrict__ tree_off, uint32_t t_lo, uint32_t n_t,
-                                          const float* x, uint32_t n_features, uint32_t rows, uint32_t rpb,
-                                          uint32_t n_classes, uint32_t* hist) {
+                                          const float* x, uint32_t row_stride, uint32_t feat_stride,
+                                          uint32_t rows, uint32_t rpb, uint32_t n_classes, uint32_t* hist) {
   const uint32_t r = threadIdx.x & (rpb - 1);
   if (r >= rows) return;
   const uint32_t t_step = blockDim.x / rpb;
-  const float* xr = x + (size_t)r * n_features;
+  const float* xr = x + (size_t)r * row_stride;
   uint32_t* hr = hist + r * n_classes;
   uint32_t t_next = threadIdx.x / rpb;
   uint32_t base[PRED_ILP], pos[PRED_ILP];  // pos: absolute node index, NONE when the slot is idle
@@ -58,19 +60,19 @@ __device__ __forceinline__ void walk_tile(const ct_packed_node* __restrict__ nod
   }
   bool any = pos[0] != NONE;
   while (any) {
-    ct_packed_node nd[PRED_ILP];
+    uint4 nd[PRED_ILP];  // {threshold bits, feature, left, value}: one 16-byte load per node
 #pragma unroll
     for (int k = 0; k < PRED_ILP; ++k)
-      if (pos[k] != NONE) nd[k] = nodes[pos[k]];
+      if (pos[k] != NONE) nd[k] = __ldg(reinterpret_cast<const uint4*>(nodes) + pos[k]);
     any = false;
 #pragma unroll
     for (int k = 0; k < PRED_ILP; ++k) {
       if (pos[k] == NONE) continue;
       any = true;
-      if (nd[k].left != 0) {
-        pos[k] = base[k] + nd[k].left + (xr[nd[k].feature] < nd[k].threshold ? 0u : 1u);
+      if (nd[k].z != 0) {
+        pos[k] = base[k] + nd[k].z + (xr[nd[k].y * feat_stride] < __uint_as_float(nd[k].x) ? 0u : 1u);
       } else {
-        atomicAdd(hr + nd[k].value, 1u);
+        atomicAdd(hr + nd[k].w, 1u);
         pos[k] = NONE;
         if (t_next < n_t) {
           base[k] = __ldg(tree_off + t_lo + t_next);
@@ -106,11 +108,14 @@ __device__ __forceinline__ uint32_t warp_argmax(const uint32_t* votes, uint32_t 
   return bc;
 }
 
-__device__ __forceinline__ const float* stage_rows(const float* x, uint32_t rows, uint32_t n_features,
-                                                   float* xs, bool fits) {
-  if (!fits) return x;
-  for (uint32_t i = threadIdx.x; i < rows * n_features; i += blockDim.x) xs[i] = __ldg(x + i);
-  return xs;
+// Stage a tile's rows feature-major: xs[f * rpb + r] = x[r][f] (row-fastest,
+// so the shared-memory stores are conflict-free).
+__device__ __forceinline__ void stage_rows(const float* x, uint32_t rows, uint32_t rpb, uint32_t n_features,
+                                           float* xs) {
+  for (uint32_t i = threadIdx.x; i < rows * n_features; i += blockDim.x) {
+    const uint32_t f = i / rows, r = i - f * rows;
+    xs[f * rpb + r] = __ldg(x + (size_t)r * n_features + f);
+  }
 }
 
 // One tile of one tree group: walk, then either vote (single group) or add
@@ -124,9 +129,12 @@ __device__ __forceinline__ void tile_work(const ct_packed_node* nodes, const uin
   const uint32_t rows = min(rpb, n_rows - row0);
   for (uint32_t i = threadIdx.x; i < rpb * n_classes; i += blockDim.x) hist[i] = 0;
   const bool fits = (size_t)rpb * n_features * sizeof(float) <= X_SMEM_BYTES;
-  const float* xt = stage_rows(x + (size_t)row0 * n_features, rows, n_features, xs, fits);
+  if (fits) stage_rows(x + (size_t)row0 * n_features, rows, rpb, n_features, xs);
   __syncthreads();
-  walk_tile(nodes, tree_off, t_lo, n_t, xt, n_features, rows, rpb, n_classes, hist);
+  if (fits)
+    walk_tile(nodes, tree_off, t_lo, n_t, xs, 1, rpb, rows, rpb, n_classes, hist);
+  else
+    walk_tile(nodes, tree_off, t_lo, n_t, x + (size_t)row0 * n_features, n_features, 1, rows, rpb, n_classes, hist);
   __syncthreads();
   if (single_group) {
     const uint32_t warp = threadIdx.x >> 5;
@@ -232,6 +240,7 @@ int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_tr
             uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
             cudaStream_t st) {
   CT_ARG_CHECK(nodes && tree_off && x, "predict: NULL input");
+  CT_ARG_CHECK(((uintptr_t)nodes & 15u) == 0, "predict: nodes must be 16-byte aligned");
   CT_ARG_CHECK(n_trees >= 1 && n_features >= 1, "predict: empty forest or no features");
   CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "predict: n_classes out of range");
   if (n_rows == 0) return CT_OK;

@@ -16,9 +16,12 @@
 //   * fit jobs (host arrays in, a new resident forest out) run on fit-worker
 //     threads with their own low-priority streams and device arenas, so
 //     their kernels overlap the predict batches;
-//   * every device allocation is made at creation or when a forest is added,
-//     against the byte budget; a request that does not fit is rejected with
-//     CT_ERR_OOM instead of allocating.
+//   * every device allocation is made at creation, against the byte budget:
+//     forests are carved from a pool reserved there (a device allocation
+//     issued while requests run would serialize all streams), and a request
+//     or forest that does not fit is rejected with CT_ERR_OOM;
+//   * a removed forest's pool bytes return once the batches launched on it
+//     have completed (per-forest reference counts).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -26,6 +29,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -58,7 +62,58 @@ struct Forest {
   uint32_t* off = nullptr;
   uint32_t n_nodes = 0, n_trees = 0, n_features = 0, n_classes = 0;
   uint32_t group = 0;  // trees per L2-sized group
-  size_t bytes = 0;
+  size_t bytes = 0;     // pool bytes
+  size_t pool_off = 0;
+  uint32_t refs = 0;    // launched batches not yet completed
+  bool removed = false;
+};
+
+// First-fit allocator over one device region, 256-byte granules, coalescing.
+class Pool {
+ public:
+  static constexpr size_t NO_ROOM = ~size_t(0);
+  void reset(size_t bytes) {
+    total_ = bytes;
+    used_ = 0;
+    free_.clear();
+    if (bytes) free_[0] = bytes;
+  }
+  size_t alloc(size_t bytes) {
+    bytes = round(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const size_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_[off + bytes] = len - bytes;
+      used_ += bytes;
+      return off;
+    }
+    return NO_ROOM;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = round(bytes);
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  static size_t round(size_t b) { return (b + 255) & ~size_t(255); }
+  size_t used() const { return used_; }
+  size_t total() const { return total_; }
+
+ private:
+  std::map<size_t, size_t> free_;
+  size_t total_ = 0, used_ = 0;
 };
 
 struct Job {
@@ -104,6 +159,9 @@ class Server {
   std::condition_variable cv_work, cv_done;
   bool stop = false;
   std::vector<Forest> forests;
+  char* pool_base = nullptr;
+  Pool pool;
+  cudaStream_t upload_st = nullptr;
   Lane lanes[2];
   std::deque<Job*> fit_q;
   std::vector<FitWorker> fit_workers;
@@ -162,6 +220,11 @@ class Server {
       CT_TRY(take(arena, (void**)&fw.arena));
       fw.arena_bytes = arena;
     }
+    size_t pool_bytes = cfg.forest_pool_bytes ? cfg.forest_pool_bytes : std::min<size_t>(4ull << 30, budget / 4);
+    pool_bytes = Pool::round(pool_bytes);
+    CT_TRY(take(pool_bytes, (void**)&pool_base));
+    pool.reset(pool_bytes);
+    CT_CUDA_TRY(cudaStreamCreateWithFlags(&upload_st, cudaStreamNonBlocking));
     for (int l = 0; l < 2; ++l) lanes[l].th = std::thread([this, l] { lane_loop(l); });
     for (auto& fw : fit_workers) fw.th = std::thread([this, &fw] { fit_loop(fw); });
     return CT_OK;
@@ -227,33 +290,66 @@ class Server {
       if (fw.arena) cudaFree(fw.arena);
       if (fw.st) cudaStreamDestroy(fw.st);
     }
-    for (auto& f : forests) {
-      if (f.nodes) cudaFree(f.nodes);
-      if (f.off) cudaFree(f.off);
-    }
+    if (pool_base) cudaFree(pool_base);
+    if (upload_st) cudaStreamDestroy(upload_st);
   }
 
+  // Pool bytes are taken under the lock; the upload runs outside it (on the
+  // caller's stream), so the predict lanes are never held up by a forest
+  // being added.
   int add_forest(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* off, uint32_t n_trees,
-                 uint32_t n_features, uint32_t n_classes, uint32_t* id) {
+                 uint32_t n_features, uint32_t n_classes, uint32_t* id, cudaStream_t st = nullptr) {
     CT_ARG_CHECK(nodes && off && id && n_nodes && n_trees, "server: empty forest");
     CT_ARG_CHECK(n_features <= cfg.max_features, "server: forest has more features than max_features");
     CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "server: n_classes out of range");
-    std::lock_guard<std::mutex> lk(mu);
+    if (!st) st = upload_st;
     Forest f;
     f.n_nodes = n_nodes;
     f.n_trees = n_trees;
     f.n_features = n_features;
     f.n_classes = n_classes;
-    f.bytes = (size_t)n_nodes * sizeof(ct_packed_node) + (size_t)n_trees * 4;
+    const size_t node_bytes = Pool::round((size_t)n_nodes * sizeof(ct_packed_node)), off_bytes = (size_t)n_trees * 4;
+    f.bytes = Pool::round(node_bytes + off_bytes);
     f.group = n_classes <= cfg.max_classes ? predict_group_size(n_trees, n_nodes) : n_trees;
-    CT_CUDA_TRY(cudaSetDevice(device));
-    CT_TRY(take((size_t)n_nodes * sizeof(ct_packed_node), (void**)&f.nodes));
-    CT_TRY(take((size_t)n_trees * 4, (void**)&f.off));
-    CT_CUDA_TRY(cudaMemcpy(f.nodes, nodes, (size_t)n_nodes * sizeof(ct_packed_node), cudaMemcpyHostToDevice));
-    CT_CUDA_TRY(cudaMemcpy(f.off, off, (size_t)n_trees * 4, cudaMemcpyHostToDevice));
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      f.pool_off = pool.alloc(f.bytes);
+      if (f.pool_off == Pool::NO_ROOM) {
+        set_last_error("server: forest pool full (" + std::to_string(pool.used()) + " of " +
+                       std::to_string(pool.total()) + " bytes held, " + std::to_string(f.bytes) + " asked)");
+        return CT_ERR_OOM;
+      }
+    }
+    f.nodes = reinterpret_cast<ct_packed_node*>(pool_base + f.pool_off);
+    f.off = reinterpret_cast<uint32_t*>(pool_base + f.pool_off + node_bytes);
+    if (cudaMemcpyAsync(f.nodes, nodes, (size_t)n_nodes * sizeof(ct_packed_node), cudaMemcpyHostToDevice, st) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(f.off, off, off_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+      std::lock_guard<std::mutex> lk(mu);
+      pool.release(f.pool_off, f.bytes);
+      set_last_error("server: forest upload failed");
+      return CT_ERR_CUDA;
+    }
+    std::lock_guard<std::mutex> lk(mu);
     forests.push_back(f);
     *id = (uint32_t)(forests.size() - 1);
     return CT_OK;
+  }
+
+  int remove_forest(uint32_t id) {
+    std::lock_guard<std::mutex> lk(mu);
+    CT_ARG_CHECK(id < forests.size() && !forests[id].removed, "server: unknown forest id");
+    Forest& f = forests[id];
+    f.removed = true;
+    if (f.refs == 0) pool.release(f.pool_off, f.bytes);
+    return CT_OK;
+  }
+
+  // caller holds mu
+  void unref(uint32_t id) {
+    Forest& f = forests[id];
+    if (--f.refs == 0 && f.removed) pool.release(f.pool_off, f.bytes);
   }
 
   int submit(ct_request* r) {
@@ -273,7 +369,7 @@ class Server {
       }
       fit_q.push_back(j);
     } else {
-      if (r->forest >= forests.size()) {
+      if (r->forest >= forests.size() || forests[r->forest].removed) {
         delete j;
         set_last_error("server: unknown forest id");
         return CT_ERR_ARG;
@@ -331,7 +427,10 @@ class Server {
   void complete_slot(Slot& s) {
     const double t = now_s();
     std::lock_guard<std::mutex> lk(mu);
-    for (Job* j : s.jobs) finish(j, t, CT_OK);
+    for (Job* j : s.jobs) {
+      unref(j->req->forest);
+      finish(j, t, CT_OK);
+    }
     s.jobs.clear();
     cv_done.notify_all();
   }
@@ -387,14 +486,27 @@ class Server {
     uint64_t xoff = 0, roff = 0, voff = 0;
     uint32_t blocks = 0, max_c = 1;
     bool grouped = false;
-    std::vector<Forest> fs(batch.size());
+    std::vector<Forest> fs;
     {
+      // a forest removed after the request was queued: the request fails;
+      // the others hold a reference until their batch completes
       std::lock_guard<std::mutex> lk(mu);
-      for (size_t i = 0; i < batch.size(); ++i) {
-        fs[i] = forests[batch[i]->req->forest];
-        max_c = std::max(max_c, fs[i].n_classes);
+      size_t kept = 0;
+      for (Job* j : batch) {
+        Forest& f = forests[j->req->forest];
+        if (f.removed) {
+          finish(j, now_s(), CT_ERR_ARG);
+          continue;
+        }
+        ++f.refs;
+        fs.push_back(f);
+        max_c = std::max(max_c, f.n_classes);
+        batch[kept++] = j;
       }
+      if (kept < batch.size()) cv_done.notify_all();
+      batch.resize(kept);
     }
+    if (batch.empty()) return;
     const uint32_t rpb = predict_rows_per_block(max_c);
     int err = 0;
     for (size_t i = 0; i < batch.size(); ++i) {
@@ -448,7 +560,10 @@ class Server {
     if (err) {
       cudaEventSynchronize(s.ev);
       std::lock_guard<std::mutex> lk(mu);
-      for (Job* j : s.jobs) finish(j, now_s(), CT_ERR_CUDA);
+      for (Job* j : s.jobs) {
+        unref(j->req->forest);
+        finish(j, now_s(), CT_ERR_CUDA);
+      }
       s.jobs.clear();
       cv_done.notify_all();
     }
@@ -564,7 +679,7 @@ class Server {
       offs[t] = (uint32_t)packed.size();
       for (uint32_t i = 0; i < nn; ++i) packed.push_back(ct_packed_node{ot[i], of[i], ol[i], ov[i]});
     }
-    return add_forest(packed.data(), (uint32_t)packed.size(), offs.data(), T, F, C, fid);
+    return add_forest(packed.data(), (uint32_t)packed.size(), offs.data(), T, F, C, fid, st);
   }
 
   static double pct(std::vector<double> v, double q) {
@@ -594,6 +709,8 @@ class Server {
     out->rows_per_s = out->wall_s > 0 ? n_rows / out->wall_s : 0.0;
     out->hbm_used_bytes = used;
     out->hbm_budget_bytes = budget;
+    out->forest_bytes = pool.used();
+    out->forest_pool_bytes = pool.total();
   }
 
   void reset_stats() {
@@ -636,6 +753,11 @@ int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_n
   CT_ARG_CHECK(handle, "NULL server");
   return reinterpret_cast<Server*>(handle)->add_forest(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes,
                                                         forest_id);
+}
+
+int ct_server_remove_forest(void* handle, uint32_t forest_id) {
+  CT_ARG_CHECK(handle, "NULL server");
+  return reinterpret_cast<Server*>(handle)->remove_forest(forest_id);
 }
 
 int ct_server_submit(void* handle, ct_request* req) {

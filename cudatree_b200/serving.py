@@ -22,7 +22,8 @@ CT_REQ_FIT = 1
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch_rows", C.c_uint32), ("max_features", C.c_uint32), ("small_rows", C.c_uint32),
                 ("fit_workers", C.c_uint32), ("max_fit_rows", C.c_uint32), ("max_fit_trees", C.c_uint32),
-                ("max_classes", C.c_uint32), ("reserved", C.c_uint32), ("hbm_budget_bytes", C.c_uint64)]
+                ("max_classes", C.c_uint32), ("reserved", C.c_uint32), ("hbm_budget_bytes", C.c_uint64),
+                ("forest_pool_bytes", C.c_uint64)]
 
 
 class Request(C.Structure):
@@ -40,7 +41,8 @@ class ServerStats(C.Structure):
                 ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("p50_small_ms", C.c_double),
                 ("p99_small_ms", C.c_double), ("p50_fit_ms", C.c_double), ("p99_fit_ms", C.c_double),
                 ("max_ms", C.c_double), ("wall_s", C.c_double), ("rows_per_s", C.c_double),
-                ("hbm_used_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64)]
+                ("hbm_used_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64),
+                ("forest_bytes", C.c_uint64), ("forest_pool_bytes", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -53,14 +55,16 @@ def pinned(a: np.ndarray) -> torch.Tensor:
 
 
 class ForestServer:
-    """Resident forests + request loop on the current CUDA device."""
+    """Resident forests + request loop on the current CUDA device.  All of the
+    server's device memory (staging, fit arenas, the forest pool) is taken at
+    construction, inside hbm_budget_bytes."""
 
     def __init__(self, max_batch_rows=0, max_features=512, small_rows=4096, fit_workers=2,
-                 max_fit_rows=20000, max_fit_trees=10, hbm_budget_bytes=0, max_classes=64):
+                 max_fit_rows=20000, max_fit_trees=10, hbm_budget_bytes=0, max_classes=64, forest_pool_bytes=0):
         _lib.load()
         torch.cuda.init()
         cfg = ServerConfig(max_batch_rows, max_features, small_rows, fit_workers, max_fit_rows,
-                           max_fit_trees, max_classes, 0, hbm_budget_bytes)
+                           max_fit_trees, max_classes, 0, hbm_budget_bytes, forest_pool_bytes)
         h = C.c_void_p()
         _lib.call("ct_server_create", C.byref(cfg), C.byref(h))
         self._h = h
@@ -91,6 +95,11 @@ class ForestServer:
         if table is not None:
             self._tables[fid.value] = np.asarray(table)
         return fid.value
+
+    def remove_forest(self, forest_id: int) -> None:
+        """Retire a forest; its pool bytes return when its launched batches complete."""
+        _lib.call("ct_server_remove_forest", self._h, forest_id)
+        self._tables.pop(forest_id, None)
 
     def predict_request(self, forest_id: int, x_pinned: torch.Tensor, out_pinned: torch.Tensor) -> Request:
         n = x_pinned.shape[0]

@@ -222,7 +222,7 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
  * predict.cu (base_tree.py:44-81, predict.cu:12-69) and the host vote
  * (random_forest.py:339-377).  x [n_rows][n_features] float32 row-major;
  * votes [n_rows][n_classes] uint32 (may be NULL); pred [n_rows] uint32 class
- * ids (may be NULL).  All device pointers. */
+ * ids (may be NULL).  All device pointers; nodes 16-byte aligned. */
 typedef struct ct_packed_node {
   float threshold;
   uint32_t feature;
@@ -240,7 +240,9 @@ int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_
  * the predict requests that have arrived into one multi-request launch per
  * lane (small requests on a high-priority stream, large ones on a
  * low-priority stream), runs small fit jobs on worker streams, and holds all
- * its device memory inside an HBM budget. */
+ * its device memory inside an HBM budget.  Every device allocation happens in
+ * ct_server_create: forests are carved from a pool reserved there, because a
+ * device allocation made while requests run would serialize the streams. */
 enum { CT_REQ_PREDICT = 0, CT_REQ_FIT = 1 };
 
 typedef struct ct_server_config {
@@ -254,6 +256,8 @@ typedef struct ct_server_config {
                                 (0 = 64)                                              */
   uint32_t reserved;
   uint64_t hbm_budget_bytes; /* device bytes the server may hold (0 = 80% of free)    */
+  uint64_t forest_pool_bytes;/* resident-forest pool inside the budget
+                                (0 = min(4 GiB, a quarter of the budget))             */
 } ct_server_config;
 
 typedef struct ct_request {
@@ -283,14 +287,19 @@ typedef struct ct_server_stats {
   double p50_fit_ms, p99_fit_ms;       /* fit jobs                              */
   double max_ms, wall_s, rows_per_s;
   uint64_t hbm_used_bytes, hbm_budget_bytes;
+  uint64_t forest_bytes, forest_pool_bytes; /* pool bytes held by forests / pool size */
 } ct_server_stats;
 
 int ct_server_create(const ct_server_config* cfg, void** handle);
 int ct_server_destroy(void* handle);
-/* Copies a packed forest (host arrays, layout of ct_predict) to the device. */
+/* Copies a packed forest (host arrays, layout of ct_predict) into the forest
+ * pool; CT_ERR_OOM when the pool has no room. */
 int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes,
                          const uint32_t* tree_offset, uint32_t n_trees, uint32_t n_features,
                          uint32_t n_classes, uint32_t* forest_id);
+/* Retires a forest: new requests for it fail with CT_ERR_ARG; its pool bytes
+ * return once the batches already launched on it have completed. */
+int ct_server_remove_forest(void* handle, uint32_t forest_id);
 /* Queues a request now; its buffers must stay valid until ct_server_wait. */
 int ct_server_submit(void* handle, ct_request* req);
 int ct_server_wait(void* handle, ct_request* req, double timeout_s);

@@ -127,3 +127,27 @@ def test_tree_groups_match_oracle_and_server(cuda_device):
         assert r.status == 0
         np.testing.assert_array_equal(f.compt_table[out.numpy().astype(np.int64)], f.predict(xs2))
     srv.close()
+
+
+def test_forest_pool_remove_and_reuse(cuda_device):
+    """Forests live in a pool reserved at creation: a forest larger than the
+    pool is refused, a removed forest's bytes are reused, and requests for a
+    removed forest fail."""
+    x, y = _blobs(3000, 12, 4, 21)
+    forest = RandomForestClassifier(n_estimators=12, seed=3).fit(x, y)
+    from cudatree_b200.random_forest import pack_trees
+    packed, _ = pack_trees(forest._trees)
+    need = packed.nbytes + 4 * len(forest._trees)
+    srv = ForestServer(max_features=16, fit_workers=0, forest_pool_bytes=int(need * 1.5))
+    a = srv.add_forest(forest)
+    with pytest.raises(CudaTreeError):
+        srv.add_forest(forest)  # the pool holds one copy
+    held = srv.stats()["forest_bytes"]
+    assert held >= need
+    srv.remove_forest(a)
+    assert srv.stats()["forest_bytes"] == 0
+    with pytest.raises(CudaTreeError):
+        srv.predict(a, x[:10])
+    b = srv.add_forest(forest)
+    np.testing.assert_array_equal(srv.predict(b, x), forest.predict(x))
+    srv.close()
