@@ -190,20 +190,22 @@ def run_serving(args, x_cov, y_cov, seed):
         pool = (rng.standard_normal((65536, f)).astype(np.float32) + means[rng.integers(0, c, 65536)])
         pools.append(pool)
     # plain-path throughput: one 65,536-row batch on the 500-tree forest
-    nodes, offs = big._device_forest()
+    nodes, offs, compact = big._device_forest()
     from cudatree_b200 import _lib
+    fn = "ct_predict_compact" if compact else "ct_predict"
     xd = torch.from_numpy(pools[0]).cuda()
     out = torch.empty(xd.shape[0], dtype=torch.int32, device="cuda")
+    votes = torch.empty((xd.shape[0], big.n_labels), dtype=torch.int32, device="cuda")
     st = torch.cuda.current_stream()
     for _ in range(2):
-        _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
-                  big.n_features, big.n_labels, None, out.data_ptr(), st.cuda_stream)
+        _lib.call(fn, nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
+                  big.n_features, big.n_labels, votes.data_ptr(), out.data_ptr(), st.cuda_stream)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
     reps = 5
     for _ in range(reps):
-        _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
-                  big.n_features, big.n_labels, None, out.data_ptr(), st.cuda_stream)
+        _lib.call(fn, nodes.data_ptr(), offs.data_ptr(), len(big._trees), xd.data_ptr(), xd.shape[0],
+                  big.n_features, big.n_labels, votes.data_ptr(), out.data_ptr(), st.cuda_stream)
     e1.record(st)
     torch.cuda.synchronize()
     batch_rows_per_s = reps * xd.shape[0] / (e0.elapsed_time(e1) / 1000.0)
@@ -262,6 +264,7 @@ def run_serving(args, x_cov, y_cov, seed):
         "rows_per_s": stats["rows_per_s"], "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"],
         "p50_ms_le4096_rows": stats["p50_small_ms"], "p99_ms_le4096_rows": stats["p99_small_ms"],
         "p50_fit_ms": stats["p50_fit_ms"], "p99_fit_ms": stats["p99_fit_ms"], "batches": int(stats["batches"]),
+        "zero_copy_requests": int(stats["zero_copy_requests"]),
         "hbm_used_gb": stats["hbm_used_bytes"] / 1e9,
         "identical_to_plain_predict": bool(same), "checked_requests": checked,
         "plain_predict_rows_per_s_500_trees": batch_rows_per_s,
@@ -270,24 +273,27 @@ def run_serving(args, x_cov, y_cov, seed):
 
 def run_predict_only(args):
     """Plain predict throughput on a forest fit to the covtype-shaped data:
-    65,536-row batches through ct_predict, with and without the vote table
-    (the table lets the launch walk L2-sized tree groups)."""
+    65,536-row batches through ct_predict (packed nodes) and
+    ct_predict_compact (8-byte nodes), with and without the vote table (the
+    table lets the launch walk L2-sized tree groups)."""
     import torch
 
     from cudatree_b200 import RandomForestClassifier, _lib, synthetic
     x, y = synthetic.covtype_like()
     forest = RandomForestClassifier(args.serve_trees, max_features=MAX_FEATURES, seed=77).fit(x, y)
-    nodes, offs = forest._device_forest()
     xd = torch.from_numpy(x[:65536]).cuda()
     out = torch.empty(xd.shape[0], dtype=torch.int32, device="cuda")
     votes = torch.empty((xd.shape[0], forest.n_labels), dtype=torch.int32, device="cuda")
     st = torch.cuda.current_stream()
     res = {}
-    for name, vt in (("no_vote_table", None), ("tree_groups", votes)):
+    for name, vt, compact in (("packed_no_vote_table", None, False), ("packed_tree_groups", votes, False),
+                              ("compact_no_vote_table", None, True), ("compact_tree_groups", votes, True)):
+        nodes, offs, _ = forest._device_forest(compact)
+
         def call():
-            _lib.call("ct_predict", nodes.data_ptr(), offs.data_ptr(), len(forest._trees), xd.data_ptr(),
-                      xd.shape[0], forest.n_features, forest.n_labels, None if vt is None else vt.data_ptr(),
-                      out.data_ptr(), st.cuda_stream)
+            _lib.call("ct_predict_compact" if compact else "ct_predict", nodes.data_ptr(), offs.data_ptr(),
+                      len(forest._trees), xd.data_ptr(), xd.shape[0], forest.n_features, forest.n_labels,
+                      None if vt is None else vt.data_ptr(), out.data_ptr(), st.cuda_stream)
         for _ in range(args.warmup):
             call()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -21,9 +21,13 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
 int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
                  const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
                  uint32_t* ov);
-int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_trees, const float* x,
+int predict(const void* nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees, const float* x,
             uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
             cudaStream_t st);
+uint32_t compact_feature_bits(uint32_t n_features);
+bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes);
+int compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features, uint32_t max_tree_nodes,
+                   ct_compact_node* out, cudaStream_t st);
 size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features);
 int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
             size_t wsb, cudaStream_t st);
@@ -232,8 +236,24 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
 int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,
                uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
                void* stream) {
-  CT_GUARD(return predict(nodes, tree_offset, n_trees, x, n_rows, n_features, n_classes, votes, pred,
+  CT_GUARD(return predict(nodes, 0, tree_offset, n_trees, x, n_rows, n_features, n_classes, votes, pred,
                           (cudaStream_t)stream);)
+}
+
+int ct_compact_fits(uint32_t n_features, uint32_t max_tree_nodes) {
+  return n_features >= 1 && compact_fits(n_features, max_tree_nodes) ? 1 : 0;
+}
+
+int ct_compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features, uint32_t max_tree_nodes,
+                      ct_compact_node* out, void* stream) {
+  CT_GUARD(return compact_forest(nodes, n_nodes, n_features, max_tree_nodes, out, (cudaStream_t)stream);)
+}
+
+int ct_predict_compact(const ct_compact_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,
+                       uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
+                       void* stream) {
+  CT_GUARD(return predict(nodes, compact_feature_bits(n_features), tree_offset, n_trees, x, n_rows, n_features,
+                          n_classes, votes, pred, (cudaStream_t)stream);)
 }
 
 }  // extern "C"

@@ -309,7 +309,7 @@ View make_view(const ct_problem* p, const ct_lists* l);
 // [block0, block0 + tiles * ceil(n_trees / group)) of the launch are its,
 // group-major; rows [row0, row0 + n_rows) of the batch are its.
 struct BatchReq {
-  const ct_packed_node* nodes;
+  const void* nodes;      // packed (fbits 0) or compact nodes
   const uint32_t* tree_off;
   const float* x;         // [n_rows][n_features] on the device
   uint32_t* pred;         // [n_rows] on the device
@@ -322,12 +322,17 @@ struct BatchReq {
   uint32_t tiles;
   uint32_t group;         // trees per group (>= n_trees: one group, no vote table)
   uint32_t row0;
-  uint32_t pad[2];
+  uint32_t fbits;         // 0: packed nodes; else compact nodes with this many feature bits
+  uint32_t rpb;           // rows per tile (predict_rows_per_block)
 };
-uint32_t predict_rows_per_block(uint32_t n_classes);
-uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes);
+uint32_t predict_rows_per_block(uint32_t n_classes, uint32_t n_features);
+size_t predict_tile_smem(uint32_t rpb, uint32_t n_classes, uint32_t n_features);
+uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes, size_t node_bytes);
+uint32_t compact_feature_bits(uint32_t n_features);
+bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes);
+void compact_host(const ct_packed_node* in, uint32_t n, uint32_t fbits, ct_compact_node* out);
 int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
-                  uint32_t rows_per_block, uint32_t max_classes, bool any_grouped, cudaStream_t st);
+                  size_t smem, bool any_grouped, cudaStream_t st);
 int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st);
 int check_problem(const ct_problem* p);
 

@@ -3,7 +3,7 @@
 // Reference: predict.cu:12-69 walks one tree per launch with one active lane
 // per warp, and random_forest.py:339-362 stacks per-tree labels on the host
 // and votes row by row in Python.  Here one launch walks every tree of the
-// packed forest:
+// forest:
 //   * blocks cover (row tile, tree group); the trees are cut into groups whose
 //     nodes fit comfortably in L2, and blocks are numbered group-major, so the
 //     blocks in flight walk one group and its nodes come from DRAM about once
@@ -11,10 +11,17 @@
 //   * walks inside a block are numbered row-fastest: with 32 rows per tile a
 //     lane keeps one row and a warp's lanes walk the same tree (shared loads
 //     of its top levels); each thread keeps PRED_ILP walks in flight;
+//   * the walk is bound by the L1 data path (bytes returned per node visit),
+//     so a node is one vector load: 16 bytes in the packed form, 8 bytes in
+//     the compact form, which is used whenever a forest's trees fit it;
 //   * votes go to a shared-memory histogram; with several groups the
 //     histograms are added into a global [rows][classes] table and a second
 //     kernel takes the majority, lowest class on ties
 //     (np.argmax(np.bincount(...)), random_forest.py:358).
+#include <cstring>
+#include <mutex>
+#include <set>
+
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -27,20 +34,54 @@ constexpr uint32_t X_SMEM_BYTES = 32 * 1024;     // rows of x staged per block w
 constexpr uint32_t HIST_SMEM_BYTES = 64 * 1024;  // vote histogram [rows][classes]
 constexpr size_t GROUP_L2_BYTES = 32ull << 20;   // node bytes of one tree group
 
+__host__ __device__ __forceinline__ bool predict_rows_staged(uint32_t rpb, uint32_t n_features) {
+  return (size_t)rpb * n_features * sizeof(float) <= X_SMEM_BYTES;
+}
+
+// Packed form: 16 bytes {threshold, feature, left, value}; left 0 = leaf.
+struct PackedForm {
+  using Raw = uint4;
+  static constexpr size_t BYTES = 16;
+  __device__ static Raw load(const void* nodes, uint32_t pos) {
+    return __ldg(reinterpret_cast<const uint4*>(nodes) + pos);
+  }
+  __device__ static bool inner(const Raw& n) { return n.z != 0; }
+  __device__ static uint32_t left(const Raw& n, uint32_t) { return n.z; }
+  __device__ static uint32_t feature(const Raw& n, uint32_t) { return n.y; }
+  __device__ static float threshold(const Raw& n) { return __uint_as_float(n.x); }
+  __device__ static uint32_t value(const Raw& n) { return n.w; }
+};
+
+// Compact form: 8 bytes; inner {threshold, left << fbits | feature}, leaf
+// {class id, 0}.  left >= 1 for inner nodes, so the second word is nonzero.
+struct CompactForm {
+  using Raw = uint2;
+  static constexpr size_t BYTES = 8;
+  __device__ static Raw load(const void* nodes, uint32_t pos) {
+    return __ldg(reinterpret_cast<const uint2*>(nodes) + pos);
+  }
+  __device__ static bool inner(const Raw& n) { return n.y != 0; }
+  __device__ static uint32_t left(const Raw& n, uint32_t fbits) { return n.y >> fbits; }
+  __device__ static uint32_t feature(const Raw& n, uint32_t fbits) { return n.y & ((1u << fbits) - 1u); }
+  __device__ static float threshold(const Raw& n) { return __uint_as_float(n.x); }
+  __device__ static uint32_t value(const Raw& n) { return n.x; }
+};
+
 // Walk every (row, tree) pair of a tile for trees [t_lo, t_lo + n_t) and add
 // the leaf votes to hist[row][class].  Feature f of tile row r is
 // x[r * row_stride + f * feat_stride]: the staged shared-memory tile is
 // feature-major (row_stride 1, feat_stride rpb), so the lanes of a warp, one
-// row each, read distinct banks; unstaged rows are read from global memory.  Walks are numbered w = t * rpb + row (row-fastest);
-// rpb is a power of two dividing blockDim.x, so a thread's row is fixed
-// (threadIdx.x % rpb) and its tree index advances by blockDim.x / rpb per walk.
-// Each thread keeps PRED_ILP walks in flight; their node loads are issued
-// together, then each walk steps or, at a leaf, votes and starts the thread's
-// next tree.
-__device__ __forceinline__ void walk_tile(const ct_packed_node* __restrict__ nodes,
-                                          const uint32_t* __restrict__ tree_off, uint32_t t_lo, uint32_t n_t,
-                                          const float* x, uint32_t row_stride, uint32_t feat_stride,
-                                          uint32_t rows, uint32_t rpb, uint32_t n_classes, uint32_t* hist) {
+// row each, read distinct banks; unstaged rows are read from global memory.
+// Walks are numbered w = t * rpb + row (row-fastest); rpb is a power of two
+// dividing blockDim.x, so a thread's row is fixed (threadIdx.x % rpb) and its
+// tree index advances by blockDim.x / rpb per walk.  Each thread keeps
+// PRED_ILP walks in flight; their node loads are issued together, then each
+// walk steps or, at a leaf, votes and starts the thread's next tree.
+template <typename Form>
+__device__ __forceinline__ void walk_tile(const void* __restrict__ nodes, const uint32_t* __restrict__ tree_off,
+                                          uint32_t t_lo, uint32_t n_t, uint32_t fbits, const float* x,
+                                          uint32_t row_stride, uint32_t feat_stride, uint32_t rows, uint32_t rpb,
+                                          uint32_t n_classes, uint32_t* hist) {
   const uint32_t r = threadIdx.x & (rpb - 1);
   if (r >= rows) return;
   const uint32_t t_step = blockDim.x / rpb;
@@ -60,19 +101,20 @@ __device__ __forceinline__ void walk_tile(const ct_packed_node* __restrict__ nod
   }
   bool any = pos[0] != NONE;
   while (any) {
-    uint4 nd[PRED_ILP];  // {threshold bits, feature, left, value}: one 16-byte load per node
+    typename Form::Raw nd[PRED_ILP];
 #pragma unroll
     for (int k = 0; k < PRED_ILP; ++k)
-      if (pos[k] != NONE) nd[k] = __ldg(reinterpret_cast<const uint4*>(nodes) + pos[k]);
+      if (pos[k] != NONE) nd[k] = Form::load(nodes, pos[k]);
     any = false;
 #pragma unroll
     for (int k = 0; k < PRED_ILP; ++k) {
       if (pos[k] == NONE) continue;
       any = true;
-      if (nd[k].z != 0) {
-        pos[k] = base[k] + nd[k].z + (xr[nd[k].y * feat_stride] < __uint_as_float(nd[k].x) ? 0u : 1u);
+      if (Form::inner(nd[k])) {
+        const float v = xr[Form::feature(nd[k], fbits) * feat_stride];
+        pos[k] = base[k] + Form::left(nd[k], fbits) + (v < Form::threshold(nd[k]) ? 0u : 1u);
       } else {
-        atomicAdd(hr + nd[k].w, 1u);
+        atomicAdd(hr + Form::value(nd[k]), 1u);
         pos[k] = NONE;
         if (t_next < n_t) {
           base[k] = __ldg(tree_off + t_lo + t_next);
@@ -108,19 +150,21 @@ __device__ __forceinline__ uint32_t warp_argmax(const uint32_t* votes, uint32_t 
   return bc;
 }
 
-// Stage a tile's rows feature-major: xs[f * rpb + r] = x[r][f] (row-fastest,
-// so the shared-memory stores are conflict-free).
+// Stage a tile's rows feature-major: xs[f * rpb + r] = x[r][f].  The reads
+// are coalesced (x may be mapped host memory, read once over the link); the
+// shared-memory stores conflict, which costs far less than the walk's reads.
 __device__ __forceinline__ void stage_rows(const float* x, uint32_t rows, uint32_t rpb, uint32_t n_features,
                                            float* xs) {
   for (uint32_t i = threadIdx.x; i < rows * n_features; i += blockDim.x) {
-    const uint32_t f = i / rows, r = i - f * rows;
-    xs[f * rpb + r] = __ldg(x + (size_t)r * n_features + f);
+    const uint32_t r = i / n_features, f = i - r * n_features;
+    xs[f * rpb + r] = x[i];
   }
 }
 
 // One tile of one tree group: walk, then either vote (single group) or add
 // the histogram into the global vote table.
-__device__ __forceinline__ void tile_work(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t t_lo,
+template <typename Form>
+__device__ __forceinline__ void tile_work(const void* nodes, const uint32_t* tree_off, uint32_t fbits, uint32_t t_lo,
                                           uint32_t n_t, bool single_group, const float* x, uint32_t n_rows,
                                           uint32_t n_features, uint32_t n_classes, uint32_t rpb, uint32_t row0,
                                           uint32_t* votes, uint32_t* pred, uint32_t* smem) {
@@ -128,13 +172,14 @@ __device__ __forceinline__ void tile_work(const ct_packed_node* nodes, const uin
   float* xs = reinterpret_cast<float*>(smem + rpb * n_classes);
   const uint32_t rows = min(rpb, n_rows - row0);
   for (uint32_t i = threadIdx.x; i < rpb * n_classes; i += blockDim.x) hist[i] = 0;
-  const bool fits = (size_t)rpb * n_features * sizeof(float) <= X_SMEM_BYTES;
+  const bool fits = predict_rows_staged(rpb, n_features);
   if (fits) stage_rows(x + (size_t)row0 * n_features, rows, rpb, n_features, xs);
   __syncthreads();
   if (fits)
-    walk_tile(nodes, tree_off, t_lo, n_t, xs, 1, rpb, rows, rpb, n_classes, hist);
+    walk_tile<Form>(nodes, tree_off, t_lo, n_t, fbits, xs, 1, rpb, rows, rpb, n_classes, hist);
   else
-    walk_tile(nodes, tree_off, t_lo, n_t, x + (size_t)row0 * n_features, n_features, 1, rows, rpb, n_classes, hist);
+    walk_tile<Form>(nodes, tree_off, t_lo, n_t, fbits, x + (size_t)row0 * n_features, n_features, 1, rows, rpb,
+                    n_classes, hist);
   __syncthreads();
   if (single_group) {
     const uint32_t warp = threadIdx.x >> 5;
@@ -149,15 +194,16 @@ __device__ __forceinline__ void tile_work(const ct_packed_node* nodes, const uin
   }
 }
 
+template <typename Form>
 __global__ void __launch_bounds__(PRED_THREADS, 4)
-k_predict(const ct_packed_node* __restrict__ nodes, const uint32_t* __restrict__ tree_off, uint32_t n_trees,
+k_predict(const void* __restrict__ nodes, const uint32_t* __restrict__ tree_off, uint32_t n_trees, uint32_t fbits,
           uint32_t group, uint32_t tiles, const float* __restrict__ x, uint32_t n_rows, uint32_t n_features,
           uint32_t n_classes, uint32_t rpb, uint32_t* __restrict__ votes, uint32_t* __restrict__ pred) {
   extern __shared__ uint32_t smem[];
   const uint32_t g = blockIdx.x / tiles, tile = blockIdx.x - g * tiles;  // group-major
   const uint32_t t_lo = g * group;
-  tile_work(nodes, tree_off, t_lo, min(group, n_trees - t_lo), group >= n_trees, x, n_rows, n_features, n_classes,
-            rpb, tile * rpb, votes, pred, smem);
+  tile_work<Form>(nodes, tree_off, fbits, t_lo, min(group, n_trees - t_lo), group >= n_trees, x, n_rows, n_features,
+                  n_classes, rpb, tile * rpb, votes, pred, smem);
 }
 
 __global__ void k_vote_rows(const uint32_t* __restrict__ votes, uint32_t n_rows, uint32_t n_classes,
@@ -168,26 +214,88 @@ __global__ void k_vote_rows(const uint32_t* __restrict__ votes, uint32_t n_rows,
   if ((threadIdx.x & 31) == 0 && pred) pred[row] = c;
 }
 
-uint32_t group_size(uint32_t n_trees, uint64_t n_nodes) {
-  const uint64_t per_tree = (n_nodes * sizeof(ct_packed_node) + n_trees - 1) / n_trees;
+__global__ void k_compact(const ct_packed_node* __restrict__ in, uint32_t n, uint32_t fbits,
+                          uint2* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint4 p = __ldg(reinterpret_cast<const uint4*>(in) + i);
+    out[i] = p.z ? make_uint2(p.x, (p.z << fbits) | p.y) : make_uint2(p.w, 0u);
+  }
+}
+
+// Raise a kernel's dynamic shared-memory limit once per device.
+template <typename K>
+int allow_smem(K kernel, int bytes) {
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  CT_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(dev)) return CT_OK;
+  CT_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert(dev);
+  return CT_OK;
+}
+
+}  // namespace
+
+// Rows per tile: 32, halved until the [rows][classes] histogram and the
+// staged [features][rows] tile fit their shared-memory budgets.
+uint32_t predict_rows_per_block(uint32_t n_classes, uint32_t n_features) {
+  uint32_t r = 32;
+  while (r > 1 && ((size_t)r * n_classes * sizeof(uint32_t) > HIST_SMEM_BYTES ||
+                   (size_t)r * n_features * sizeof(float) > X_SMEM_BYTES))
+    r >>= 1;
+  return r;
+}
+
+size_t predict_tile_smem(uint32_t rpb, uint32_t n_classes, uint32_t n_features) {
+  return (size_t)rpb * n_classes * sizeof(uint32_t) +
+         (predict_rows_staged(rpb, n_features) ? (size_t)rpb * n_features * sizeof(float) : 0);
+}
+
+uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes, size_t node_bytes) {
+  const uint64_t per_tree = (n_nodes * node_bytes + n_trees - 1) / n_trees;
   uint64_t g = per_tree ? GROUP_L2_BYTES / per_tree : n_trees;
   if (g < 1) g = 1;
   return (uint32_t)std::min<uint64_t>(g, n_trees);
 }
 
-}  // namespace
-
-// Rows per tile: 32 when the [rows][classes] histogram fits, fewer for many classes.
-uint32_t predict_rows_per_block(uint32_t n_classes) {
-  uint32_t r = 32;
-  while (r > 1 && (size_t)r * n_classes * sizeof(uint32_t) > HIST_SMEM_BYTES) r >>= 1;
-  return r;
+uint32_t compact_feature_bits(uint32_t n_features) {
+  uint32_t b = 1;
+  while (b < 31 && (1u << b) < n_features) ++b;
+  return b;
 }
 
-uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes) { return group_size(n_trees, n_nodes); }
+bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes) {
+  const uint32_t b = compact_feature_bits(n_features);
+  return (1u << b) >= n_features && max_tree_nodes <= (1ull << (32 - b));
+}
+
+void compact_host(const ct_packed_node* in, uint32_t n, uint32_t fbits, ct_compact_node* out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const ct_packed_node& p = in[i];
+    uint32_t thr;
+    std::memcpy(&thr, &p.threshold, 4);
+    out[i] = p.left ? ct_compact_node{thr, (p.left << fbits) | p.feature} : ct_compact_node{p.value, 0u};
+  }
+}
+
+int compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features, uint32_t max_tree_nodes,
+                   ct_compact_node* out, cudaStream_t st) {
+  CT_ARG_CHECK(nodes && out, "compact: NULL argument");
+  CT_ARG_CHECK(((uintptr_t)nodes & 15u) == 0 && ((uintptr_t)out & 7u) == 0, "compact: misaligned arrays");
+  CT_ARG_CHECK(n_features >= 1 && compact_fits(n_features, max_tree_nodes),
+               "compact: trees too large for the compact form with this feature count");
+  if (n_nodes == 0) return CT_OK;
+  const uint32_t fbits = compact_feature_bits(n_features);
+  k_compact<<<std::min<uint32_t>(ceil_div(n_nodes, 256), 148 * 8), 256, 0, st>>>(nodes, n_nodes, fbits,
+                                                                               reinterpret_cast<uint2*>(out));
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
 
 __global__ void __launch_bounds__(PRED_THREADS, 4)
-k_predict_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, uint32_t rpb, uint32_t max_classes) {
+k_predict_batch(const BatchReq* __restrict__ reqs, uint32_t n_req) {
   extern __shared__ uint32_t smem[];
   uint32_t lo = 0, hi = n_req;  // the last request whose first block is <= blockIdx.x
   while (hi - lo > 1) {
@@ -198,9 +306,14 @@ k_predict_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, uint32_t rpb,
   const uint32_t local = blockIdx.x - rq.block0;
   const uint32_t g = local / rq.tiles, tile = local - g * rq.tiles;
   const uint32_t t_lo = g * rq.group;
-  (void)max_classes;
-  tile_work(rq.nodes, rq.tree_off, t_lo, min(rq.group, rq.n_trees - t_lo), rq.group >= rq.n_trees, rq.x,
-            rq.n_rows, rq.n_features, rq.n_classes, rpb, tile * rpb, rq.votes, rq.pred, smem);
+  const uint32_t n_t = min(rq.group, rq.n_trees - t_lo);
+  const uint32_t rpb = rq.rpb;
+  if (rq.fbits)
+    tile_work<CompactForm>(rq.nodes, rq.tree_off, rq.fbits, t_lo, n_t, rq.group >= rq.n_trees, rq.x, rq.n_rows,
+                           rq.n_features, rq.n_classes, rpb, tile * rpb, rq.votes, rq.pred, smem);
+  else
+    tile_work<PackedForm>(rq.nodes, rq.tree_off, 0, t_lo, n_t, rq.group >= rq.n_trees, rq.x, rq.n_rows,
+                          rq.n_features, rq.n_classes, rpb, tile * rpb, rq.votes, rq.pred, smem);
 }
 
 // Majority vote of the rows of requests whose trees were split into groups.
@@ -220,31 +333,27 @@ __global__ void k_vote_batch(const BatchReq* __restrict__ reqs, uint32_t n_req, 
 }
 
 int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
-                  uint32_t rows_per_block, uint32_t max_classes, bool any_grouped, cudaStream_t st) {
+                  size_t smem, bool any_grouped, cudaStream_t st) {
   if (n_req == 0 || total_blocks == 0) return CT_OK;
-  // histogram for the batch's largest class count, then the staged rows of x
-  const size_t smem = (size_t)rows_per_block * max_classes * sizeof(uint32_t) + X_SMEM_BYTES;
-  static bool configured = false;
-  if (!configured) {
-    const int most = (int)(HIST_SMEM_BYTES + X_SMEM_BYTES);
-    CT_CUDA_TRY(cudaFuncSetAttribute(k_predict_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
-    configured = true;
-  }
-  k_predict_batch<<<total_blocks, PRED_THREADS, smem, st>>>(reqs_dev, n_req, rows_per_block, max_classes);
+  CT_ARG_CHECK(smem <= HIST_SMEM_BYTES + X_SMEM_BYTES, "predict batch: tile shared memory too large");
+  CT_TRY(allow_smem(k_predict_batch, (int)(HIST_SMEM_BYTES + X_SMEM_BYTES)));
+  k_predict_batch<<<total_blocks, PRED_THREADS, smem, st>>>(reqs_dev, n_req);
   if (any_grouped) k_vote_batch<<<ceil_div(total_rows, 8), 256, 0, st>>>(reqs_dev, n_req, total_rows);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
 
-int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_trees, const float* x,
+// fbits == 0: packed nodes; else compact nodes with that many feature bits.
+int predict(const void* nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees, const float* x,
             uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
             cudaStream_t st) {
   CT_ARG_CHECK(nodes && tree_off && x, "predict: NULL input");
-  CT_ARG_CHECK(((uintptr_t)nodes & 15u) == 0, "predict: nodes must be 16-byte aligned");
+  CT_ARG_CHECK(((uintptr_t)nodes & (fbits ? 7u : 15u)) == 0, "predict: nodes must be aligned to the node size");
   CT_ARG_CHECK(n_trees >= 1 && n_features >= 1, "predict: empty forest or no features");
   CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "predict: n_classes out of range");
+  CT_ARG_CHECK(!fbits || fbits == compact_feature_bits(n_features), "predict: compact form of another feature count");
   if (n_rows == 0) return CT_OK;
-  const uint32_t rpb = predict_rows_per_block(n_classes);
+  const uint32_t rpb = predict_rows_per_block(n_classes, n_features);
   const uint32_t tiles = ceil_div(n_rows, rpb);
   // Tree groups need the vote table; without one every block walks all
   // trees.  The forest's size is estimated from the last tree's offset (one
@@ -254,21 +363,22 @@ int predict(const ct_packed_node* nodes, const uint32_t* tree_off, uint32_t n_tr
     uint32_t last_off = 0;
     CT_CUDA_TRY(cudaMemcpyAsync(&last_off, tree_off + n_trees - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CT_CUDA_TRY(cudaStreamSynchronize(st));
-    group = group_size(n_trees, (uint64_t)last_off * n_trees / (n_trees - 1));
+    group = predict_group_size(n_trees, (uint64_t)last_off * n_trees / (n_trees - 1),
+                               fbits ? CompactForm::BYTES : PackedForm::BYTES);
   }
   const uint32_t groups = ceil_div(n_trees, group);
-  const size_t hist_bytes = (size_t)rpb * n_classes * sizeof(uint32_t);
-  const size_t x_bytes = (size_t)rpb * n_features * sizeof(float);
-  const size_t smem = hist_bytes + (x_bytes <= X_SMEM_BYTES ? x_bytes : 0);
-  static bool configured = false;
-  if (!configured) {
-    const int most = (int)(HIST_SMEM_BYTES + X_SMEM_BYTES);
-    CT_CUDA_TRY(cudaFuncSetAttribute(k_predict, cudaFuncAttributeMaxDynamicSharedMemorySize, most));
-    configured = true;
-  }
+  const size_t smem = predict_tile_smem(rpb, n_classes, n_features);
   if (groups > 1) CT_CUDA_TRY(cudaMemsetAsync(votes, 0, (size_t)n_rows * n_classes * sizeof(uint32_t), st));
-  k_predict<<<tiles * groups, PRED_THREADS, smem, st>>>(nodes, tree_off, n_trees, group, tiles, x, n_rows,
-                                                         n_features, n_classes, rpb, votes, pred);
+  const int most = (int)(HIST_SMEM_BYTES + X_SMEM_BYTES);
+  if (fbits) {
+    CT_TRY(allow_smem(k_predict<CompactForm>, most));
+    k_predict<CompactForm><<<tiles * groups, PRED_THREADS, smem, st>>>(
+        nodes, tree_off, n_trees, fbits, group, tiles, x, n_rows, n_features, n_classes, rpb, votes, pred);
+  } else {
+    CT_TRY(allow_smem(k_predict<PackedForm>, most));
+    k_predict<PackedForm><<<tiles * groups, PRED_THREADS, smem, st>>>(
+        nodes, tree_off, n_trees, 0, group, tiles, x, n_rows, n_features, n_classes, rpb, votes, pred);
+  }
   if (groups > 1) k_vote_rows<<<ceil_div(n_rows, 8), 256, 0, st>>>(votes, n_rows, n_classes, pred);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;

@@ -3,11 +3,16 @@
 //
 // The reference has no serving path (its predict re-uploads X and every tree
 // per call, base_tree.py:57-62).  Here:
-//   * forests stay resident on the device as packed breadth-first nodes;
+//   * forests stay resident on the device as breadth-first nodes, in the
+//     8-byte compact form whenever the trees fit it;
 //   * two predict lanes, each a worker thread with its own CUDA stream: small
 //     requests (<= small_rows rows) on a high-priority stream, larger ones on
 //     a low-priority stream, so a 65k-row request does not hold back 1-row
 //     requests;
+//   * small requests whose host buffers are page-locked and mapped are
+//     zero-copy: the kernel stages their rows from host memory and writes the
+//     predictions back, so they never wait behind bulk copies in the copy
+//     engines (a 100 MB request copy takes ~2 ms);
 //   * a lane takes every request that has arrived (up to its staging
 //     capacity) into one multi-request predict launch; with two staging
 //     slots a lane launches the next batch while the previous one runs, and
@@ -52,13 +57,24 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
 namespace {
 
 
+// Page-locked host memory mapped at the same address on the device.
+bool device_addressable(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost && a.devicePointer == p;
+}
+
 double now_s() {
   using namespace std::chrono;
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
 struct Forest {
-  ct_packed_node* nodes = nullptr;
+  void* nodes = nullptr;  // compact nodes when fbits != 0, else packed
+  uint32_t fbits = 0;
   uint32_t* off = nullptr;
   uint32_t n_nodes = 0, n_trees = 0, n_features = 0, n_classes = 0;
   uint32_t group = 0;  // trees per L2-sized group
@@ -130,6 +146,7 @@ struct Slot {
   BatchReq* req_host = nullptr;  // pinned
   cudaEvent_t ev = nullptr;
   std::vector<Job*> jobs;
+  std::vector<uint8_t> direct;  // per job: rows and predictions in host memory, no copies
   double launched = 0;
 };
 
@@ -167,7 +184,7 @@ class Server {
   std::vector<FitWorker> fit_workers;
   // statistics
   std::vector<double> lat_small, lat_large, lat_fit;
-  uint64_t n_req = 0, n_rows = 0, n_batches = 0, n_fit = 0, n_rejected = 0;
+  uint64_t n_req = 0, n_rows = 0, n_batches = 0, n_fit = 0, n_rejected = 0, n_zero_copy = 0;
   double t_first = 0, t_last = 0;
   std::string error;
 
@@ -308,9 +325,25 @@ class Server {
     f.n_trees = n_trees;
     f.n_features = n_features;
     f.n_classes = n_classes;
-    const size_t node_bytes = Pool::round((size_t)n_nodes * sizeof(ct_packed_node)), off_bytes = (size_t)n_trees * 4;
+    uint32_t max_tree = 0;
+    for (uint32_t t = 0; t < n_trees; ++t) {
+      const uint32_t end = t + 1 < n_trees ? off[t + 1] : n_nodes;
+      CT_ARG_CHECK(off[t] < end && end <= n_nodes, "server: tree offsets out of order");
+      max_tree = std::max(max_tree, end - off[t]);
+    }
+    std::vector<ct_compact_node> compact;
+    const void* src = nodes;
+    size_t elem = sizeof(ct_packed_node);
+    if (compact_fits(n_features, max_tree)) {
+      f.fbits = compact_feature_bits(n_features);
+      compact.resize(n_nodes);
+      compact_host(nodes, n_nodes, f.fbits, compact.data());
+      src = compact.data();
+      elem = sizeof(ct_compact_node);
+    }
+    const size_t node_bytes = Pool::round((size_t)n_nodes * elem), off_bytes = (size_t)n_trees * 4;
     f.bytes = Pool::round(node_bytes + off_bytes);
-    f.group = n_classes <= cfg.max_classes ? predict_group_size(n_trees, n_nodes) : n_trees;
+    f.group = n_classes <= cfg.max_classes ? predict_group_size(n_trees, n_nodes, elem) : n_trees;
     {
       std::lock_guard<std::mutex> lk(mu);
       f.pool_off = pool.alloc(f.bytes);
@@ -320,9 +353,9 @@ class Server {
         return CT_ERR_OOM;
       }
     }
-    f.nodes = reinterpret_cast<ct_packed_node*>(pool_base + f.pool_off);
+    f.nodes = pool_base + f.pool_off;
     f.off = reinterpret_cast<uint32_t*>(pool_base + f.pool_off + node_bytes);
-    if (cudaMemcpyAsync(f.nodes, nodes, (size_t)n_nodes * sizeof(ct_packed_node), cudaMemcpyHostToDevice, st) !=
+    if (cudaMemcpyAsync(f.nodes, src, (size_t)n_nodes * elem, cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaMemcpyAsync(f.off, off, off_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
@@ -483,7 +516,9 @@ class Server {
   }
 
   void launch(Lane& ln, Slot& s, std::vector<Job*>& batch) {
-    uint64_t xoff = 0, roff = 0, voff = 0;
+    const bool small_lane = &ln == &lanes[0];
+    uint64_t xoff = 0, roff = 0, voff = 0, zero = 0;
+    size_t smem = 0;
     uint32_t blocks = 0, max_c = 1;
     bool grouped = false;
     std::vector<Forest> fs;
@@ -507,16 +542,25 @@ class Server {
       batch.resize(kept);
     }
     if (batch.empty()) return;
-    const uint32_t rpb = predict_rows_per_block(max_c);
     int err = 0;
+    s.direct.assign(batch.size(), 0);
     for (size_t i = 0; i < batch.size(); ++i) {
       ct_request* r = batch[i]->req;
       const Forest& f = fs[i];
       BatchReq& br = s.req_host[i];
+      const uint32_t rpb = predict_rows_per_block(f.n_classes, f.n_features);
+      smem = std::max(smem, predict_tile_smem(rpb, f.n_classes, f.n_features));
+      // small requests whose rows are staged whole read and answer host
+      // memory directly when the device can address it
+      s.direct[i] = small_lane && predict_tile_smem(rpb, f.n_classes, f.n_features) >
+                                      (size_t)rpb * f.n_classes * sizeof(uint32_t) &&
+                    device_addressable(r->x) && device_addressable(r->pred);
       br.nodes = f.nodes;
+      br.fbits = f.fbits;
+      br.rpb = rpb;
       br.tree_off = f.off;
-      br.x = s.x_dev + xoff;
-      br.pred = s.pred_dev + roff;
+      br.x = s.direct[i] ? r->x : s.x_dev + xoff;
+      br.pred = s.direct[i] ? r->pred : s.pred_dev + roff;
       br.n_rows = r->n_rows;
       br.n_features = f.n_features;
       br.n_classes = f.n_classes;
@@ -532,20 +576,25 @@ class Server {
         voff += (uint64_t)r->n_rows * f.n_classes;
       }
       blocks += br.tiles * ceil_div(f.n_trees, f.group);
-      if (cudaMemcpyAsync(s.x_dev + xoff, r->x, (size_t)r->n_rows * f.n_features * sizeof(float),
-                          cudaMemcpyHostToDevice, ln.st) != cudaSuccess)
-        err = 1;
-      xoff += (uint64_t)r->n_rows * f.n_features;
+      if (s.direct[i]) {
+        ++zero;
+      } else {
+        if (cudaMemcpyAsync(s.x_dev + xoff, r->x, (size_t)r->n_rows * f.n_features * sizeof(float),
+                            cudaMemcpyHostToDevice, ln.st) != cudaSuccess)
+          err = 1;
+        xoff += (uint64_t)r->n_rows * f.n_features;
+      }
       roff += r->n_rows;
     }
     if (voff && cudaMemsetAsync(s.votes_dev, 0, voff * sizeof(uint32_t), ln.st) != cudaSuccess) err = 1;
     if (cudaMemcpyAsync(s.req_dev, s.req_host, batch.size() * sizeof(BatchReq), cudaMemcpyHostToDevice, ln.st) !=
         cudaSuccess)
       err = 1;
-    if (predict_batch(s.req_dev, (uint32_t)batch.size(), blocks, (uint32_t)roff, rpb, max_c, grouped, ln.st) != CT_OK)
+    if (predict_batch(s.req_dev, (uint32_t)batch.size(), blocks, (uint32_t)roff, smem, grouped, ln.st) != CT_OK)
       err = 1;
     for (size_t i = 0; i < batch.size(); ++i) {
       ct_request* r = batch[i]->req;
+      if (s.direct[i]) continue;
       if (cudaMemcpyAsync(r->pred, s.pred_dev + s.req_host[i].row0, (size_t)r->n_rows * 4, cudaMemcpyDeviceToHost,
                           ln.st) != cudaSuccess)
         err = 1;
@@ -556,6 +605,7 @@ class Server {
     {
       std::lock_guard<std::mutex> lk(mu);
       ++n_batches;
+      n_zero_copy += zero;
     }
     if (err) {
       cudaEventSynchronize(s.ev);
@@ -709,6 +759,7 @@ class Server {
     out->rows_per_s = out->wall_s > 0 ? n_rows / out->wall_s : 0.0;
     out->hbm_used_bytes = used;
     out->hbm_budget_bytes = budget;
+    out->zero_copy_requests = n_zero_copy;
     out->forest_bytes = pool.used();
     out->forest_pool_bytes = pool.total();
   }
@@ -718,7 +769,7 @@ class Server {
     lat_small.clear();
     lat_large.clear();
     lat_fit.clear();
-    n_req = n_rows = n_batches = n_fit = n_rejected = 0;
+    n_req = n_rows = n_batches = n_fit = n_rejected = n_zero_copy = 0;
     t_first = t_last = 0;
   }
 };

@@ -100,7 +100,9 @@ def pack_trees(trees):
     return packed, offsets
 
 
-def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_votes):
+def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_votes, compact=False):
+    """Walk the forest on the device: packed nodes (ct_predict) or, with
+    compact=True, a device tensor of 8-byte compact nodes (ct_predict_compact)."""
     dev = _device()
     x = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
     if x.ndim != 2 or x.shape[1] != n_features:
@@ -113,8 +115,8 @@ def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_vot
     xd = torch.from_numpy(x).to(dev)
     votes = torch.empty((n, n_classes), dtype=torch.int32, device=dev)  # also the tree-group vote table
     pred = torch.empty((n,), dtype=torch.int32, device=dev)
-    _lib.call("ct_predict", _ptr(nodes), _ptr(offs), n_trees, _ptr(xd), n, n_features, n_classes,
-              _ptr(votes), _ptr(pred), _stream())
+    _lib.call("ct_predict_compact" if compact else "ct_predict", _ptr(nodes), _ptr(offs), n_trees, _ptr(xd), n,
+              n_features, n_classes, _ptr(votes), _ptr(pred), _stream())
     return (votes if want_votes else pred).cpu().numpy().view(np.uint32)
 
 
@@ -313,25 +315,42 @@ class RandomForestClassifier:
         return self
 
     # ----------------------------------------------------------- predict
-    def _device_forest(self):
+    def _device_forest(self, compact=None):
+        """(nodes, tree offsets, is_compact) on the device.  compact=None picks
+        the 8-byte compact form whenever the trees fit it."""
+        if compact is None:
+            compact = self._compact_fits()
+        key = "compact" if compact else "packed"
         if self._packed is None:
+            self._packed = {}
+        if key not in self._packed:
             dev = _device()
             packed, offsets = pack_trees(self._trees)
-            self._packed = (_to_dev(packed, dev), _to_dev(offsets, dev))
-        return self._packed
+            nodes, offs = _to_dev(packed, dev), _to_dev(offsets, dev)
+            if compact:
+                out = torch.empty(packed.shape[0] * 8, dtype=torch.uint8, device=dev)
+                _lib.call("ct_compact_forest", _ptr(nodes), packed.shape[0], self.n_features,
+                          max(t.n_nodes for t in self._trees), _ptr(out), _stream())
+                nodes = out
+            self._packed[key] = (nodes, offs, compact)
+        return self._packed[key]
 
-    def _votes(self, x) -> np.ndarray:
+    def _compact_fits(self) -> bool:
+        most = max(t.n_nodes for t in self._trees)
+        return bool(_lib.load().ct_compact_fits(self.n_features, most))
+
+    def _votes(self, x, compact=None) -> np.ndarray:
         if not self._trees:
             raise ValueError("forest is not fitted")
-        nodes, offs = self._device_forest()
-        return _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, True)
+        nodes, offs, cp = self._device_forest(compact)
+        return _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, True, cp)
 
     def predict(self, x):
         """Majority vote, lowest class on ties, in original label space (random_forest.py:339-362)."""
         if not self._trees:
             raise ValueError("forest is not fitted")
-        nodes, offs = self._device_forest()
-        res = _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, False)
+        nodes, offs, cp = self._device_forest()
+        res = _predict_packed(nodes, offs, len(self._trees), x, self.n_features, self.n_labels, False, cp)
         return self.compt_table[res.astype(np.int64)]
 
     def predict_proba(self, x):

@@ -42,7 +42,8 @@ class ServerStats(C.Structure):
                 ("p99_small_ms", C.c_double), ("p50_fit_ms", C.c_double), ("p99_fit_ms", C.c_double),
                 ("max_ms", C.c_double), ("wall_s", C.c_double), ("rows_per_s", C.c_double),
                 ("hbm_used_bytes", C.c_uint64), ("hbm_budget_bytes", C.c_uint64),
-                ("forest_bytes", C.c_uint64), ("forest_pool_bytes", C.c_uint64)]
+                ("forest_bytes", C.c_uint64), ("forest_pool_bytes", C.c_uint64),
+                ("zero_copy_requests", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -234,6 +234,27 @@ int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_
                const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
                uint32_t* votes, uint32_t* pred, void* stream);
 
+/* Compact forest: the same trees in 8-byte nodes, which halve the bytes a
+ * walk step reads (the walk is bound by them).  With b = feature bits (the
+ * smallest b >= 1 with 2^b >= n_features): inner node {threshold bits,
+ * left << b | feature}, leaf {class id, 0}.  Usable when every tree has at
+ * most 2^(32-b) nodes; same node order and tree_offset as the packed form. */
+typedef struct ct_compact_node {
+  uint32_t word0; /* threshold bits (inner) or class id (leaf)        */
+  uint32_t word1; /* left << feature_bits | feature; 0 marks a leaf   */
+} ct_compact_node;
+
+/* 1 when trees of up to max_tree_nodes nodes fit the compact form. */
+int ct_compact_fits(uint32_t n_features, uint32_t max_tree_nodes);
+/* Device packed -> device compact (stream ordered); CT_ERR_ARG when the
+ * trees do not fit. */
+int ct_compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features,
+                      uint32_t max_tree_nodes, ct_compact_node* out, void* stream);
+/* ct_predict on the compact form (nodes 8-byte aligned); same results. */
+int ct_predict_compact(const ct_compact_node* nodes, const uint32_t* tree_offset, uint32_t n_trees,
+                       const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
+                       uint32_t* votes, uint32_t* pred, void* stream);
+
 /* ----------------------------------------------------------- serving --- */
 /* No counterpart in the reference (its predict re-uploads X and every tree
  * per call, base_tree.py:57-62).  A server keeps forests resident, batches
@@ -264,7 +285,9 @@ typedef struct ct_request {
   double arrival_s;          /* ct_server_replay: seconds after the replay starts    */
   uint32_t kind;             /* CT_REQ_PREDICT or CT_REQ_FIT                          */
   uint32_t forest;           /* predict: resident forest id                           */
-  const float* x;            /* host [n_rows][n_features] (pinned: async copies)      */
+  const float* x;            /* host [n_rows][n_features]; pinned for async copies;
+                                small requests with mapped pinned x and pred are
+                                served without copies                              */
   const uint32_t* y;         /* fit: host [n_rows] class ids < n_classes              */
   uint32_t* pred;            /* predict: host [n_rows] class ids (output)             */
   uint32_t n_rows;
@@ -288,6 +311,7 @@ typedef struct ct_server_stats {
   double max_ms, wall_s, rows_per_s;
   uint64_t hbm_used_bytes, hbm_budget_bytes;
   uint64_t forest_bytes, forest_pool_bytes; /* pool bytes held by forests / pool size */
+  uint64_t zero_copy_requests;  /* small requests served from mapped host memory      */
 } ct_server_stats;
 
 int ct_server_create(const ct_server_config* cfg, void** handle);

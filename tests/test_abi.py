@@ -33,6 +33,10 @@ def test_struct_layouts_match_header_sizes():
     assert C.sizeof(_lib.Node) == 32
     assert C.sizeof(_lib.SplitResult) == 32
     assert C.sizeof(_lib.PackedNode) == 16
+    from cudatree_b200 import serving
+    assert C.sizeof(serving.ServerConfig) == 48
+    assert C.sizeof(serving.Request) == 96
+    assert C.sizeof(serving.ServerStats) == 152
     assert np.dtype(_lib.NODE_DTYPE_FIELDS).itemsize == 32
     assert np.dtype(_lib.SPLIT_DTYPE_FIELDS).itemsize == 32
 
@@ -123,3 +127,15 @@ def test_canonicalize_rejects_unreachable_nodes():
                                          np.zeros(4, np.float32).ctypes.data, z.ctypes.data, 4,
                                          *[o.ctypes.data for o in out])
     assert st == 6 and "unreachable" in _lib.last_error()
+
+
+def test_compact_fit_rule():
+    """Compact nodes hold left << b | feature in 32 bits, b = feature bits."""
+    lib = _lib.load()
+    assert lib.ct_compact_fits(54, 1 << 26) == 1      # b = 6
+    assert lib.ct_compact_fits(54, (1 << 26) + 1) == 0
+    assert lib.ct_compact_fits(64, 1 << 26) == 1      # 64 features still need only 6 bits
+    assert lib.ct_compact_fits(65, 1 << 26) == 0      # b = 7
+    assert lib.ct_compact_fits(1, 1 << 31) == 1       # b = 1
+    assert lib.ct_compact_fits(3000, 1 << 20) == 1    # b = 12
+    assert lib.ct_compact_fits(0, 10) == 0

@@ -89,3 +89,22 @@ def test_golden_forests(cuda_device, mode):
             np.testing.assert_array_equal(tr.feature_idx_array, g[f"{name}/{i}/feature"])
             np.testing.assert_array_equal(tr.feature_threshold_array, g[f"{name}/{i}/threshold"])
             np.testing.assert_array_equal(tr.values_array.astype(np.int64), g[f"{name}/{i}/value"])
+
+
+@pytest.mark.parametrize("n,f,c,seed", [(1797, 64, 10, 0), (3000, 3000, 7, 1), (20000, 5, 3, 2)])
+def test_compact_nodes_match_packed_and_oracle(cuda_device, n, f, c, seed):
+    """8-byte compact nodes give the same votes as packed nodes and the oracle
+    (feature bits from 3 to 12; deep trees from noisy labels)."""
+    x, y = _synthetic(n, f, c, seed)
+    if seed == 2:
+        y = np.random.default_rng(5).integers(0, c, size=n)  # noise labels: deep trees
+    forest = RandomForestClassifier(n_estimators=12, seed=seed).fit(x, y)
+    assert forest._compact_fits()
+    xs = np.concatenate([x[:2000], np.random.default_rng(9).normal(size=(500, f)).astype(np.float32)])
+    packed = forest._votes(xs, compact=False)
+    compact = forest._votes(xs, compact=True)
+    np.testing.assert_array_equal(compact, packed)
+    ref = O.Forest(trees=[O.Tree(t.left_children, t.right_children, t.feature_idx_array,
+                                 t.feature_threshold_array, t.values_array.astype(np.int64))
+                          for t in forest._trees], classes=forest.compt_table, n_features=f)
+    np.testing.assert_array_equal(compact, O.vote_counts(ref, xs))

@@ -58,6 +58,7 @@ def test_mixed_replay_matches_plain_predict(served):
     stats = srv.replay(reqs)
     assert stats["requests"] == 200 and stats["rejected"] == 0
     assert stats["p99_ms"] >= stats["p50_ms"] > 0
+    assert stats["zero_copy_requests"] > 0  # small requests on pinned buffers skip the copies
     for r, (forest, xs, xp, out) in zip(reqs, keep):
         assert r.status == 0
         got = forest.compt_table[out.numpy().astype(np.int64)]
@@ -135,15 +136,16 @@ def test_forest_pool_remove_and_reuse(cuda_device):
     removed forest fail."""
     x, y = _blobs(3000, 12, 4, 21)
     forest = RandomForestClassifier(n_estimators=12, seed=3).fit(x, y)
-    from cudatree_b200.random_forest import pack_trees
-    packed, _ = pack_trees(forest._trees)
-    need = packed.nbytes + 4 * len(forest._trees)
+    assert forest._compact_fits()  # held as 8-byte nodes
+
+    def up(b):
+        return (b + 255) // 256 * 256
+    need = up(up(8 * sum(t.n_nodes for t in forest._trees)) + 4 * len(forest._trees))
     srv = ForestServer(max_features=16, fit_workers=0, forest_pool_bytes=int(need * 1.5))
     a = srv.add_forest(forest)
     with pytest.raises(CudaTreeError):
         srv.add_forest(forest)  # the pool holds one copy
-    held = srv.stats()["forest_bytes"]
-    assert held >= need
+    assert srv.stats()["forest_bytes"] == need
     srv.remove_forest(a)
     assert srv.stats()["forest_bytes"] == 0
     with pytest.raises(CudaTreeError):
