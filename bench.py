@@ -34,6 +34,7 @@ WORKLOAD = ("covtype-shaped synthetic 581012x54 f32 (10 Gaussian + 44 one-hot), 
             "100 trees, bootstrap, max_features=7, uint32 indices, fully grown")
 N_TREES = 100
 MAX_FEATURES = 7
+PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.84
 
 
 def peaks():
@@ -336,13 +337,17 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
-            trees = step(profile=True)
+            trees = step()
             launches += forest.last_fit_stats["total_launches"]
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier(world)
     step_s = ev0.elapsed_time(ev1) / 1000.0 / args.steps
     job_s = max_over_ranks(step_s, world)
+    # per-kernel-group times and algorithmic bytes: one more step, with CUDA
+    # events between the groups on the launching stream (outside the timed region)
+    step(profile=True)
+    torch.cuda.synchronize()
     stats = forest.last_fit_stats
     n_nodes = sum(t.n_nodes for t in trees)
 
@@ -393,11 +398,12 @@ def run_ours(args, world, rank, local):
     pi = groups.index("partition")
     p_ms = stats["ms"][pi]
     p_gbs = stats["bytes"][pi] / (p_ms * 1e6) if p_ms > 0 else None
-    traffic = None
-    tfile = ROOT / "profiles" / "partition_traffic.json"
-    if tfile.exists():
-        t = json.loads(tfile.read_text())
-        traffic = t.get("dram_bytes_per_algorithmic_byte")
+    # DRAM bytes per partition launch: the algorithmic bytes per launch times
+    # the DRAM/algorithmic ratio ncu measured on the 10-tree case of this
+    # workload (dram__bytes_read.sum + dram__bytes_write.sum over every level
+    # launch; profiles/k_part_big_covtype_10trees.md)
+    p_launches = stats["launches"][pi]
+    traffic = (PARTITION_DRAM_PER_ALGORITHMIC_BYTE * stats["bytes"][pi] / p_launches) if p_launches else None
     si = groups.index("scan")
     s_ms = stats["ms"][si]
     cpu = None
@@ -421,7 +427,9 @@ def run_ours(args, world, rank, local):
         "kernels": kernels,
         "roofline": {"bound": "hbm", "kernel": "k_partition", "achieved": round(p_gbs, 1) if p_gbs else None,
                      "peak": peak, "unit": "GB/s", "frac": round(p_gbs / peak, 4) if p_gbs else None,
-                     "peak_kind": peak_kind, "traffic": traffic,
+                     "peak_kind": peak_kind, "traffic": round(traffic) if traffic else None,
+                     "traffic_unit": "DRAM bytes per launch (ncu ratio 0.84 x algorithmic, 10-tree capture)",
+                     "algorithmic_bytes_per_launch": round(stats["bytes"][pi] / p_launches) if p_launches else None,
                      "algorithmic_bytes_per_element": "n_features x (2 x index_bytes + 1)"},
         "scan_roofline": {"kernel": "k_split_scan (+hist/carry)",
                           "achieved": round(stats["bytes"][si] / (s_ms * 1e6), 1) if s_ms > 0 else None,
