@@ -90,6 +90,15 @@ __device__ __forceinline__ float f32_unorder(uint32_t k) {
 __device__ __forceinline__ bool is_candidate(float x, float x_next) {
   return __dadd_rn((double)x, DIFF_THRESHOLD) < (double)x_next;
 }
+// is_candidate for sorted neighbours (x <= x_next) with the double test only
+// where it can matter: equal values never qualify, and a float gap above 1e-4
+// (true gap > 9.99e-5 after the subtraction's 2^-24 relative rounding) always
+// does, since the double sum x + 1e-5 exceeds x by less than that.
+__device__ __forceinline__ bool is_candidate_sorted(float x, float x_next) {
+  if (!(x_next > x)) return false;
+  if (x_next - x > 1e-4f) return true;
+  return is_candidate(x, x_next);
+}
 __device__ __forceinline__ double gini_part(int64_t sq_sum, double n_side, double n_total) {
   double ratio = __ddiv_rn((double)sq_sum, __dmul_rn(n_side, n_side));
   return __dmul_rn(__dsub_rn(1.0, ratio), __ddiv_rn(n_side, n_total));
@@ -112,6 +121,15 @@ __device__ __forceinline__ int64_t warp_incl_scan_i64(int64_t v) {
 #pragma unroll
   for (int s = 1; s < 32; s <<= 1) {
     int64_t o = __shfl_up_sync(FULL, v, s);
+    if (lane >= (unsigned)s) v += o;
+  }
+  return v;
+}
+__device__ __forceinline__ int32_t warp_incl_scan_i32(int32_t v) {
+  const unsigned lane = lane_id();
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const int32_t o = __shfl_up_sync(FULL, v, s);
     if (lane >= (unsigned)s) v += o;
   }
   return v;

@@ -13,8 +13,8 @@
 //                  (reference reduce_2d / find_min_imp / get_thresholds)
 //   k_plan         node record, child ids, partition work list
 //   k_fill_mark    mark table + left class totals (reference fill_table)
-//   k_partition    stable partition of every feature's node range with warp
-//                  ballot/popc ranks and a decoupled look-back across pieces
+//   (partition)    stable partition of every feature's node range: plan and
+//                  mark table here, the kernels in ct_partition.cu
 //                  (reference scan_reshuffle, dfs_module.cu:224-307)
 //   k_children     child records for the next step
 #include <cfloat>
@@ -208,6 +208,7 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   sr = warp_sum_i64(sr);
   __syncwarp();
   const uint32_t n = nd.n;
+  const bool narrow = n < (1u << 25);
   const double nn = (double)n;
   const uint32_t lo = pc.j * scan_piece;
   const uint32_t hi = min(lo + scan_piece, n);
@@ -255,13 +256,24 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       __syncwarp();
       const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
       const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
-      const int64_t il = warp_incl_scan_i64(dl);
-      const int64_t ir = warp_incl_scan_i64(dr);
+      int64_t il, ir, tl, tr;  // inclusive warp prefix and warp total of each increment
+      if (narrow) {  // |partial sums| <= 32 (2n + 1) < 2^31
+        const int32_t a = warp_incl_scan_i32((int32_t)dl), b = warp_incl_scan_i32((int32_t)dr);
+        il = a;
+        ir = b;
+        tl = __shfl_sync(FULL, a, 31);
+        tr = __shfl_sync(FULL, b, 31);
+      } else {
+        il = warp_incl_scan_i64(dl);
+        ir = warp_incl_scan_i64(dr);
+        tl = __shfl_sync(FULL, il, 31);
+        tr = __shfl_sync(FULL, ir, 31);
+      }
       const int64_t SL = sl + il;
       const int64_t SR = sr + ir;
-      sl += __shfl_sync(FULL, il, 31);
-      sr += __shfl_sync(FULL, ir, 31);
-      if (valid && p + 1 < n && is_candidate(x, xn)) {
+      sl += tl;
+      sr += tr;
+      if (valid && p + 1 < n && is_candidate_sorted(x, xn)) {
         const double nl = (double)(p + 1);
         const double nr = __dsub_rn(nn, nl);
         const double gl = gini_part(SL, nl, nn);

@@ -25,7 +25,7 @@ namespace ct {
 namespace {
 
 constexpr uint32_t SPIN_LIMIT = 1u << 20;
-constexpr int BIG_WARPS = TILE_ELEMS / (32 * PART_ROUNDS);
+constexpr int BIG_WARPS = 8;  // warps of a k_part_big CTA
 constexpr int BIG_THREADS = BIG_WARPS * 32;
 constexpr int SMALL_THREADS = 256;
 constexpr uint32_t FEAT_BLOCK = 8;
@@ -170,13 +170,12 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 // RING buffers, RING-1 tiles ahead of the one being partitioned.  Copies
 // are 16-byte aligned and rounded, so they read up to 15 bytes past a
 // tile's last element (list buffers carry that padding).
-constexpr uint32_t RING = 3;
 
-template <typename IdxT>
+template <typename IdxT, uint32_t TILE>
 __device__ __forceinline__ void issue_tile(const IdxT* seg_in, uint32_t n, uint32_t j, unsigned char* buf,
                                            uint64_t* bar, uint32_t* off_out) {
-  const uint32_t lo = j * TILE_ELEMS;
-  const uint32_t cnt = min(TILE_ELEMS, n - lo);
+  const uint32_t lo = j * TILE;
+  const uint32_t cnt = min(TILE, n - lo);
   const uintptr_t a = reinterpret_cast<uintptr_t>(seg_in + lo);
   const uintptr_t a0 = a & ~uintptr_t(15);
   const uintptr_t e1 = (a + (uintptr_t)cnt * sizeof(IdxT) + 15) & ~uintptr_t(15);
@@ -185,14 +184,15 @@ __device__ __forceinline__ void issue_tile(const IdxT* seg_in, uint32_t n, uint3
   bulk_g2s(buf, reinterpret_cast<const void*>(a0), (uint32_t)(e1 - a0), bar);
 }
 
-template <typename IdxT>
+template <typename IdxT, uint32_t ROUNDS>
 constexpr uint32_t ring_buf_bytes() {
-  return TILE_ELEMS * sizeof(IdxT) + 128;
+  return BIG_WARPS * 32 * ROUNDS * sizeof(IdxT) + 128;
 }
 
-template <typename IdxT>
-__global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
-  constexpr uint32_t BUF = ring_buf_bytes<IdxT>();
+template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
+__global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
+  constexpr uint32_t TILE = BIG_WARPS * 32 * ROUNDS;
+  constexpr uint32_t BUF = ring_buf_bytes<IdxT, ROUNDS>();
   extern __shared__ __align__(128) unsigned char ring_smem[];
   unsigned char(*sbuf)[BUF] = reinterpret_cast<unsigned char(*)[BUF]>(ring_smem);
   __shared__ alignas(8) uint64_t bars[RING];
@@ -207,7 +207,9 @@ __global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
     for (uint32_t i = 0; i < RING; ++i) mbar_init(&bars[i], 1);
     mbar_fence_init();
   }
-  uint32_t uses[RING] = {0u, 0u, 0u};  // completed phases per ring buffer (uniform)
+  uint32_t uses[RING];  // completed phases per ring buffer (uniform)
+#pragma unroll
+  for (uint32_t i = 0; i < RING; ++i) uses[i] = 0;
   uint32_t g = 0;                      // tiles consumed by this CTA (ring position)
   while (true) {
     __syncthreads();
@@ -223,16 +225,16 @@ __global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
     const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
     IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
     const uint32_t n = sg.n;
-    const uint32_t ntiles = ceil_div(n, TILE_ELEMS);
+    const uint32_t ntiles = ceil_div(n, TILE);
     if (threadIdx.x == 0)
       for (uint32_t j = 0; j < RING - 1 && j < ntiles; ++j)
-        issue_tile<IdxT>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING]);
+        issue_tile<IdxT, TILE>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING]);
     uint32_t carry = 0;
     for (uint32_t j = 0; j < ntiles; ++j, ++g) {
       const uint32_t b = g % RING;
       if (threadIdx.x == 0 && j + RING - 1 < ntiles) {  // refill the buffer freed by tile j-1
         const uint32_t bn = (g + RING - 1) % RING;
-        issue_tile<IdxT>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn]);
+        issue_tile<IdxT, TILE>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn]);
       }
       bool ok = true;
       {
@@ -257,14 +259,14 @@ __global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
         return;
       }
       uses[b] += 1;
-      const uint32_t lo = j * TILE_ELEMS;
-      const uint32_t cnt = min(TILE_ELEMS, n - lo);
+      const uint32_t lo = j * TILE;
+      const uint32_t cnt = min(TILE, n - lo);
       const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
-      const uint32_t wlo = warp * (32 * PART_ROUNDS);
-      unsigned lmask[PART_ROUNDS];
+      const uint32_t wlo = warp * (32 * ROUNDS);
+      unsigned lmask[ROUNDS];
       uint32_t wc = 0;
 #pragma unroll
-      for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+      for (uint32_t r = 0; r < ROUNDS; ++r) {
         const uint32_t q = wlo + r * 32 + lane;
         const bool left = q < cnt && left_bit(sg.bits, (uint32_t)rows[q < cnt ? q : 0]);
         lmask[r] = __ballot_sync(FULL, left);
@@ -281,7 +283,7 @@ __global__ void __launch_bounds__(BIG_THREADS, 4) k_part_big(PartWork w) {
       }
       uint32_t run = carry + woff;
 #pragma unroll
-      for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+      for (uint32_t r = 0; r < ROUNDS; ++r) {
         const uint32_t q = wlo + r * 32 + lane;
         const bool left = (lmask[r] >> lane) & 1u;
         const uint32_t rl = run + __popc(lmask[r] & lt);
@@ -325,18 +327,28 @@ int resident_blocks(K kernel, int threads, size_t dyn_smem = 0) {
   return sms * (per > 0 ? per : 1);
 }
 
-template <typename IdxT>
-int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
-  const size_t smem = RING * ring_buf_bytes<IdxT>();
+template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
+int launch_big_v(const PartWork& w, uint64_t want, cudaStream_t st) {
+  const size_t smem = RING * ring_buf_bytes<IdxT, ROUNDS>();
   static bool configured = false;  // per instantiation; the attribute is per device function
   if (!configured) {
-    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_big<IdxT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_big<IdxT, ROUNDS, RING, MINB>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     configured = true;
   }
-  const int cap = resident_blocks(k_part_big<IdxT>, BIG_THREADS, smem);
-  k_part_big<IdxT><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, smem, st>>>(w);
+  const int cap = resident_blocks(k_part_big<IdxT, ROUNDS, RING, MINB>, BIG_THREADS, smem);
+  k_part_big<IdxT, ROUNDS, RING, MINB><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, smem, st>>>(w);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
+}
+
+// Tiles of 2,048 elements (8 warps x 8 rounds of 32), two ring buffers, six
+// CTAs per SM (at most 40 registers): 16 KB of ring per CTA leaves most of
+// the SM's L1 to the mark bits the chains gather, which measured faster than
+// 4,096-element tiles with three or four buffers.
+template <typename IdxT>
+int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
+  return launch_big_v<IdxT, 8, 2, 6>(w, want, st);
 }
 
 }  // namespace

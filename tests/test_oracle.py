@@ -111,3 +111,26 @@ def test_accuracy_close_to_sklearn():
     ours_score = float(np.mean(O.predict(ours, x[n:]) == y[n:]))
     sk = SkRF(n_estimators=8, random_state=0).fit(x[:n], y[:n]).score(x[n:], y[n:])
     assert ours_score >= 0.9 * sk
+
+
+def test_candidate_shortcut_matches_double_test():
+    """The split scan decides 'x + 1e-5 < x_next' (double) with a float
+    shortcut: equal values never qualify, a float gap above 1e-4 always does.
+    Check the shortcut against the double test on edge and random pairs."""
+    rng = np.random.default_rng(0)
+    base = np.concatenate([
+        rng.normal(size=20000), rng.normal(scale=1e6, size=5000), rng.normal(scale=1e-6, size=5000),
+        [0.0, -0.0, 1e-5, -1e-5, 1e-4, 3e38, -3e38, 1e30, 2.0 ** 37, 65504.0]]).astype(np.float32)
+    gaps = np.concatenate([
+        np.zeros(base.size // 4), rng.uniform(0, 3e-5, base.size // 4),
+        rng.uniform(9e-5, 1.1e-4, base.size // 4), rng.exponential(1e-3, base.size - 3 * (base.size // 4))])
+    x = base
+    xn = (x.astype(np.float64) + gaps.astype(np.float64)).astype(np.float32)
+    near = np.nextafter(x, np.float32(np.inf))  # one ulp apart
+    x = np.concatenate([x, x, xn]).astype(np.float32)
+    xn = np.concatenate([xn, near, x[: xn.size]]).astype(np.float32)  # includes x > x_next pairs
+    exact = (x.astype(np.float64) + 1e-5) < xn.astype(np.float64)
+    with np.errstate(over="ignore", invalid="ignore"):
+        d = (xn - x).astype(np.float32)
+    fast = np.where(~(xn > x), False, np.where(d > np.float32(1e-4), True, exact))
+    np.testing.assert_array_equal(fast, exact)
