@@ -11,6 +11,7 @@ namespace ct {
 
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+const std::string& last_error_text() { return g_last_error; }
 
 size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots);
 int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
@@ -21,6 +22,10 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
 int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
                  const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
                  uint32_t* ov);
+size_t fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees);
+int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* counts, void* scratch,
+                size_t scratch_bytes, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot, uint32_t* ov,
+                cudaStream_t st);
 int predict(const void* nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees, const float* x,
             uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
             cudaStream_t st);
@@ -97,7 +102,7 @@ int ct_bootstrap_compact(const ct_problem* p, const ct_lists* lists, uint32_t sl
       CT_CUDA_TRY(cudaMemcpyAsync(words, workspace, sizeof(words), cudaMemcpyDeviceToHost, st));
       CT_CUDA_TRY(cudaStreamSynchronize(st));
       if (words[1]) {
-        set_last_error("bootstrap compaction look-back wait gave up");
+        set_last_error("bootstrap compaction: a bounded wait for a tile copy gave up");
         return CT_ERR_TIMEOUT;
       }
     }
@@ -231,6 +236,17 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                "NULL argument");
   CT_GUARD(return canonicalize(left, right, feature, threshold, value, n_nodes, out_left, out_right, out_feature,
                                out_threshold, out_value);)
+}
+
+size_t ct_fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees) {
+  return fetch_trees_scratch(total_nodes, n_trees);
+}
+
+int ct_fetch_trees(const ct_tree_buffers* trees, uint32_t n_trees, const uint32_t* counts, void* scratch,
+                   size_t scratch_bytes, uint32_t* out_left, uint32_t* out_right, uint16_t* out_feature,
+                   float* out_threshold, uint32_t* out_value, void* stream) {
+  CT_GUARD(return fetch_trees(trees, n_trees, counts, scratch, scratch_bytes, out_left, out_right, out_feature,
+                              out_threshold, out_value, (cudaStream_t)stream);)
 }
 
 int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,

@@ -13,6 +13,8 @@
 // renumbering.
 #include <algorithm>
 #include <cstring>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "ct_internal.cuh"
@@ -459,6 +461,114 @@ int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* fe
     ot[i] = threshold[r];
     ov[i] = value[r];
   }
+  return CT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Read-back of one fit call's trees: the used prefix of every tree's raw
+// arrays is gathered into contiguous device arrays (one kernel), copied to
+// the host in five transfers, and renumbered breadth-first on host threads.
+namespace {
+
+__global__ void k_gather_trees(ct_tree_buffers tb, const uint32_t* __restrict__ off, uint32_t n_trees,
+                               uint32_t total, uint32_t* __restrict__ out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = n_trees;  // tree t with off[t] <= i < off[t + 1]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) / 2;
+      if (off[mid] <= i) lo = mid; else hi = mid;
+    }
+    const size_t src = (size_t)lo * tb.capacity + (i - off[lo]);
+    out[i] = tb.left[src];
+    out[(size_t)total + i] = tb.right[src];
+    out[2 * (size_t)total + i] = tb.feature[src];
+    out[3 * (size_t)total + i] = __float_as_uint(tb.threshold[src]);
+    out[4 * (size_t)total + i] = tb.value[src];
+  }
+}
+
+// Page-locked staging for the raw read-back, shared by the process and grown
+// on demand (portable across devices).  Page-locked allocation synchronizes
+// the device, so a server reserves its largest size up front.
+struct Staging {
+  std::mutex mu;
+  void* p = nullptr;
+  size_t bytes = 0;
+  int grow(size_t need) {  // caller holds mu
+    if (bytes >= need) return CT_OK;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    CT_CUDA_TRY(cudaHostAlloc(&p, need, cudaHostAllocPortable));
+    bytes = need;
+    return CT_OK;
+  }
+};
+Staging g_staging;
+
+}  // namespace
+
+int fetch_trees_reserve(uint64_t total_nodes) {
+  std::lock_guard<std::mutex> lk(g_staging.mu);
+  return g_staging.grow(5 * total_nodes * sizeof(uint32_t));
+}
+
+size_t fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees) {
+  return 5 * total_nodes * sizeof(uint32_t) + ((size_t)n_trees + 1) * sizeof(uint32_t) + 256;
+}
+
+int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* counts, void* scratch,
+                size_t scratch_bytes, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot, uint32_t* ov,
+                cudaStream_t st) {
+  CT_ARG_CHECK(tb && counts && scratch && ol && orr && of && ot && ov, "fetch trees: NULL argument");
+  std::vector<uint32_t> off(n_trees + 1, 0);
+  for (uint32_t t = 0; t < n_trees; ++t) {
+    CT_ARG_CHECK(counts[t] >= 1 && counts[t] <= tb->capacity, "fetch trees: node count out of range");
+    CT_ARG_CHECK((uint64_t)off[t] + counts[t] < (1ull << 32), "fetch trees: too many nodes for one call");
+    off[t + 1] = off[t] + counts[t];
+  }
+  const uint32_t total = off[n_trees];
+  if (n_trees == 0) return CT_OK;
+  CT_ARG_CHECK(scratch_bytes >= fetch_trees_scratch(total, n_trees), "fetch trees: scratch too small");
+  uint32_t* d_cols = reinterpret_cast<uint32_t*>(scratch);
+  uint32_t* d_off = d_cols + 5 * (size_t)total;
+  CT_CUDA_TRY(cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
+  k_gather_trees<<<std::min<uint32_t>(ceil_div(total, 256), 148 * 16), 256, 0, st>>>(*tb, d_off, n_trees, total,
+                                                                                    d_cols);
+  CT_CUDA_TRY(cudaGetLastError());
+  std::lock_guard<std::mutex> lk(g_staging.mu);
+  CT_TRY(g_staging.grow((size_t)5 * total * sizeof(uint32_t)));
+  CT_CUDA_TRY(cudaMemcpyAsync(g_staging.p, d_cols, (size_t)5 * total * 4, cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint32_t* hl = static_cast<const uint32_t*>(g_staging.p);
+  const uint32_t* hr = hl + total;
+  const uint32_t* hf = hr + total;
+  const float* ht = reinterpret_cast<const float*>(hf + total);
+  const uint32_t* hv = hf + 2 * (size_t)total;
+  const uint32_t workers = std::max(1u, std::min({n_trees, 16u, std::thread::hardware_concurrency()}));
+  std::vector<int> status(workers, CT_OK);
+  std::vector<std::string> errors(workers);
+  auto run = [&](uint32_t w) {
+    for (uint32_t t = w; t < n_trees; t += workers) {
+      const uint32_t o = off[t];
+      const int rc = canonicalize(hl + o, hr + o, hf + o, ht + o, hv + o, counts[t], ol + o, orr + o, of + o,
+                                  ot + o, ov + o);
+      if (rc != CT_OK) {
+        status[w] = rc;
+        errors[w] = "tree " + std::to_string(t) + ": " + last_error_text();
+        return;
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (uint32_t w = 1; w < workers; ++w) pool.emplace_back(run, w);
+  run(0);
+  for (auto& th : pool) th.join();
+  for (uint32_t w = 0; w < workers; ++w)
+    if (status[w] != CT_OK) {
+      set_last_error(errors[w]);
+      return status[w];
+    }
   return CT_OK;
 }
 

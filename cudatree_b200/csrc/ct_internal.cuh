@@ -15,6 +15,7 @@ namespace ct {
 
 // -------------------------------------------------------------- errors ---
 void set_last_error(const std::string& msg);
+const std::string& last_error_text();  // this thread's last error
 #define CT_CUDA_TRY(expr)                                                              \
   do {                                                                                 \
     cudaError_t _e = (expr);                                                           \

@@ -216,24 +216,43 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   uint32_t bpos = NONE;
   float bil = 0.f, bir = 0.f;
   const unsigned lt = lanemask_lt();
-  for (uint32_t base = lo; base < hi; base += 32 * SCAN_BATCH) {
-    // loads of the whole batch first: index, then label and value
-    uint32_t rows[SCAN_BATCH], cs[SCAN_BATCH];
-    float xs[SCAN_BATCH];
+  // Software pipeline over batches of SCAN_BATCH rounds: while batch b is
+  // scanned, the label/value gathers of batch b+1 and the index loads of
+  // batch b+2 are in flight.
+  constexpr uint32_t B = 32 * SCAN_BATCH;
+  uint32_t rows_n[SCAN_BATCH], cs[SCAN_BATCH];
+  float xs[SCAN_BATCH];
+  {
+    uint32_t rows[SCAN_BATCH];
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
-      const uint32_t p = base + r * 32 + lane;
+      const uint32_t p = lo + r * 32 + lane;
       rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+      const uint32_t q = p + B;
+      rows_n[r] = q < hi ? (uint32_t)lst[q] : 0u;
     }
-    const uint32_t pe = base + 32 * SCAN_BATCH;  // first position after the batch
-    const uint32_t row_e = (lane == 31 && pe < hi) ? (uint32_t)lst[pe] : 0u;
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
-      const bool valid = base + r * 32 + lane < hi;
+      const bool valid = lo + r * 32 + lane < hi;
       cs[r] = valid ? label_of<LabT>(v, rows[r]) : NONE;
       xs[r] = valid ? xf[rows[r]] : 0.f;
     }
-    const float x_e = (lane == 31 && pe < hi) ? xf[row_e] : 0.f;
+  }
+  for (uint32_t base = lo; base < hi; base += B) {
+    uint32_t cs_n[SCAN_BATCH];
+    float xs_n[SCAN_BATCH];
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const bool valid = base + B + r * 32 + lane < hi;
+      cs_n[r] = valid ? label_of<LabT>(v, rows_n[r]) : NONE;
+      xs_n[r] = valid ? xf[rows_n[r]] : 0.f;
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      const uint32_t q = base + 2 * B + r * 32 + lane;
+      rows_n[r] = q < hi ? (uint32_t)lst[q] : 0u;
+    }
+    const float x_e = __shfl_sync(FULL, xs_n[0], 0);  // first value of the next batch
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t p = base + r * 32 + lane;
@@ -286,6 +305,11 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
           bir = __double2float_rn(gr);
         }
       }
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+      cs[r] = cs_n[r];
+      xs[r] = xs_n[r];
     }
   }
   warp_argmin2(best, bpos, bil, bir);

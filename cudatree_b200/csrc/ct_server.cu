@@ -47,9 +47,11 @@ namespace ct {
 size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
 int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees, const ct_fit_options* o,
         const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
-int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
-                 const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
-                 uint32_t* ov);
+size_t fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees);
+int fetch_trees_reserve(uint64_t total_nodes);
+int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* counts, void* scratch,
+                size_t scratch_bytes, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot, uint32_t* ov,
+                cudaStream_t st);
 size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features);
 int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
             size_t wsb, cudaStream_t st);
@@ -231,6 +233,9 @@ class Server {
     }
     const uint32_t nfw = cfg.fit_workers;
     fit_workers.resize(nfw);
+    // page-locked read-back staging for the largest fit job, taken now: a
+    // page-locked allocation while requests run would stall every stream
+    if (nfw) CT_TRY(fetch_trees_reserve((uint64_t)cfg.max_fit_trees * 2 * cfg.max_fit_rows));
     const size_t arena = fit_arena_bytes();
     for (auto& fw : fit_workers) {
       CT_CUDA_TRY(cudaStreamCreateWithPriority(&fw.st, cudaStreamNonBlocking, prio_lo));
@@ -276,6 +281,7 @@ class Server {
     add(mb);                           // marks
     add((size_t)t * 2 * n * 4 * 5);    // raw trees
     add((size_t)t * 4);                // node counts
+    add(fetch_trees_scratch((uint64_t)t * 2 * n, t));  // tree read-back
     add(fit_workspace_bytes(&p, t, &o));
     return b + 4096;
   }
@@ -669,6 +675,8 @@ class Server {
     const uint32_t cap = 2 * n;
     uint32_t* raw = a.take<uint32_t>((size_t)T * cap * 5);
     uint32_t* counts = a.take<uint32_t>(T);
+    const size_t fsb = fetch_trees_scratch((uint64_t)T * 2 * n, T);
+    char* fscratch = a.take<char>(fsb);
     ct_problem p{};
     p.x_fm = x_fm;
     p.labels = labels;
@@ -710,26 +718,20 @@ class Server {
     std::vector<uint32_t> cnt(T);
     CT_CUDA_TRY(cudaMemcpyAsync(cnt.data(), counts, T * 4, cudaMemcpyDeviceToHost, st));
     CT_CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<ct_packed_node> packed;
+    uint64_t total = 0;
     std::vector<uint32_t> offs(T);
-    std::vector<uint32_t> h[5];
     for (uint32_t t = 0; t < T; ++t) {
-      const uint32_t nn = cnt[t];
-      for (int k = 0; k < 5; ++k) {
-        h[k].resize(nn);
-        CT_CUDA_TRY(cudaMemcpyAsync(h[k].data(), raw + (size_t)k * T * cap + (size_t)t * cap, nn * 4,
-                                    cudaMemcpyDeviceToHost, st));
-      }
-      CT_CUDA_TRY(cudaStreamSynchronize(st));
-      std::vector<uint32_t> ol(nn), orr(nn), ov(nn);
-      std::vector<uint16_t> of(nn);
-      std::vector<float> ot(nn);
-      CT_TRY(canonicalize(h[0].data(), h[1].data(), h[2].data(), reinterpret_cast<const float*>(h[3].data()),
-                          h[4].data(), nn, ol.data(), orr.data(), of.data(), ot.data(), ov.data()));
-      offs[t] = (uint32_t)packed.size();
-      for (uint32_t i = 0; i < nn; ++i) packed.push_back(ct_packed_node{ot[i], of[i], ol[i], ov[i]});
+      offs[t] = (uint32_t)total;
+      total += cnt[t];
     }
-    return add_forest(packed.data(), (uint32_t)packed.size(), offs.data(), T, F, C, fid, st);
+    std::vector<uint32_t> ol(total), orr(total), ov(total);
+    std::vector<uint16_t> of(total);
+    std::vector<float> ot(total);
+    CT_TRY(fetch_trees(&tb, T, cnt.data(), fscratch, fsb, ol.data(), orr.data(), of.data(), ot.data(), ov.data(),
+                       st));
+    std::vector<ct_packed_node> packed(total);
+    for (uint64_t i = 0; i < total; ++i) packed[i] = ct_packed_node{ot[i], of[i], ol[i], ov[i]};
+    return add_forest(packed.data(), (uint32_t)total, offs.data(), T, F, C, fid, st);
   }
 
   static double pct(std::vector<double> v, double q) {

@@ -270,22 +270,27 @@ class RandomForestClassifier:
                     stats[key] = [a + b for a, b in zip(stats[key], st[key])]
                 stats["steps"] += st["steps"]
                 stats["total_launches"] += st["total_launches"]
-            counts = n_nodes[:kk].cpu().numpy().astype(np.int64)
-            for s in range(kk):
-                trees.append(self._canonical_tree(raw, s * cap, int(counts[s])))
+            trees.extend(self._fetch_trees(tb, n_nodes, kk, dev))
         self.last_fit_stats = stats
         return trees
 
-    def _canonical_tree(self, raw, off, n_nodes):
-        host = {k: v[off:off + n_nodes].cpu().numpy() for k, v in raw.items()}
-        left = np.empty(n_nodes, np.uint32)
-        right = np.empty(n_nodes, np.uint32)
-        feat = np.empty(n_nodes, np.uint16)
-        thr = np.empty(n_nodes, np.float32)
-        val = np.empty(n_nodes, np.uint32)
-        src = [np.ascontiguousarray(host[k]) for k in ("left", "right", "feature", "threshold", "value")]
-        _lib.call("ct_tree_canonicalize", *[a.ctypes.data for a in src], n_nodes, left.ctypes.data,
-                  right.ctypes.data, feat.ctypes.data, thr.ctypes.data, val.ctypes.data)
+    def _fetch_trees(self, tb, n_nodes, kk, dev):
+        """The kk trees of the last ct_fit call, canonical order, as tree objects
+        over slices of five concatenated host arrays (one read-back)."""
+        counts = n_nodes[:kk].cpu().numpy().astype(np.uint32)
+        total = int(counts.sum())
+        cols = [np.empty(total, dt) for dt in (np.uint32, np.uint32, np.uint16, np.float32, np.uint32)]
+        sb = int(_lib.load().ct_fetch_trees_scratch(total, kk))
+        scratch = _dev_bytes(sb, dev)
+        _lib.call("ct_fetch_trees", C.byref(tb), kk, counts.ctypes.data, _ptr(scratch), sb,
+                  *[c.ctypes.data for c in cols], _stream())
+        out, o = [], 0
+        for c in counts.tolist():
+            out.append(self._make_tree(*[col[o:o + c] for col in cols]))
+            o += c
+        return out
+
+    def _make_tree(self, left, right, feat, thr, val):
         tree = RandomClassifierTree(self)
         tree.left_children = left
         tree.right_children = right

@@ -215,6 +215,17 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                          uint32_t* out_left, uint32_t* out_right, uint16_t* out_feature,
                          float* out_threshold, uint32_t* out_value);
 
+/* Reads back the trees of one ct_fit call in canonical order.  counts[t]
+ * (host) is trees->n_nodes[t]; tree t lands at [o_t, o_t + counts[t]) of the
+ * host output arrays, o_t = counts[0] + ... + counts[t-1].  The used nodes
+ * are gathered on the device into scratch (ct_fetch_trees_scratch bytes),
+ * copied in one transfer, and renumbered on host threads.  Replaces the
+ * full-buffer readback of decorate (random_tree.py:50-63). */
+size_t ct_fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees);
+int ct_fetch_trees(const ct_tree_buffers* trees, uint32_t n_trees, const uint32_t* counts,
+                   void* scratch, size_t scratch_bytes, uint32_t* out_left, uint32_t* out_right,
+                   uint16_t* out_feature, float* out_threshold, uint32_t* out_value, void* stream);
+
 /* ----------------------------------------------------------- predict --- */
 /* Packed forest: node i of the flat array is {threshold, feature, left, value}
  * with children left and left+1 inside the tree (breadth-first order);
