@@ -130,6 +130,8 @@ PROTOTYPES = {
     "ct_server_destroy": (C.c_int, [P]),
     "ct_server_add_forest": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),
     "ct_server_remove_forest": (C.c_int, [P, C.c_uint32]),
+    "ct_server_forest_info": (C.c_int, [P, C.c_uint32, P, P, P, P]),
+    "ct_server_read_forest": (C.c_int, [P, C.c_uint32, P, P]),
     "ct_server_submit": (C.c_int, [P, P]),
     "ct_server_wait": (C.c_int, [P, P, C.c_double]),
     "ct_server_replay": (C.c_int, [P, P, C.c_uint32, C.c_double, P]),

@@ -75,6 +75,8 @@ double now_s() {
 }
 
 struct Forest {
+  std::shared_ptr<std::vector<ct_packed_node>> host;  // exact packed copy (read-back)
+  std::shared_ptr<std::vector<uint32_t>> host_off;
   void* nodes = nullptr;  // compact nodes when fbits != 0, else packed
   uint32_t fbits = 0;
   uint32_t* off = nullptr;
@@ -370,9 +372,37 @@ class Server {
       set_last_error("server: forest upload failed");
       return CT_ERR_CUDA;
     }
+    f.host = std::make_shared<std::vector<ct_packed_node>>(nodes, nodes + n_nodes);
+    f.host_off = std::make_shared<std::vector<uint32_t>>(off, off + n_trees);
     std::lock_guard<std::mutex> lk(mu);
     forests.push_back(f);
     *id = (uint32_t)(forests.size() - 1);
+    return CT_OK;
+  }
+
+  int forest_info(uint32_t id, uint32_t* n_nodes, uint32_t* n_trees, uint32_t* n_features, uint32_t* n_classes) {
+    std::lock_guard<std::mutex> lk(mu);
+    CT_ARG_CHECK(id < forests.size() && !forests[id].removed, "server: unknown forest id");
+    const Forest& f = forests[id];
+    if (n_nodes) *n_nodes = f.n_nodes;
+    if (n_trees) *n_trees = f.n_trees;
+    if (n_features) *n_features = f.n_features;
+    if (n_classes) *n_classes = f.n_classes;
+    return CT_OK;
+  }
+
+  int read_forest(uint32_t id, ct_packed_node* nodes, uint32_t* off) {
+    std::shared_ptr<std::vector<ct_packed_node>> h;
+    std::shared_ptr<std::vector<uint32_t>> o;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      CT_ARG_CHECK(id < forests.size() && !forests[id].removed, "server: unknown forest id");
+      h = forests[id].host;
+      o = forests[id].host_off;
+    }
+    CT_ARG_CHECK(nodes && off, "server: NULL output");
+    std::copy(h->begin(), h->end(), nodes);
+    std::copy(o->begin(), o->end(), off);
     return CT_OK;
   }
 
@@ -381,6 +411,8 @@ class Server {
     CT_ARG_CHECK(id < forests.size() && !forests[id].removed, "server: unknown forest id");
     Forest& f = forests[id];
     f.removed = true;
+    f.host.reset();
+    f.host_off.reset();
     if (f.refs == 0) pool.release(f.pool_off, f.bytes);
     return CT_OK;
   }
@@ -806,6 +838,17 @@ int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_n
   CT_ARG_CHECK(handle, "NULL server");
   return reinterpret_cast<Server*>(handle)->add_forest(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes,
                                                         forest_id);
+}
+
+int ct_server_forest_info(void* handle, uint32_t forest_id, uint32_t* n_nodes, uint32_t* n_trees,
+                          uint32_t* n_features, uint32_t* n_classes) {
+  CT_ARG_CHECK(handle, "NULL server");
+  return reinterpret_cast<Server*>(handle)->forest_info(forest_id, n_nodes, n_trees, n_features, n_classes);
+}
+
+int ct_server_read_forest(void* handle, uint32_t forest_id, ct_packed_node* nodes, uint32_t* tree_offset) {
+  CT_ARG_CHECK(handle, "NULL server");
+  return reinterpret_cast<Server*>(handle)->read_forest(forest_id, nodes, tree_offset);
 }
 
 int ct_server_remove_forest(void* handle, uint32_t forest_id) {

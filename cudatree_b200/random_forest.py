@@ -100,6 +100,23 @@ def pack_trees(trees):
     return packed, offsets
 
 
+def unpack_trees(packed, offsets, n_features, dtype_labels):
+    """Inverse of pack_trees: RandomClassifierTree objects from packed nodes."""
+    from .random_tree import restore_tree
+    packed = np.asarray(packed, dtype=PACKED_DTYPE)
+    offsets = np.asarray(offsets, dtype=np.int64)
+    ends = np.append(offsets[1:], packed.shape[0])
+    dt = np.dtype(dtype_labels)
+    trees = []
+    for o, e in zip(offsets.tolist(), ends.tolist()):
+        sl = packed[o:e]
+        left = sl["left"].astype(np.uint32)
+        right = np.where(left != 0, left + 1, 0).astype(np.uint32)
+        trees.append(restore_tree(left, right, sl["threshold"].astype(np.float32), sl["value"].astype(dt),
+                                  sl["feature"].astype(np.uint16), dt.str, n_features))
+    return trees
+
+
 def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_votes, compact=False):
     """Walk the forest on the device: packed nodes (ct_predict) or, with
     compact=True, a device tensor of 8-byte compact nodes (ct_predict_compact)."""

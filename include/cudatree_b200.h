@@ -332,6 +332,13 @@ int ct_server_destroy(void* handle);
 int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes,
                          const uint32_t* tree_offset, uint32_t n_trees, uint32_t n_features,
                          uint32_t n_classes, uint32_t* forest_id);
+/* Size and shape of a resident forest, then its exact packed nodes and tree
+ * offsets (host arrays of n_nodes and n_trees entries): forests fitted by
+ * fit jobs can be read back, compared or serialized. */
+int ct_server_forest_info(void* handle, uint32_t forest_id, uint32_t* n_nodes, uint32_t* n_trees,
+                          uint32_t* n_features, uint32_t* n_classes);
+int ct_server_read_forest(void* handle, uint32_t forest_id, ct_packed_node* nodes,
+                          uint32_t* tree_offset);
 /* Retires a forest: new requests for it fail with CT_ERR_ARG; its pool bytes
  * return once the batches already launched on it have completed. */
 int ct_server_remove_forest(void* handle, uint32_t forest_id);

@@ -153,3 +153,41 @@ def test_forest_pool_remove_and_reuse(cuda_device):
     b = srv.add_forest(forest)
     np.testing.assert_array_equal(srv.predict(b, x), forest.predict(x))
     srv.close()
+
+
+def _same_trees(a, b):
+    assert len(a._trees) == len(b._trees)
+    for s, t in zip(a._trees, b._trees):
+        np.testing.assert_array_equal(s.left_children, t.left_children)
+        np.testing.assert_array_equal(s.right_children, t.right_children)
+        np.testing.assert_array_equal(s.feature_idx_array, t.feature_idx_array)
+        np.testing.assert_array_equal(s.feature_threshold_array, t.feature_threshold_array)
+        np.testing.assert_array_equal(s.values_array.astype(np.int64), t.values_array.astype(np.int64))
+
+
+def test_read_forest_round_trip(served):
+    srv, forests = served
+    for fid, forest, x in forests:
+        back = srv.forest(fid)
+        _same_trees(back, forest)
+        np.testing.assert_array_equal(back.predict(x[:500]), forest.predict(x[:500]))
+
+
+def test_forest_queue_matches_solo_fits(cuda_device):
+    """Uneven jobs fitted concurrently through the queue give, job by job, the
+    trees a solo fit with the same seed gives."""
+    from cudatree_b200.serving import fit_forests
+    rng = np.random.default_rng(12)
+    jobs = []
+    for j in range(7):
+        n = int(rng.integers(300, 6000))
+        f = int(rng.integers(3, 90))
+        c = int(rng.integers(2, 12))
+        x, y = _blobs(n, f, c, 100 + j)
+        jobs.append((x, y * 3 + 1))  # labels that need compaction
+    seeds = [1000 + j for j in range(len(jobs))]
+    got = fit_forests(jobs, n_estimators=6, seeds=seeds, workers=3)
+    for (x, y), seed, g in zip(jobs, seeds, got):
+        solo = RandomForestClassifier(n_estimators=6, seed=seed).fit(x, y)
+        _same_trees(g, solo)
+        np.testing.assert_array_equal(g.predict(x), solo.predict(x))
