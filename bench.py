@@ -163,6 +163,95 @@ def run_reference(args, world, rank):
     return 0
 
 
+# ------------------------------------------------------------ other configs
+def _sk_fit_s(x, y, trees, max_features, bootstrap, cores):
+    from sklearn.ensemble import RandomForestClassifier as SkRF
+    rf = SkRF(n_estimators=trees, max_features=max_features, bootstrap=bootstrap, n_jobs=cores, random_state=0)
+    t0 = time.perf_counter()
+    rf.fit(x, y)
+    return time.perf_counter() - t0, rf
+
+
+def _fit_pair(x, y, n_trees, m, bootstrap, bfs_threshold, seed, plain_trees):
+    """Batched fit seconds (warm, CUDA events), plain fit seconds on plain_trees
+    trees scaled to n_trees, and whether plain grew the same trees."""
+    import torch
+
+    from cudatree_b200 import RandomForestClassifier, _lib
+    f = RandomForestClassifier(n_trees, max_features=m, bootstrap=bootstrap, seed=seed)
+    f.fit_init(x, y)
+    thr = f.bfs_threshold if bfs_threshold is None else bfs_threshold
+    f._fit_trees(0, n_trees, "batched", thr)  # warm-up
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    trees = f._fit_trees(0, n_trees, "batched", thr)
+    e1.record(st)
+    torch.cuda.synchronize()
+    batched_s = e0.elapsed_time(e1) / 1000.0
+    f.profile = True
+    f._fit_trees(0, n_trees, "batched", thr)
+    stats = f.last_fit_stats
+    f.profile = False
+    t0 = time.perf_counter()
+    ptrees = f._fit_trees(0, plain_trees, "plain", thr)
+    torch.cuda.synchronize()
+    plain_s = (time.perf_counter() - t0) * n_trees / plain_trees
+    same = all(np.array_equal(a.left_children, b.left_children) and
+               np.array_equal(a.feature_threshold_array, b.feature_threshold_array) and
+               np.array_equal(a.values_array, b.values_array) for a, b in zip(ptrees, trees))
+    f.fit_release()
+    gi = {g: i for i, g in enumerate(_lib.KERNEL_GROUPS)}
+    gbs = {g: round(stats["bytes"][gi[g]] / (stats["ms"][gi[g]] * 1e6), 1) if stats["ms"][gi[g]] > 0 else None
+           for g in ("scan", "partition")}
+    return batched_s, plain_s, same, gbs, sum(t.n_nodes for t in trees)
+
+
+def run_configs(args):
+    """The reference's other configurations: digits-shaped (1,797 x 64, 50
+    trees, no bootstrap, bfs_threshold 4196), wide (10,000 x 3,000, 100
+    classes, 200 trees, max_features 55, uint16 indices) and the queue of 256
+    uneven jobs (10 trees each), each beside scikit-learn on the same host."""
+    from cudatree_b200 import RandomForestClassifier, synthetic
+    from cudatree_b200.serving import fit_forests
+    cores = len(os.sched_getaffinity(0))
+    out = {}
+    x, y = synthetic.digits_like()
+    b, p, same, gbs, nodes = _fit_pair(x, y, 50, 8, False, 4196, 11, 50)
+    sk, _ = _sk_fit_s(x, y, 50, 8, False, cores)
+    out["digits_1797x64_50trees"] = {"batched_fit_s": b, "plain_fit_s": p, "plain_trees_identical": same,
+                                     "nodes": nodes, "sklearn_fit_s": sk, "sklearn_cores": cores}
+    x, y = synthetic.wide()
+    b, p, same, gbs, nodes = _fit_pair(x, y, 200, 55, True, None, 12, 10)
+    sk, _ = _sk_fit_s(x, y, 32, 55, True, cores)
+    out["wide_10000x3000_c100_200trees"] = {
+        "batched_fit_s": b, "plain_fit_s": p, "plain_sample": "10 trees scaled to 200",
+        "plain_trees_identical": same, "nodes": nodes, "kernel_GB_per_s": gbs,
+        "sklearn_fit_s": sk * 200 / 32, "sklearn_sample": "32 trees scaled to 200", "sklearn_cores": cores}
+    n_jobs = args.queue_jobs
+    jobs = [synthetic.blob_job(j) for j in range(n_jobs)]
+    fit_forests(jobs[:4], n_estimators=10, seeds=range(4), workers=4)  # warm-up
+    t0 = time.perf_counter()
+    forests = fit_forests(jobs, n_estimators=10, seeds=range(n_jobs), workers=args.queue_workers)
+    q_s = time.perf_counter() - t0
+    checked = list(range(0, n_jobs, max(1, n_jobs // 8)))
+    same = True
+    for j in checked:
+        solo = RandomForestClassifier(10, seed=j).fit(*jobs[j])
+        same &= all(np.array_equal(a.left_children, c.left_children) and
+                    np.array_equal(a.feature_threshold_array, c.feature_threshold_array)
+                    for a, c in zip(forests[j]._trees, solo._trees))
+    sample = min(16, n_jobs)
+    sk = sum(_sk_fit_s(jobs[j][0], jobs[j][1], 10, int(np.ceil(np.sqrt(jobs[j][0].shape[1]))), True, cores)[0]
+             for j in range(sample))
+    out[f"queue_{n_jobs}_jobs_10trees"] = {
+        "total_s": q_s, "jobs_per_s": n_jobs / q_s, "workers": args.queue_workers,
+        "trees_identical_to_solo_fits": bool(same), "checked_jobs": len(checked),
+        "sklearn_sequential_s": sk * n_jobs / sample, "sklearn_sample": f"{sample} jobs scaled to {n_jobs}",
+        "sklearn_cores": cores}
+    return out
+
+
 # ------------------------------------------------------------------ serving
 def run_serving(args, x_cov, y_cov, seed):
     """Serving workload: a 500-tree covtype-shaped forest + 8 resident forests
@@ -382,6 +471,7 @@ def run_ours(args, world, rank, local):
     d2h = sum(t.n_nodes for t in trees) * 20 + 4 * n_trees
 
     serving = None if args.skip_serving else run_serving(args, x, y, seed)
+    configs = None if args.skip_configs or rank != 0 else run_configs(args)
     if rank != 0:
         return 0
     peak, peak_kind = peaks()
@@ -435,6 +525,7 @@ def run_ours(args, world, rank, local):
                           "achieved": round(stats["bytes"][si] / (s_ms * 1e6), 1) if s_ms > 0 else None,
                           "peak": peak, "unit": "GB/s"},
         "predict": serving,
+        "configs": configs,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": int(x.nbytes + y.shape[0]),
                 "d2h_bytes_per_step": int(d2h)},
@@ -463,6 +554,10 @@ def main():
     ap.add_argument("--rate", type=float, default=2000.0)
     ap.add_argument("--fit-frac", type=float, default=0.05, help="fraction of serving requests that are fit jobs")
     ap.add_argument("--serving-only", action="store_true", help="run the serving workload alone (profiling runs)")
+    ap.add_argument("--skip-configs", action="store_true", help="skip the digits, wide and queue configurations")
+    ap.add_argument("--configs-only", action="store_true", help="run only the digits, wide and queue configurations")
+    ap.add_argument("--queue-jobs", type=int, default=256)
+    ap.add_argument("--queue-workers", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
@@ -470,6 +565,10 @@ def main():
     if args.predict_only:
         dist_setup(1)
         return run_predict_only(args)
+    if args.configs_only:
+        dist_setup(1)
+        print(json.dumps({"configs": run_configs(args)}), flush=True)
+        return 0
     if args.serving_only:
         dist_setup(1)
         from cudatree_b200 import synthetic
