@@ -96,7 +96,6 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
 
 __global__ void k_begin_level(Counters* c) {
   c->n_next = 0;
-  c->n_small = 0;
   c->next_total = 0;
   c->small_total = 0;
   c->split_total = 0;
@@ -123,6 +122,10 @@ struct FitLayout {
   uint32_t cap_list;
   uint32_t chunk;
   uint32_t scan_piece;
+  uint32_t subtree_cut;  // nodes of at most this many rows are grown by warp subtrees (0: off)
+  uint32_t cap_small;
+  ct_node* small;        // small nodes waiting for their warp subtree (kept across levels)
+  mutable uint64_t small_bound;  // upper bound of the entries in small
   uint32_t* n_in;
   ct_node* list[2];
   uint32_t* tot[2];
@@ -142,7 +145,12 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->cap_list = (uint32_t)std::min<uint64_t>(cap_list64, 0xffffffffull);
   L->chunk = std::min<uint32_t>(L->cap_list, CHUNK_NODES_MAX);
   L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
+  // the warp subtree packs a row id into 27 bits of its sort key
+  L->subtree_cut = p->n_rows < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 32u) : 0u;
+  L->cap_small = L->subtree_cut ? 2 * L->chunk : 0u;
   Arena a{base, size, 0};
+  L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
+  L->small_bound = 0;
   L->n_in = a.take<uint32_t>(slots);
   for (int i = 0; i < 2; ++i) {
     L->list[i] = a.take<ct_node>(L->cap_list);
@@ -225,6 +233,18 @@ int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot_l
   return launch_root<uint32_t, uint16_t>(v, L, slot_lo, n_slots, p->seed, tree_lo, tv, cur, st);
 }
 
+// Grow the warp subtrees of every small node set aside so far.  Their rows
+// stay valid in their list buffer: later steps write only other nodes'
+// (disjoint) ranges.  Deferring them to one launch lets long subtrees overlap.
+int flush_subtrees(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, cudaStream_t st) {
+  if (!L.subtree_cut || L.small_bound == 0) return CT_OK;
+  CT_TRY(launch_subtrees(v, p->index_bytes, p->label_bytes, L.small,
+                         (uint32_t)std::min<uint64_t>(L.small_bound, L.cap_small), L.s, tv, st));
+  CT_CUDA_TRY(cudaMemsetAsync(&L.s.ctr->n_small, 0, sizeof(uint32_t), st));
+  L.small_bound = 0;
+  return CT_OK;
+}
+
 // One step over list[cur][0..n) -> children appended to list[1-cur].
 int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, int cur, uint32_t n,
          uint64_t total, cudaStream_t st) {
@@ -234,11 +254,13 @@ int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView&
     const ct_node* nodes = L.list[cur] + lo;
     const uint32_t* tot = L.tot[cur] + (size_t)lo * C;
     const LevelBounds b{cn, total};
+    if (L.subtree_cut && L.small_bound + 2ull * cn > L.cap_small) CT_TRY(flush_subtrees(p, v, L, tv, st));
     CT_TRY(launch_reset_step(L.s.ctr, cn, st));
     CT_TRY(launch_split(v, ib, lb, nodes, tot, L.s, b, L.scan_piece, st));
     CT_TRY(launch_partition(v, ib, lb, nodes, L.s, b, tv, st));
     CT_TRY(launch_children(v, ib, lb, nodes, tot, L.s, b, tv, L.list[1 - cur], L.tot[1 - cur], L.cap_list,
-                           0, nullptr, 0, st));
+                           L.subtree_cut, L.small, L.cap_small, st));
+    if (L.subtree_cut) L.small_bound += 2ull * cn;
   }
   return CT_OK;
 }
@@ -252,6 +274,7 @@ int level_loop(const ct_problem* p, const View& v, const FitLayout& L, const Tre
     CT_TRY(step(p, v, L, tv, cur, n, total, st));
     CT_TRY(read_counters(L, &h, st));
     account_level(p, h);
+    if (L.subtree_cut) L.small_bound = h.n_small;
     n = h.n_next;
     total = h.next_total;
     cur = 1 - cur;
@@ -297,7 +320,12 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
   CT_TRY(root(p, v, L, 0, n_trees, first_tree, tv, 0, st));
   Counters h;
   CT_TRY(read_counters(L, &h, st));
-  return level_loop(p, v, L, tv, 0, h.n_next, h.next_total, st);
+  CT_TRY(level_loop(p, v, L, tv, 0, h.n_next, h.next_total, st));
+  if (L.small_bound) {
+    CT_TRY(flush_subtrees(p, v, L, tv, st));
+    CT_TRY(read_counters(L, &h, st));
+  }
+  return CT_OK;
 }
 
 int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
@@ -344,6 +372,7 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
       CT_TRY(step(p, v, L, tv, 0, 1, cur.nd.n, st));
       CT_TRY(read_counters(L, &h, st));
       account_level(p, h);
+      if (L.subtree_cut) L.small_bound = h.n_small;
       std::vector<ct_node> kids(h.n_next);
       std::vector<uint32_t> ktot((size_t)h.n_next * C);
       if (h.n_next) {
@@ -382,6 +411,10 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
       CT_CUDA_TRY(cudaMemcpyAsync(L.tot[0], tots.data(), tots.size() * sizeof(uint32_t),
                                   cudaMemcpyHostToDevice, st));
       CT_TRY(level_loop(p, v, L, tv, 0, (uint32_t)nodes.size(), total, st));
+    }
+    if (L.small_bound) {  // this tree's subtrees, before the next tree reuses the slot
+      CT_TRY(flush_subtrees(p, v, L, tv, st));
+      CT_TRY(read_counters(L, &h, st));
     }
   }
   return CT_OK;

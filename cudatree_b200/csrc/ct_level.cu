@@ -580,6 +580,179 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
   }
 }
 
+// ------------------------------------------------------------------------
+// Warp subtrees.  A node of at most 32 rows is grown to its leaves by one
+// warp, one row per lane, without partitioning any feature list: below such
+// a node, re-partitioning all F lists every level costs far more than the m
+// features each node scans.  The rows are read from feature 0's list, so
+// lane order is feature-0 order and a node's leaf label is the label of its
+// lowest lane (the first-row rule of the level steps).  A sub-node is a mask
+// of lanes.  Per node the selected features are those of k_select (first m
+// non-constant ones of the node's permutation); each is sorted across the
+// lanes by (value, row) with a bitonic network, the sorted order the index
+// lists hold, and scanned with the arithmetic of k_split_scan; the best is the
+// lowest (score, feature id, position).  Pending nodes sit on a per-warp
+// stack in shared memory; raw node ids come from the tree's node counter
+// (the host renumbers breadth-first), so the trees are the level steps' trees.
+struct SubEntry {
+  uint32_t mask;
+  uint32_t raw;
+  uint64_t key;
+};
+
+__device__ __forceinline__ uint64_t warp_sort_u64(uint64_t v, uint32_t lane) {
+#pragma unroll
+  for (uint32_t k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      const uint64_t o = __shfl_xor_sync(FULL, v, j);
+      const bool up = (lane & k) == 0u;
+      const bool lo = (lane & j) == 0u;
+      v = (lo == up) ? (o < v ? o : v) : (o > v ? o : v);
+    }
+  }
+  return v;
+}
+
+template <typename IdxT, typename LabT>
+__device__ __forceinline__ void subtree_leaf(const View& v, const TreeView& tv, size_t toff, uint32_t raw,
+                                             uint32_t mask, uint32_t lab, uint32_t lane) {
+  const uint32_t value = __shfl_sync(FULL, lab, __ffs(mask) - 1);
+  if (lane == 0) {
+    tv.left[toff + raw] = 0;
+    tv.right[toff + raw] = 0;
+    tv.feature[toff + raw] = 0;
+    tv.threshold[toff + raw] = 0.f;
+    tv.value[toff + raw] = value;
+  }
+}
+
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
+  __shared__ SubEntry stack_all[WARPS_PER_BLOCK][33];
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
+  SubEntry* stack = stack_all[threadIdx.x >> 5];
+  const ct_node nd = small[w];
+  const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+  const bool have = lane < nd.n;
+  const uint32_t row = have ? (uint32_t)l0[lane] : 0u;
+  const uint32_t lab = have ? label_of<LabT>(v, row) : NONE;
+  const uint32_t F = v.n_features, m = v.max_features;
+  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+  const unsigned lt = lanemask_lt();
+  int sp = 0;
+  SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
+  while (true) {
+    const uint32_t mask = cur.mask;
+    const uint32_t n = __popc(mask);
+    const bool in = (mask >> lane) & 1u;
+    // class totals of the node: Σ_c T_c² as a sum over its rows of T_(c(row))
+    const uint32_t tcls = __popc(__match_any_sync(FULL, in ? lab : NONE));
+    const int64_t sr0 = (int64_t)warp_sum_u32(in ? tcls : 0u);
+    const double nn = (double)n;
+    double best = dinf();
+    uint32_t bf = NONE, bp = 0, bmask = 0;
+    float bil = 0.f, bir = 0.f, bthr = 0.f;
+    uint32_t taken = 0;
+    // the next feature's values are gathered while the current one is sorted and scanned
+    uint32_t f_nx = feature_perm(0, F, cur.key, v.feistel_h);
+    float x_nx = in ? v.x_fm[(size_t)f_nx * v.n_rows + row] : 0.f;
+    for (uint32_t i = 0; i < F && taken < m; ++i) {
+      const uint32_t f = f_nx;
+      const float* xf = v.x_fm + (size_t)f * v.n_rows;
+      const float xv = x_nx;
+      if (i + 1 < F) {
+        f_nx = feature_perm(i + 1, F, cur.key, v.feistel_h);
+        x_nx = in ? v.x_fm[(size_t)f_nx * v.n_rows + row] : 0.f;
+      }
+      const uint32_t ord = f32_order(xv);
+      if (__reduce_min_sync(FULL, in ? ord : 0xffffffffu) == __reduce_max_sync(FULL, in ? ord : 0u)) continue;
+      ++taken;
+      const uint64_t key = in ? ((uint64_t)ord << 32) | ((uint64_t)row << 5) | lane : ~0ull;
+      const uint64_t sk = warp_sort_u64(key, lane);  // lane p holds sorted position p
+      const bool valid = lane < n;
+      const uint32_t src = (uint32_t)sk & 31u;
+      const uint32_t srow = (uint32_t)sk >> 5;
+      const uint32_t cl = __shfl_sync(FULL, lab, src);
+      const uint32_t c = valid ? cl : NONE;
+      const float x = f32_unorder((uint32_t)(sk >> 32));
+      const float xn = __shfl_down_sync(FULL, x, 1);
+      const unsigned grp = __match_any_sync(FULL, c);
+      const int32_t k = (int32_t)__popc(grp & lt);
+      const int32_t tc = (int32_t)__popc(grp);
+      const int32_t il = warp_incl_scan_i32(valid ? 2 * k + 1 : 0);
+      const int32_t ir = warp_incl_scan_i32(valid ? 1 - 2 * (tc - k) : 0);
+      double sc = dinf();
+      float gil = 0.f, gir = 0.f;
+      if (valid && lane + 1 < n && is_candidate_sorted(x, xn)) {
+        const double nl = (double)(lane + 1);
+        const double nr = __dsub_rn(nn, nl);
+        const double gl = gini_part((int64_t)il, nl, nn);
+        const double gr = gini_part(sr0 + (int64_t)ir, nr, nn);
+        sc = __dadd_rn(gl, gr);
+        gil = __double2float_rn(gl);
+        gir = __double2float_rn(gr);
+      }
+      uint32_t pos = lane;
+      warp_argmin2(sc, pos, gil, gir);
+      if (sc < dinf() && (sc < best || (sc == best && f < bf))) {
+        best = sc;
+        bf = f;
+        bp = pos;
+        bil = gil;
+        bir = gir;
+        bmask = __reduce_or_sync(FULL, (valid && lane <= pos) ? (1u << src) : 0u);
+        const uint32_t r0 = __shfl_sync(FULL, srow, pos);
+        const uint32_t r1 = __shfl_sync(FULL, srow, (pos + 1) & 31u);
+        bthr = midpoint(xf[r0], xf[r1]);
+      }
+    }
+    bool split = bf != NONE;
+    uint32_t c0 = 0;
+    if (split && lane == 0) {
+      c0 = atomicAdd(&tv.n_nodes[nd.slot + tv.slot_base], 2u);
+      if (c0 + 2ull > tv.capacity) {
+        atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+        split = false;
+      }
+    }
+    split = __shfl_sync(FULL, split, 0);
+    c0 = __shfl_sync(FULL, c0, 0);
+    if (!split) {
+      subtree_leaf<IdxT, LabT>(v, tv, toff, cur.raw, mask, lab, lane);
+    } else {
+      if (lane == 0) {
+        tv.left[toff + cur.raw] = c0;
+        tv.right[toff + cur.raw] = c0 + 1;
+        tv.feature[toff + cur.raw] = bf;
+        tv.threshold[toff + cur.raw] = bthr;
+        tv.value[toff + cur.raw] = 0;
+      }
+      const uint32_t masks[2] = {bmask, mask & ~bmask};
+      const float imps[2] = {bil, bir};
+      for (int side = 0; side < 2; ++side) {
+        const uint32_t cm = masks[side];
+        if (imps[side] == 0.0f || __popc(cm) < v.mss) {
+          subtree_leaf<IdxT, LabT>(v, tv, toff, c0 + side, cm, lab, lane);
+        } else if (sp < 33) {
+          if (lane == 0) stack[sp] = SubEntry{cm, c0 + (uint32_t)side, child_key(cur.key, side)};
+          ++sp;
+        } else {
+          if (lane == 0) atomicOr(&s.ctr->error, DEV_ERR_INTERNAL);
+        }
+      }
+    }
+    __syncwarp();
+    if (sp == 0) break;
+    --sp;
+    cur = stack[sp];
+    __syncwarp();
+  }
+}
+
 __global__ void k_reset_step(Counters* c, uint32_t n_nodes) {
   c->n_nodes = n_nodes;
   c->n_scan_pieces = 0;
@@ -751,6 +924,20 @@ int launch_children(const View& v, uint32_t ib, uint32_t lb, const ct_node* node
   children_impl<I, L>(v, nodes, tot, s, caps, tv, next, next_tot, cap_next, small_cut, small, cap_small, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
+                    const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
+  if (cap_small == 0) return CT_OK;
+  Prof* pf = current_prof();
+  pf->begin(CT_K_SUBTREE);
+#define CALL(I, L) k_subtree<I, L><<<blocks_for_warps(cap_small), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, cap_small)
+  CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  pf->end();
+  pf->launched(CT_K_SUBTREE);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

@@ -268,6 +268,7 @@ class Server {
     p.min_samples_split = 1;
     ct_fit_options o{};
     o.mode = CT_FIT_BATCHED;
+    o.subtree_cutoff = 32;
     const size_t ib = p.index_bytes, nf = (size_t)n * f;
     size_t mb = 0;
     mb = (((size_t)t * n + 255) & ~size_t(255)) + (size_t)t * mark_bit_words(n) * 4 + 64;
@@ -724,6 +725,7 @@ class Server {
     p.seed = r->seed;
     ct_fit_options o{};
     o.mode = CT_FIT_BATCHED;
+    o.subtree_cutoff = 32;
     const size_t wsb = fit_workspace_bytes(&p, T, &o);
     char* ws = a.take<char>(wsb);
     if (!ws || !a.ok()) {

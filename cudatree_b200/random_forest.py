@@ -141,9 +141,14 @@ class RandomForestClassifier:
     """A random forest classifier (Gini, fully grown trees) on one B200."""
 
     def __init__(self, n_estimators=10, max_features=None, min_samples_split=1, bootstrap=True,
-                 verbose=False, debug=False, *, seed=None, fit_mode="batched"):
+                 verbose=False, debug=False, *, seed=None, fit_mode="batched", subtree_cutoff=32):
         if fit_mode not in ("batched", "plain"):
             raise ValueError("fit_mode must be 'batched' or 'plain'")
+        if not 0 <= int(subtree_cutoff) <= 32:
+            raise ValueError("subtree_cutoff must be in [0, 32]")
+        # nodes of at most subtree_cutoff rows are grown whole by one warp
+        # (same trees; 0 keeps every node in the level steps)
+        self.subtree_cutoff = int(subtree_cutoff)
         self.n_estimators = int(n_estimators)
         self.max_features = max_features
         self.min_samples_split = int(min_samples_split)
@@ -161,7 +166,8 @@ class RandomForestClassifier:
     # ------------------------------------------------------------ pickling
     def _params(self):
         return dict(max_features=self.max_features, min_samples_split=self.min_samples_split,
-                    bootstrap=self.bootstrap, seed=self.seed, fit_mode=self.fit_mode)
+                    bootstrap=self.bootstrap, seed=self.seed, fit_mode=self.fit_mode,
+                    subtree_cutoff=self.subtree_cutoff)
 
     def __reduce__(self):
         return restore_forest, (self._trees, getattr(self, "dtype_labels", np.dtype(np.uint8)).str,
@@ -238,7 +244,7 @@ class RandomForestClassifier:
         if mode == "plain":
             return 1
         prob = self._problem()
-        opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, 0, 0)
+        opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, self.subtree_cutoff, 0)
         free, _ = torch.cuda.mem_get_info()
         budget = int(free * 0.7)
         k = self.n_estimators
@@ -268,7 +274,7 @@ class RandomForestClassifier:
         n_nodes = torch.zeros(per_call, dtype=torch.int32, device=dev)
         tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
                               _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
-        opts = _lib.FitOptions(mode_id, int(bfs_threshold), 0, 0)
+        opts = _lib.FitOptions(mode_id, int(bfs_threshold), self.subtree_cutoff, 0)
         opts.reserved[0] = 1 if self.profile else 0
         ws = C.c_size_t()
         _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))

@@ -108,3 +108,25 @@ def test_compact_nodes_match_packed_and_oracle(cuda_device, n, f, c, seed):
                                  t.feature_threshold_array, t.values_array.astype(np.int64))
                           for t in forest._trees], classes=forest.compt_table, n_features=f)
     np.testing.assert_array_equal(compact, O.vote_counts(ref, xs))
+
+
+@pytest.mark.parametrize("mss", [1, 3])
+def test_warp_subtrees_grow_the_same_trees(cuda_device, mss):
+    """Nodes of at most subtree_cutoff rows are grown whole by one warp; the
+    trees must equal those of the level steps alone (cutoff 0) and the
+    oracle's, for deep trees (noise labels), ties and min_samples_split."""
+    rng = np.random.default_rng(1031)  # labels independent of x
+    x, _ = _synthetic(1500, 24, 5, 31)
+    y = rng.integers(0, 5, size=1500)
+    forests = {}
+    for cut in (0, 8, 32):
+        forests[cut] = RandomForestClassifier(n_estimators=4, min_samples_split=mss, seed=77,
+                                              subtree_cutoff=cut).fit(x, y)
+    for cut in (8, 32):
+        for a, b in zip(forests[cut]._trees, forests[0]._trees):
+            np.testing.assert_array_equal(a.left_children, b.left_children)
+            np.testing.assert_array_equal(a.feature_idx_array, b.feature_idx_array)
+            np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
+            np.testing.assert_array_equal(a.values_array, b.values_array)
+    ref = O.fit_forest(x, y, n_estimators=4, min_samples_split=mss, seed=77)
+    _assert_same_trees(forests[32]._trees, ref.trees)
