@@ -238,6 +238,11 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                                out_threshold, out_value);)
 }
 
+int ct_transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, uint32_t* nan_flag,
+                      void* stream) {
+  CT_GUARD(return transpose_rows(x_rm, n_rows, n_cols, x_cm, (cudaStream_t)stream, nan_flag);)
+}
+
 size_t ct_fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees) {
   return fetch_trees_scratch(total_nodes, n_trees);
 }

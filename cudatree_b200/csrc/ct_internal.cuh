@@ -338,7 +338,8 @@ bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes);
 void compact_host(const ct_packed_node* in, uint32_t n, uint32_t fbits, ct_compact_node* out);
 int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
                   size_t smem, bool any_grouped, cudaStream_t st);
-int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st);
+int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st,
+                   uint32_t* nan_flag = nullptr);
 int check_problem(const ct_problem* p);
 
 }  // namespace ct

@@ -148,19 +148,31 @@ __global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
 }  // namespace
 
 // Row-major [n_rows][n_cols] -> column-major [n_cols][n_rows] through a
-// 32x33 shared-memory tile (coalesced reads and writes).
-__global__ void k_transpose(const float* __restrict__ in, uint32_t n_rows, uint32_t n_cols, float* __restrict__ out) {
+// 32x33 shared-memory tile (coalesced reads and writes); row tiles are
+// strided over gridDim.y.  A NaN anywhere sets *nan_flag (when given), so
+// the input check needs no pass over x on the host.
+__global__ void k_transpose(const float* __restrict__ in, uint32_t n_rows, uint32_t n_cols, float* __restrict__ out,
+                            uint32_t* nan_flag) {
   __shared__ float tile[32][33];
-  const uint32_t c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
-    const uint32_t r = r0 + k, c = c0 + threadIdx.x;
-    if (r < n_rows && c < n_cols) tile[k][threadIdx.x] = in[(size_t)r * n_cols + c];
+  const uint32_t c0 = blockIdx.x * 32;
+  bool nan = false;
+  for (uint32_t r0 = blockIdx.y * 32; r0 < n_rows; r0 += gridDim.y * 32) {
+    for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+      const uint32_t r = r0 + k, c = c0 + threadIdx.x;
+      if (r < n_rows && c < n_cols) {
+        const float v = in[(size_t)r * n_cols + c];
+        nan |= v != v;
+        tile[k][threadIdx.x] = v;
+      }
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
+      const uint32_t c = c0 + k, r = r0 + threadIdx.x;
+      if (r < n_rows && c < n_cols) out[(size_t)c * n_rows + r] = tile[threadIdx.x][k];
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (uint32_t k = threadIdx.y; k < 32; k += blockDim.y) {
-    const uint32_t c = c0 + k, r = r0 + threadIdx.x;
-    if (r < n_rows && c < n_cols) out[(size_t)c * n_rows + r] = tile[threadIdx.x][k];
-  }
+  if (__syncthreads_or(nan) && threadIdx.x == 0 && threadIdx.y == 0 && nan_flag) atomicOr(nan_flag, 1u);
 }
 
 size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features) {
@@ -210,12 +222,13 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
   return CT_OK;
 }
 
-int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st) {
+int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st,
+                   uint32_t* nan_flag) {
   CT_ARG_CHECK(x_rm && x_cm, "transpose: NULL argument");
   if (n_rows == 0 || n_cols == 0) return CT_OK;
-  const dim3 grid(ceil_div(n_cols, 32), ceil_div(n_rows, 32));
-  CT_ARG_CHECK(grid.y <= 65535u, "transpose: too many rows for one launch");
-  k_transpose<<<grid, dim3(32, 8), 0, st>>>(x_rm, n_rows, n_cols, x_cm);
+  CT_ARG_CHECK(ceil_div(n_cols, 32) <= 0x7fffffffu, "transpose: too many columns");
+  const dim3 grid(ceil_div(n_cols, 32), std::min<uint32_t>(ceil_div(n_rows, 32), 65535u));
+  k_transpose<<<grid, dim3(32, 8), 0, st>>>(x_rm, n_rows, n_cols, x_cm, nan_flag);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

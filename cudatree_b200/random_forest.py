@@ -100,6 +100,23 @@ def pack_trees(trees):
     return packed, offsets
 
 
+def compact_labels(y):
+    """(table, ids): the sorted distinct labels and each label's index in the
+    table, as np.unique(y, return_inverse=True) gives them (the reference's
+    __compact_labels, random_forest.py:85-99).  Integer labels of modest
+    range take a counting path (linear, no sort)."""
+    y = np.asarray(y)
+    if y.dtype.kind in "iu" and y.size:
+        lo, hi = int(y.min()), int(y.max())
+        if hi - lo < (1 << 22) and -(1 << 62) < lo and hi < (1 << 62):
+            off = y.astype(np.int64) - lo
+            present = np.bincount(off, minlength=hi - lo + 1) > 0
+            table = (np.flatnonzero(present) + lo).astype(y.dtype)
+            lut = np.cumsum(present, dtype=np.int64) - 1
+            return table, lut[off]
+    return np.unique(y, return_inverse=True)
+
+
 def unpack_trees(packed, offsets, n_features, dtype_labels):
     """Inverse of pack_trees: RandomClassifierTree objects from packed nodes."""
     from .random_tree import restore_tree
@@ -187,9 +204,7 @@ class RandomForestClassifier:
         if x.shape[0] == 0:
             raise ValueError("cannot fit on zero samples")
         x32 = np.ascontiguousarray(x, dtype=np.float32)
-        if np.isnan(x32).any():
-            raise ValueError("samples contain NaN")
-        self.compt_table, y_c = np.unique(y, return_inverse=True)
+        self.compt_table, y_c = compact_labels(y)
         self.n_labels = int(self.compt_table.shape[0])
         if self.n_labels > _lib.MAX_CLASSES:
             raise ValueError(f"at most {_lib.MAX_CLASSES} classes are supported")
@@ -215,7 +230,10 @@ class RandomForestClassifier:
             xd = x_src.to(dev, non_blocking=True)  # pinned host tensors copy asynchronously
         else:
             xd = torch.from_numpy(x32).to(dev)
-        self._x_fm = xd.t().contiguous()
+        self._x_fm = torch.empty((self.n_features, self.n_samples), dtype=torch.float32, device=dev)
+        nan = torch.zeros(1, dtype=torch.int32, device=dev)
+        _lib.call("ct_transpose_rows", _ptr(xd), self.n_samples, self.n_features, _ptr(self._x_fm), _ptr(nan),
+                  _stream())
         self._labels = _to_dev(y_c.astype(self.dtype_labels), dev)
         self._presort = _dev_bytes(self.n_features * self.n_samples * self.index_bytes, dev)
         ws = C.c_size_t()
@@ -224,6 +242,9 @@ class RandomForestClassifier:
         _lib.call("ct_presort", _ptr(self._x_fm), self.n_samples, self.n_features, self.index_bytes,
                   _ptr(self._presort), _ptr(pws), ws.value, _stream())
         del pws
+        if int(nan.item()):
+            self.fit_release()
+            raise ValueError("samples contain NaN")
         self.last_fit_timing = {"upload_presort_s": time.perf_counter() - t0}
 
     def _problem(self) -> _lib.Problem:

@@ -215,6 +215,14 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                          uint32_t* out_left, uint32_t* out_right, uint16_t* out_feature,
                          float* out_threshold, uint32_t* out_value);
 
+/* Row-major samples [n_rows][n_cols] -> feature-major [n_cols][n_rows] on the
+ * device (the transpose of fit_init, random_forest.py:233).  When nan_flag
+ * (device, zeroed by the caller) is given, it becomes nonzero if any value is
+ * NaN: fits reject NaN, which has no place in the sorted order (the
+ * reference does not check, random_forest.py:214-217). */
+int ct_transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm,
+                      uint32_t* nan_flag, void* stream);
+
 /* Reads back the trees of one ct_fit call in canonical order.  counts[t]
  * (host) is trees->n_nodes[t]; tree t lands at [o_t, o_t + counts[t]) of the
  * host output arrays, o_t = counts[0] + ... + counts[t-1].  The used nodes

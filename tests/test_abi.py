@@ -139,3 +139,20 @@ def test_compact_fit_rule():
     assert lib.ct_compact_fits(1, 1 << 31) == 1       # b = 1
     assert lib.ct_compact_fits(3000, 1 << 20) == 1    # b = 12
     assert lib.ct_compact_fits(0, 10) == 0
+
+
+def test_compact_labels_matches_np_unique():
+    """Label compaction (the reference's __compact_labels) gives exactly the
+    table and ids of np.unique(return_inverse=True), on its counting path and
+    its sorting path."""
+    from cudatree_b200.random_forest import compact_labels
+    rng = np.random.default_rng(0)
+    cases = [rng.integers(-5, 40, 1000), rng.integers(0, 7, 5000).astype(np.uint8), np.array([3, 3, 3]),
+             rng.integers(0, 2**40, 100), rng.normal(size=50), np.array(["b", "a", "b"]),
+             rng.integers(0, 3, 10).astype(np.uint64), np.array([2**63 + 5, 2**63 + 1], dtype=np.uint64)]
+    for y in cases:
+        t, i = compact_labels(y)
+        t2, i2 = np.unique(y, return_inverse=True)
+        assert t.dtype == t2.dtype
+        np.testing.assert_array_equal(t, t2)
+        np.testing.assert_array_equal(i, i2)

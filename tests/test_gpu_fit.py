@@ -130,3 +130,15 @@ def test_warp_subtrees_grow_the_same_trees(cuda_device, mss):
             np.testing.assert_array_equal(a.values_array, b.values_array)
     ref = O.fit_forest(x, y, n_estimators=4, min_samples_split=mss, seed=77)
     _assert_same_trees(forests[32]._trees, ref.trees)
+
+
+def test_nan_samples_are_rejected(cuda_device):
+    """The device transpose flags NaN; the fit raises and a clean fit still works."""
+    x, y = _synthetic(500, 6, 3, 5)
+    bad = x.copy()
+    bad[123, 4] = np.nan
+    with pytest.raises(ValueError, match="NaN"):
+        RandomForestClassifier(n_estimators=2, seed=1).fit(bad, y)
+    ok = RandomForestClassifier(n_estimators=2, seed=1).fit(x, y)
+    ref = O.fit_forest(x, y, n_estimators=2, seed=1)
+    _assert_same_trees(ok._trees, ref.trees)
