@@ -121,6 +121,8 @@ PROTOTYPES = {
     "ct_fit_stats": (C.c_int, [C.c_void_p]),
     "ct_tree_canonicalize": (C.c_int, [P, P, P, P, P, C.c_uint32, P, P, P, P, P]),
     "ct_predict": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
+    "ct_autotune_workspace_size": (C.c_int, [P, C.c_uint32, C.c_uint32, P]),
+    "ct_autotune": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, P, C.c_size_t, P, P, P]),
     "ct_transpose_rows": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P]),
     "ct_fetch_trees_scratch": (C.c_size_t, [C.c_uint64, C.c_uint32]),
     "ct_fetch_trees": (C.c_int, [P, C.c_uint32, P, P, C.c_size_t, P, P, P, P, P, P]),

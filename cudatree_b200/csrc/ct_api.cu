@@ -22,6 +22,9 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
 int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
                  const uint32_t* value, uint32_t n, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot,
                  uint32_t* ov);
+size_t autotune_workspace_bytes(const ct_problem* p, uint32_t n_trees, uint32_t mode);
+int autotune(const ct_problem* p, const ct_lists* l, uint32_t n_trees, uint32_t mode, const ct_tree_buffers* trees,
+             void* ws, size_t wsb, ct_fit_options* best, float* best_ms, cudaStream_t st);
 size_t fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees);
 int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* counts, void* scratch,
                 size_t scratch_bytes, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot, uint32_t* ov,
@@ -236,6 +239,20 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                "NULL argument");
   CT_GUARD(return canonicalize(left, right, feature, threshold, value, n_nodes, out_left, out_right, out_feature,
                                out_threshold, out_value);)
+}
+
+
+int ct_autotune_workspace_size(const ct_problem* p, uint32_t n_trees, uint32_t mode, size_t* bytes) {
+  CT_ARG_CHECK(p && bytes && n_trees >= 1, "NULL argument");
+  CT_TRY(check_problem(p));
+  CT_GUARD(*bytes = autotune_workspace_bytes(p, n_trees, mode); return CT_OK;)
+}
+
+int ct_autotune(const ct_problem* p, const ct_lists* lists, uint32_t n_trees, uint32_t mode,
+                const ct_tree_buffers* trees, void* workspace, size_t workspace_bytes, ct_fit_options* best,
+                float* best_ms, void* stream) {
+  CT_GUARD(return autotune(p, lists, n_trees, mode, trees, workspace, workspace_bytes, best, best_ms,
+                           (cudaStream_t)stream);)
 }
 
 int ct_transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, uint32_t* nan_flag,

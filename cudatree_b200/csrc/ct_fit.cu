@@ -422,6 +422,85 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
 
 }  // namespace
 
+// Autotuner candidates.  Every option here grows the same trees, so they are
+// chosen by timing: the scan piece length and the warp-subtree cutoff for the
+// batched form, the depth-first/breadth-first switch for the plain form (the
+// quantity the reference fits offline, estimate_threshold.py, and predicts
+// with random_forest.py:278-289).
+std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode) {
+  std::vector<ct_fit_options> c;
+  if (mode == CT_FIT_BATCHED) {
+    for (uint32_t sp : {1024u, 2048u, 4096u, 8192u})
+      for (uint32_t cut : {0u, 16u, 32u}) {
+        ct_fit_options o{};
+        o.mode = CT_FIT_BATCHED;
+        o.subtree_cutoff = cut;
+        o.scan_piece = sp;
+        c.push_back(o);
+      }
+  } else {
+    std::vector<uint32_t> thr = {default_bfs_threshold(p), 2000u, 8000u, 32000u, std::max(2u, p->n_rows)};
+    std::sort(thr.begin(), thr.end());
+    thr.erase(std::unique(thr.begin(), thr.end()), thr.end());
+    for (uint32_t t : thr) {
+      ct_fit_options o{};
+      o.mode = CT_FIT_PLAIN;
+      o.bfs_threshold = t;
+      o.subtree_cutoff = 32;
+      c.push_back(o);
+    }
+  }
+  return c;
+}
+
+size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
+int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
+        const ct_fit_options* o, const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
+
+size_t autotune_workspace_bytes(const ct_problem* p, uint32_t n_trees, uint32_t mode) {
+  size_t most = 0;
+  for (const ct_fit_options& o : tune_candidates(p, mode)) most = std::max(most, fit_workspace_bytes(p, n_trees, &o));
+  return most;
+}
+
+int autotune(const ct_problem* p, const ct_lists* l, uint32_t n_trees, uint32_t mode, const ct_tree_buffers* trees,
+             void* ws, size_t wsb, ct_fit_options* best, float* best_ms, cudaStream_t st) {
+  CT_ARG_CHECK(best && (mode == CT_FIT_PLAIN || mode == CT_FIT_BATCHED), "autotune: bad arguments");
+  cudaEvent_t e0, e1;
+  CT_CUDA_TRY(cudaEventCreate(&e0));
+  CT_CUDA_TRY(cudaEventCreate(&e1));
+  float top = 3.0e38f;
+  int rc = CT_OK;
+  bool any = false;
+  for (const ct_fit_options& o : tune_candidates(p, mode)) {
+    if (fit_workspace_bytes(p, n_trees, &o) > wsb) continue;
+    float t = 3.0e38f;
+    for (int rep = 0; rep < 2 && rc == CT_OK; ++rep) {
+      cudaEventRecord(e0, st);
+      rc = fit(p, l, 0, n_trees, &o, trees, ws, wsb, st);
+      cudaEventRecord(e1, st);
+      if (cudaEventSynchronize(e1) != cudaSuccess) rc = CT_ERR_CUDA;
+      float ms = 0.f;
+      if (rc == CT_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) t = std::min(t, ms);
+    }
+    if (rc != CT_OK) break;
+    if (t < top) {
+      top = t;
+      *best = o;
+      any = true;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != CT_OK) return rc;
+  if (!any) {
+    set_last_error("autotune: workspace too small for every candidate");
+    return CT_ERR_OOM;
+  }
+  if (best_ms) *best_ms = top;
+  return CT_OK;
+}
+
 size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o) {
   FitLayout L;
   layout(p, n_trees, o, nullptr, 0, &L);

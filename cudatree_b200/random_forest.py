@@ -100,6 +100,9 @@ def pack_trees(trees):
     return packed, offsets
 
 
+_TUNED = {}  # tuned fit options per (mode, rows, features, classes, max_features, ...)
+
+
 def compact_labels(y):
     """(table, ids): the sorted distinct labels and each label's index in the
     table, as np.unique(y, return_inverse=True) gives them (the reference's
@@ -158,7 +161,8 @@ class RandomForestClassifier:
     """A random forest classifier (Gini, fully grown trees) on one B200."""
 
     def __init__(self, n_estimators=10, max_features=None, min_samples_split=1, bootstrap=True,
-                 verbose=False, debug=False, *, seed=None, fit_mode="batched", subtree_cutoff=32):
+                 verbose=False, debug=False, *, seed=None, fit_mode="batched", subtree_cutoff=32,
+                 autotune=False):
         if fit_mode not in ("batched", "plain"):
             raise ValueError("fit_mode must be 'batched' or 'plain'")
         if not 0 <= int(subtree_cutoff) <= 32:
@@ -166,6 +170,10 @@ class RandomForestClassifier:
         # nodes of at most subtree_cutoff rows are grown whole by one warp
         # (same trees; 0 keeps every node in the level steps)
         self.subtree_cutoff = int(subtree_cutoff)
+        # time candidate fit options on a few trees before the first fit of a
+        # data shape (options never change the trees, only the speed)
+        self.autotune_fit = bool(autotune)
+        self._tuned = None
         self.n_estimators = int(n_estimators)
         self.max_features = max_features
         self.min_samples_split = int(min_samples_split)
@@ -265,7 +273,7 @@ class RandomForestClassifier:
         if mode == "plain":
             return 1
         prob = self._problem()
-        opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, self.subtree_cutoff, 0)
+        opts = self._fit_options(_lib.CT_FIT_BATCHED, 0)
         free, _ = torch.cuda.mem_get_info()
         budget = int(free * 0.7)
         k = self.n_estimators
@@ -295,7 +303,7 @@ class RandomForestClassifier:
         n_nodes = torch.zeros(per_call, dtype=torch.int32, device=dev)
         tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
                               _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
-        opts = _lib.FitOptions(mode_id, int(bfs_threshold), self.subtree_cutoff, 0)
+        opts = self._fit_options(mode_id, bfs_threshold)
         opts.reserved[0] = 1 if self.profile else 0
         ws = C.c_size_t()
         _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))
@@ -351,6 +359,12 @@ class RandomForestClassifier:
         self.fit_init(samples, target)
         if bfs_threshold is not None:
             self.bfs_threshold = int(bfs_threshold)
+        if self.autotune_fit and self._tuned is None:
+            self._tuned = _TUNED.get(self._shape_key(self.fit_mode))
+            if self._tuned is None:
+                self._run_autotune(self.fit_mode, min(8, self.n_estimators))
+            if bfs_threshold is None and self.fit_mode == "plain":
+                self.bfs_threshold = self._tuned["bfs_threshold"]
         if self.verbose:
             print(f"bfs_threshold : {self.bfs_threshold}; bootstrap : {self.bootstrap}; "
                   f"min_samples_split : {self.min_samples_split}; fit_mode : {self.fit_mode}")
@@ -362,6 +376,54 @@ class RandomForestClassifier:
         torch.cuda.synchronize()
         self.last_fit_timing["fit_s"] = time.perf_counter() - t0
         return self
+
+    # ---------------------------------------------------------- autotune
+    def _fit_options(self, mode_id, bfs_threshold):
+        t = self._tuned or {}
+        return _lib.FitOptions(mode_id, int(bfs_threshold), int(t.get("subtree_cutoff", self.subtree_cutoff)),
+                               int(t.get("scan_piece", 0)))
+
+    def _shape_key(self, mode):
+        return (mode, self.n_samples, self.n_features, self.n_labels, self._m, self.index_bytes,
+                bool(self.bootstrap), self.min_samples_split)
+
+    def _run_autotune(self, mode, sample_trees):
+        dev = _device()
+        prob = self._problem()
+        n, f = self.n_samples, self.n_features
+        mode_id = _lib.CT_FIT_PLAIN if mode == "plain" else _lib.CT_FIT_BATCHED
+        slots = 1 if mode == "plain" else sample_trees
+        si0 = _dev_bytes(slots * f * n * self.index_bytes, dev)
+        si1 = _dev_bytes(slots * f * n * self.index_bytes, dev)
+        mark = _dev_bytes(_lib.mark_bytes(n, slots), dev)
+        lists = _lib.Lists(_ptr(si0), _ptr(si1), _ptr(mark), n, slots)
+        cap = 2 * n
+        raw = [torch.empty(sample_trees * cap, dtype=torch.int32, device=dev) for _ in range(5)]
+        n_nodes = torch.zeros(sample_trees, dtype=torch.int32, device=dev)
+        tb = _lib.TreeBuffers(*[_ptr(r) for r in raw], _ptr(n_nodes), cap)
+        wsb = C.c_size_t()
+        _lib.call("ct_autotune_workspace_size", C.byref(prob), sample_trees, mode_id, C.byref(wsb))
+        work = _dev_bytes(wsb.value, dev)
+        best = _lib.FitOptions()
+        ms = C.c_float()
+        _lib.call("ct_autotune", C.byref(prob), C.byref(lists), sample_trees, mode_id, C.byref(tb), _ptr(work),
+                  wsb.value, C.byref(best), C.byref(ms), _stream())
+        self._tuned = {"scan_piece": int(best.scan_piece), "subtree_cutoff": int(best.subtree_cutoff),
+                       "bfs_threshold": int(best.bfs_threshold) or self.bfs_threshold,
+                       "sample_trees": sample_trees, "sample_ms": float(ms.value)}
+        _TUNED[self._shape_key(mode)] = self._tuned
+        return self._tuned
+
+    def autotune(self, samples, target, sample_trees=8):
+        """Choose fit options for this data shape by timing candidate fits of
+        sample_trees trees (the reference's offline threshold estimate,
+        estimate_threshold.py, done on the device at hand); later fits of the
+        same shape with autotune=True reuse the choice.  Returns it."""
+        self.fit_init(samples, target)
+        try:
+            return dict(self._run_autotune(self.fit_mode, max(1, min(int(sample_trees), self.n_estimators))))
+        finally:
+            self.fit_release()
 
     # ----------------------------------------------------------- predict
     def _device_forest(self, compact=None):

@@ -215,6 +215,19 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
                          uint32_t* out_left, uint32_t* out_right, uint16_t* out_feature,
                          float* out_threshold, uint32_t* out_value);
 
+/* Autotuner: fits n_trees sample trees (first tree 0) with each candidate
+ * option set of the given mode and returns the fastest in *best (its time in
+ * *best_ms).  Every candidate grows the same trees, so the choice changes
+ * speed only.  Batched: scan piece length x warp-subtree cutoff; plain: the
+ * depth-first/breadth-first switch, which the reference sets with an offline
+ * regression (estimate_threshold.py, random_forest.py:278-289).  The
+ * workspace must hold ct_autotune_workspace_size bytes; lists and trees as
+ * for ct_fit with n_trees. */
+int ct_autotune_workspace_size(const ct_problem* p, uint32_t n_trees, uint32_t mode, size_t* bytes);
+int ct_autotune(const ct_problem* p, const ct_lists* lists, uint32_t n_trees, uint32_t mode,
+                const ct_tree_buffers* trees, void* workspace, size_t workspace_bytes,
+                ct_fit_options* best, float* best_ms, void* stream);
+
 /* Row-major samples [n_rows][n_cols] -> feature-major [n_cols][n_rows] on the
  * device (the transpose of fit_init, random_forest.py:233).  When nan_flag
  * (device, zeroed by the caller) is given, it becomes nonzero if any value is

@@ -142,3 +142,18 @@ def test_nan_samples_are_rejected(cuda_device):
     ok = RandomForestClassifier(n_estimators=2, seed=1).fit(x, y)
     ref = O.fit_forest(x, y, n_estimators=2, seed=1)
     _assert_same_trees(ok._trees, ref.trees)
+
+
+def test_autotune_keeps_the_trees(cuda_device):
+    """The autotuner only picks among options that grow the same trees."""
+    x, y = _synthetic(4000, 12, 4, 9)
+    tuned = RandomForestClassifier(n_estimators=6, seed=5, autotune=True).fit(x, y)
+    assert tuned._tuned is not None and tuned._tuned["scan_piece"] in (1024, 2048, 4096, 8192)
+    assert tuned._tuned["subtree_cutoff"] in (0, 16, 32)
+    ref = RandomForestClassifier(n_estimators=6, seed=5).fit(x, y)
+    for a, b in zip(tuned._trees, ref._trees):
+        np.testing.assert_array_equal(a.left_children, b.left_children)
+        np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
+        np.testing.assert_array_equal(a.values_array, b.values_array)
+    plain = RandomForestClassifier(n_estimators=3, seed=5, fit_mode="plain").autotune(x, y, sample_trees=2)
+    assert plain["bfs_threshold"] >= 2
