@@ -34,7 +34,7 @@ WORKLOAD = ("covtype-shaped synthetic 581012x54 f32 (10 Gaussian + 44 one-hot), 
             "100 trees, bootstrap, max_features=7, uint32 indices, fully grown")
 N_TREES = 100
 MAX_FEATURES = 7
-PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.84
+PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.86
 
 
 def peaks():
@@ -489,9 +489,9 @@ def run_ours(args, world, rank, local):
     p_ms = stats["ms"][pi]
     p_gbs = stats["bytes"][pi] / (p_ms * 1e6) if p_ms > 0 else None
     # DRAM bytes per partition launch: the algorithmic bytes per launch times
-    # the DRAM/algorithmic ratio ncu measured on the 10-tree case of this
+    # the DRAM/algorithmic ratio ncu measured on the 16-tree case of this
     # workload (dram__bytes_read.sum + dram__bytes_write.sum over every level
-    # launch; profiles/k_part_big_covtype_10trees.md)
+    # launch; profiles/k_part_big_covtype_16trees.md)
     p_launches = stats["launches"][pi]
     traffic = (PARTITION_DRAM_PER_ALGORITHMIC_BYTE * stats["bytes"][pi] / p_launches) if p_launches else None
     si = groups.index("scan")
@@ -518,7 +518,7 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "kernel": "k_partition", "achieved": round(p_gbs, 1) if p_gbs else None,
                      "peak": peak, "unit": "GB/s", "frac": round(p_gbs / peak, 4) if p_gbs else None,
                      "peak_kind": peak_kind, "traffic": round(traffic) if traffic else None,
-                     "traffic_unit": "DRAM bytes per launch (ncu ratio 0.84 x algorithmic, 10-tree capture)",
+                     "traffic_unit": "DRAM bytes per launch (ncu ratio 0.86 x algorithmic, 16-tree capture)",
                      "algorithmic_bytes_per_launch": round(stats["bytes"][pi] / p_launches) if p_launches else None,
                      "algorithmic_bytes_per_element": "n_features x (2 x index_bytes + 1)"},
         "scan_roofline": {"kernel": "k_split_scan (+hist/carry)",
