@@ -112,13 +112,20 @@ def dist_setup(n_gpus):
 
 
 def max_over_ranks(value: float, world: int) -> float:
+    """The slowest rank's time (replicas: every rank fits its own forest)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_seed(rank: int) -> int:
+    """Each replica grows its own forest (different trees per rank)."""
+    return 1000 + rank
 
 
 def barrier(world):
@@ -405,7 +412,7 @@ def run_ours(args, world, rank, local):
     from cudatree_b200 import RandomForestClassifier, _lib, synthetic
 
     x, y = synthetic.covtype_like()
-    seed = 1000 + rank
+    seed = replica_seed(rank)
     n_trees = args.trees
     forest = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
     forest.fit_init(x, y)
