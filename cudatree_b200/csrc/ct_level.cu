@@ -495,15 +495,27 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
   __syncwarp();
   const uint32_t lo = pp.j * PART_PIECE;
   const uint32_t hi = min(lo + PART_PIECE, nd.n);
-  for (uint32_t base = lo; base < hi; base += 32) {
-    const uint32_t p = base + lane;
-    uint32_t c = NONE;
+  // all the piece's index loads first, then the mark writes and label gathers
+  uint32_t rows[PART_ROUNDS], cls[PART_ROUNDS];
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    const uint32_t p = lo + r * 32 + lane;
+    rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    const uint32_t p = lo + r * 32 + lane;
+    cls[r] = NONE;
     if (p < hi) {
-      const uint32_t row = lst[p];
       const bool left = p <= sr.pos;
-      mk[row] = left ? 1 : 0;
-      if (left) c = label_of<LabT>(v, row);
+      mk[rows[r]] = left ? 1 : 0;
+      if (left) cls[r] = label_of<LabT>(v, rows[r]);
     }
+  }
+#pragma unroll
+  for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+    if (lo + r * 32 >= hi) break;
+    const uint32_t c = cls[r];
     const unsigned grp = __match_any_sync(FULL, c);
     if (c != NONE && (grp >> lane) == 1u) cnt[c] += __popc(grp);
     __syncwarp();

@@ -308,7 +308,17 @@ __global__ void k_pack_marks(const uint8_t* __restrict__ mark, uint32_t* __restr
     const uint8_t* m = mark + (size_t)slot * n_rows + (size_t)wd * 32;
     const uint32_t lim = wd * 32 < n_rows ? min(32u, n_rows - wd * 32) : 0u;
     uint32_t v = 0;
-    for (uint32_t k = 0; k < lim; ++k) v |= (m[k] ? 1u : 0u) << k;
+    if (lim == 32 && (reinterpret_cast<uintptr_t>(m) & 3u) == 0) {
+      // eight aligned words, four mark bytes (each 0 or 1) per word
+#pragma unroll
+      for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t q = __ldg(reinterpret_cast<const uint32_t*>(m) + k);
+        const uint32_t b4 = (q & 1u) | ((q >> 7) & 2u) | ((q >> 14) & 4u) | ((q >> 21) & 8u);
+        v |= b4 << (4 * k);
+      }
+    } else {
+      for (uint32_t k = 0; k < lim; ++k) v |= (m[k] ? 1u : 0u) << k;
+    }
     bits[i] = v;
   }
 }
