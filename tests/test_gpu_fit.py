@@ -157,3 +157,45 @@ def test_autotune_keeps_the_trees(cuda_device):
         np.testing.assert_array_equal(a.values_array, b.values_array)
     plain = RandomForestClassifier(n_estimators=3, seed=5, fit_mode="plain").autotune(x, y, sample_trees=2)
     assert plain["bfs_threshold"] >= 2
+
+
+def test_many_classes_use_16_bit_labels(cuda_device):
+    """More than 255 classes: 2-byte labels through every kernel (level
+    steps and warp subtrees), against the oracle."""
+    rng = np.random.default_rng(40)
+    n = 3000
+    y = rng.integers(0, 300, size=n) * 7  # 300 distinct, non-contiguous labels
+    x = (rng.normal(size=(n, 10)) + (y[:, None] % 13) * 0.3).astype(np.float32)
+    forest = RandomForestClassifier(n_estimators=3, seed=41).fit(x, y)
+    assert forest.dtype_labels == np.uint16
+    ref = O.fit_forest(x, y, n_estimators=3, seed=41)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x[:500]), O.predict(ref, x[:500]))
+
+
+@pytest.mark.parametrize("case", ["one_row", "two_rows_same", "one_feature", "constant_features",
+                                  "large_mss", "all_features"])
+def test_edge_shapes_match_oracle(cuda_device, case):
+    rng = np.random.default_rng(50)
+    kw = {}
+    if case == "one_row":
+        x, y = np.array([[1.0, 2.0]], np.float32), np.array([3])
+    elif case == "two_rows_same":
+        x, y = np.array([[1.0], [2.0]], np.float32), np.array([5, 5])
+    elif case == "one_feature":
+        x = rng.normal(size=(700, 1)).astype(np.float32)
+        y = (x[:, 0] > 0.2).astype(np.int64) + rng.integers(0, 2, 700)
+    elif case == "constant_features":
+        x = rng.normal(size=(600, 6)).astype(np.float32)
+        x[:, [0, 2, 5]] = 4.0
+        y = rng.integers(0, 3, 600)
+    elif case == "large_mss":
+        x, y = _synthetic(900, 8, 4, 51)
+        kw = {"min_samples_split": 60}
+    else:
+        x, y = _synthetic(900, 8, 4, 52)
+        kw = {"max_features": 8}
+    forest = RandomForestClassifier(n_estimators=3, seed=53, **kw).fit(x, y)
+    ref = O.fit_forest(x, y, n_estimators=3, seed=53, **kw)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
