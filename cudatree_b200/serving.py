@@ -72,7 +72,7 @@ def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, workers=8)
     try:
         reqs, keep = [], []
         for (x, table, ids), seed in zip(prepared, seeds):
-            xp, yp = pinned(x), pinned(ids)
+            xp, yp = x, np.ascontiguousarray(ids, dtype=np.uint32)  # pageable: no page-locking per job
             m = 0 if max_features is None else int(max_features)
             r = srv.fit_request(xp, yp, n_classes=int(table.shape[0]), n_trees=n_estimators, seed=int(seed),
                                 max_features=m)
@@ -87,6 +87,14 @@ def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, workers=8)
         return out
     finally:
         srv.close()
+
+
+def _host_ptr(a) -> int:
+    if isinstance(a, torch.Tensor):
+        return a.data_ptr()
+    if not (isinstance(a, np.ndarray) and a.flags["C_CONTIGUOUS"]):
+        raise ValueError("host arrays must be C-contiguous numpy arrays or torch tensors")
+    return a.ctypes.data
 
 
 def pinned(a: np.ndarray) -> torch.Tensor:
@@ -167,10 +175,12 @@ class ForestServer:
         return Request(0.0, CT_REQ_PREDICT, forest_id, x_pinned.data_ptr(), None, out_pinned.data_ptr(), n,
                        x_pinned.shape[1], 0, 0, 0, 0, 0, 0.0, 0, 0, None)
 
-    def fit_request(self, x_pinned: torch.Tensor, y_pinned: torch.Tensor, n_classes: int, n_trees: int,
-                    seed: int, max_features: int = 0) -> Request:
-        n, f = x_pinned.shape
-        return Request(0.0, CT_REQ_FIT, 0, x_pinned.data_ptr(), y_pinned.data_ptr(), None, n, f, n_classes,
+    def fit_request(self, x, y, n_classes: int, n_trees: int, seed: int, max_features: int = 0) -> Request:
+        """A fit job over host arrays x [n, f] float32 and y [n] uint32 class ids
+        (torch tensors or numpy arrays; pageable memory is fine for fit jobs,
+        whose copies are staged by the fit worker's own thread)."""
+        n, f = x.shape
+        return Request(0.0, CT_REQ_FIT, 0, _host_ptr(x), _host_ptr(y), None, n, f, n_classes,
                        n_trees, max_features, 0, seed, 0.0, 0, 0, None)
 
     def submit(self, req: Request) -> None:
