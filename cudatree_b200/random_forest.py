@@ -212,6 +212,8 @@ class RandomForestClassifier:
         if x.shape[0] == 0:
             raise ValueError("cannot fit on zero samples")
         x32 = np.ascontiguousarray(x, dtype=np.float32)
+        self.samples, self.target = samples, target  # as the reference keeps them (random_forest.py:215-266)
+        self._next_tree = 0
         self.compt_table, y_c = compact_labels(y)
         self.n_labels = int(self.compt_table.shape[0])
         if self.n_labels > _lib.MAX_CLASSES:
@@ -259,6 +261,20 @@ class RandomForestClassifier:
         return _lib.Problem(_ptr(self._x_fm), _ptr(self._labels), _ptr(self._presort), self.n_samples,
                             self.n_features, self.n_labels, self.index_bytes, self.dtype_labels.itemsize,
                             self._m, self.min_samples_split, int(self.bootstrap), self._seed)
+
+    @property
+    def sorted_indices(self):
+        """The device presort [F][N] (row ids in each feature's value order)."""
+        return getattr(self, "_presort", None)
+
+    def _get_sorted_indices(self, sorted_indices):
+        """(tree index, rows) for the next tree of a per-tree loop
+        (random_forest.py:113-144, called by hybridforest/builder.py:131).
+        The bootstrap sample is drawn inside the tree's fit from the forest's
+        seed and this index, so a per-tree loop grows the same trees as fit()."""
+        t = self._next_tree
+        self._next_tree += 1
+        return t, self.n_samples
 
     def fit_release(self):
         self._x_fm = None

@@ -36,7 +36,24 @@ class RandomClassifierTree:
         self.feature_threshold_array = None
         self.values_array = None
         self.dtype_labels = np.dtype(np.uint8)
-        self.n_features = forest.n_features if forest is not None else None
+        self.forest = forest
+        self.n_features = getattr(forest, "n_features", None) if forest is not None else None
+
+    def fit(self, samples, target, sorted_indices, n_samples):
+        """Grow one tree of a forest prepared by fit_init, the per-tree call
+        hybridforest's GPU worker makes (hybridforest/builder.py:129-132,
+        random_tree.py:461-491).  sorted_indices is what the forest's
+        _get_sorted_indices returned (the tree's index: its bootstrap sample is
+        drawn inside the fit from the forest's seed); samples, target and
+        n_samples are accepted for the reference's signature."""
+        f = self.forest
+        if f is None or getattr(f, "_x_fm", None) is None:
+            raise ValueError("the forest has no data: call forest.fit_init(samples, target) first")
+        grown = f._fit_trees(int(sorted_indices), 1, f.fit_mode, f.bfs_threshold)[0]
+        for name in ("left_children", "right_children", "feature_idx_array", "feature_threshold_array",
+                     "values_array", "dtype_labels", "n_features"):
+            setattr(self, name, getattr(grown, name))
+        return self
 
     @property
     def n_nodes(self) -> int:

@@ -199,3 +199,25 @@ def test_edge_shapes_match_oracle(cuda_device, case):
     ref = O.fit_forest(x, y, n_estimators=3, seed=53, **kw)
     _assert_same_trees(forest._trees, ref.trees)
     np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
+
+
+def test_per_tree_loop_of_hybridforest(cuda_device):
+    """The per-tree calls hybridforest's GPU worker makes (fit_init,
+    _get_sorted_indices, RandomClassifierTree(forest).fit, fit_release) grow
+    the trees a whole-forest fit with the same seed grows."""
+    from cudatree_b200 import RandomClassifierTree
+    x, y = _synthetic(2500, 9, 4, 61)
+    forest = RandomForestClassifier(n_estimators=1, seed=62)
+    forest.fit_init(x, y)
+    trees = []
+    for _ in range(3):
+        tree = RandomClassifierTree(forest)
+        si, n_samples = forest._get_sorted_indices(forest.sorted_indices)
+        tree.fit(forest.samples, forest.target, si, n_samples)
+        trees.append(tree)
+    forest.fit_release()
+    whole = RandomForestClassifier(n_estimators=3, seed=62).fit(x, y)
+    for a, b in zip(trees, whole._trees):
+        np.testing.assert_array_equal(a.left_children, b.left_children)
+        np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
+        np.testing.assert_array_equal(a.values_array, b.values_array)
