@@ -179,7 +179,7 @@ def _sk_fit_s(x, y, trees, max_features, bootstrap, cores):
     return time.perf_counter() - t0, rf
 
 
-def _fit_pair(x, y, n_trees, m, bootstrap, bfs_threshold, seed, plain_trees):
+def _fit_pair(x, y, n_trees, m, bootstrap, bfs_threshold, seed, plain_trees, tuned=None):
     """Batched fit seconds (warm, CUDA events), plain fit seconds on plain_trees
     trees scaled to n_trees, and whether plain grew the same trees."""
     import torch
@@ -187,6 +187,7 @@ def _fit_pair(x, y, n_trees, m, bootstrap, bfs_threshold, seed, plain_trees):
     from cudatree_b200 import RandomForestClassifier, _lib
     f = RandomForestClassifier(n_trees, max_features=m, bootstrap=bootstrap, seed=seed)
     f.fit_init(x, y)
+    f._tuned = tuned
     thr = f.bfs_threshold if bfs_threshold is None else bfs_threshold
     f._fit_trees(0, n_trees, "batched", thr)  # warm-up
     st = torch.cuda.current_stream()
@@ -229,11 +230,16 @@ def run_configs(args):
     out["digits_1797x64_50trees"] = {"batched_fit_s": b, "plain_fit_s": p, "plain_trees_identical": same,
                                      "nodes": nodes, "sklearn_fit_s": sk, "sklearn_cores": cores}
     x, y = synthetic.wide()
-    b, p, same, gbs, nodes = _fit_pair(x, y, 200, 55, True, None, 12, 10)
+    tuner = RandomForestClassifier(200, max_features=55, seed=12)
+    t0 = time.perf_counter()
+    tuned = tuner.autotune(x, y, sample_trees=32)
+    tune_s = time.perf_counter() - t0
+    b, p, same, gbs, nodes = _fit_pair(x, y, 200, 55, True, None, 12, 10, tuned)
     sk, _ = _sk_fit_s(x, y, 32, 55, True, cores)
     out["wide_10000x3000_c100_200trees"] = {
         "batched_fit_s": b, "plain_fit_s": p, "plain_sample": "10 trees scaled to 200",
         "plain_trees_identical": same, "nodes": nodes, "kernel_GB_per_s": gbs,
+        "autotuned": {k: tuned[k] for k in ("scan_piece", "subtree_cutoff")}, "autotune_s": tune_s,
         "sklearn_fit_s": sk * 200 / 32, "sklearn_sample": "32 trees scaled to 200", "sklearn_cores": cores}
     n_jobs = args.queue_jobs
     jobs = [synthetic.blob_job(j) for j in range(n_jobs)]

@@ -146,7 +146,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->chunk = std::min<uint32_t>(L->cap_list, CHUNK_NODES_MAX);
   L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
   // the warp subtree packs a row id into 27 bits of its sort key
-  L->subtree_cut = p->n_rows < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 32u) : 0u;
+  L->subtree_cut = p->n_rows < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 128u) : 0u;
   L->cap_small = L->subtree_cut ? 2 * L->chunk : 0u;
   Arena a{base, size, 0};
   L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
@@ -239,7 +239,7 @@ int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot_l
 int flush_subtrees(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, cudaStream_t st) {
   if (!L.subtree_cut || L.small_bound == 0) return CT_OK;
   CT_TRY(launch_subtrees(v, p->index_bytes, p->label_bytes, L.small,
-                         (uint32_t)std::min<uint64_t>(L.small_bound, L.cap_small), L.s, tv, st));
+                         (uint32_t)std::min<uint64_t>(L.small_bound, L.cap_small), L.subtree_cut > 32, L.s, tv, st));
   CT_CUDA_TRY(cudaMemsetAsync(&L.s.ctr->n_small, 0, sizeof(uint32_t), st));
   L.small_bound = 0;
   return CT_OK;
@@ -430,8 +430,8 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
 std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode) {
   std::vector<ct_fit_options> c;
   if (mode == CT_FIT_BATCHED) {
-    for (uint32_t sp : {1024u, 2048u, 4096u, 8192u})
-      for (uint32_t cut : {0u, 16u, 32u}) {
+    for (uint32_t sp : {1024u, 2048u, 4096u})
+      for (uint32_t cut : {0u, 32u, 128u}) {
         ct_fit_options o{};
         o.mode = CT_FIT_BATCHED;
         o.subtree_cutoff = cut;

@@ -297,9 +297,9 @@ int launch_children(const View& v, uint32_t index_bytes, uint32_t label_bytes, c
                     ct_node* next, uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut,
                     ct_node* small, uint32_t cap_small, cudaStream_t st);
 // Warp subtrees of the small nodes the children step set aside (at most
-// cap_small of them this step).
+// cap_small of them); wide: some may have 33..128 rows.
 int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
-                    const LevelScratch& s, const TreeView& tv, cudaStream_t st);
+                    bool wide, const LevelScratch& s, const TreeView& tv, cudaStream_t st);
 // Stable partition of segments (ct_partition.cu).
 int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
                          cudaStream_t st);

@@ -639,24 +639,14 @@ __device__ __forceinline__ void subtree_leaf(const View& v, const TreeView& tv, 
   }
 }
 
+// One row per lane: grows the subtree of `cur` (lanes in feature-0 order,
+// row ids and labels in registers; lanes outside the node carry NONE).
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
-  __shared__ SubEntry stack_all[WARPS_PER_BLOCK][33];
-  const uint32_t w = global_warp();
-  const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
-  SubEntry* stack = stack_all[threadIdx.x >> 5];
-  const ct_node nd = small[w];
-  const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
-  const bool have = lane < nd.n;
-  const uint32_t row = have ? (uint32_t)l0[lane] : 0u;
-  const uint32_t lab = have ? label_of<LabT>(v, row) : NONE;
+__device__ void grow_small(const View& v, const LevelScratch& s, const TreeView& tv, uint32_t tslot, size_t toff,
+                           uint32_t row, uint32_t lab, SubEntry cur, SubEntry* stack, uint32_t lane) {
   const uint32_t F = v.n_features, m = v.max_features;
-  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
   const unsigned lt = lanemask_lt();
   int sp = 0;
-  SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
   while (true) {
     const uint32_t mask = cur.mask;
     const uint32_t n = __popc(mask);
@@ -725,7 +715,7 @@ k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv
     bool split = bf != NONE;
     uint32_t c0 = 0;
     if (split && lane == 0) {
-      c0 = atomicAdd(&tv.n_nodes[nd.slot + tv.slot_base], 2u);
+      c0 = atomicAdd(&tv.n_nodes[tslot], 2u);
       if (c0 + 2ull > tv.capacity) {
         atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
         split = false;
@@ -763,6 +753,350 @@ k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv
     cur = stack[sp];
     __syncwarp();
   }
+}
+
+// Four rows per lane, for subtree roots of 33..128 rows.  Slot s (lane
+// s % 32, register s / 32) holds the root's s-th row in feature-0 order, so
+// a node's leaf label is its lowest slot's; the sort key carries each slot's
+// rank by row id, so equal values still order by row id.  A node is a
+// 128-bit mask of slots; a child of at most 32 rows is compacted onto the
+// lanes (slot order) and handed to grow_small.
+constexpr uint32_t WIDE_ROWS = 128;
+constexpr uint32_t WIDE_STACK = 4;  // pending nodes of > 32 rows are disjoint: at most 3
+struct WideEntry {
+  uint32_t m[4];
+  uint32_t raw;
+  uint32_t pad;
+  uint64_t key;
+};
+
+// Shared memory of one warp of k_subtree, in words: rows, labels and row
+// ranks of 128 slots, two class arrays, then the two stacks (8-byte fields)
+// at a 16-byte boundary; the whole region is a multiple of 16 bytes, so every
+// warp's stacks stay aligned.
+__host__ __device__ __forceinline__ uint32_t subtree_stacks_word(uint32_t n_classes) {
+  return (3 * WIDE_ROWS + 2 * n_classes + 3u) & ~3u;
+}
+__host__ __device__ __forceinline__ uint32_t subtree_warp_words(uint32_t n_classes) {
+  return subtree_stacks_word(n_classes) + WIDE_STACK * (uint32_t)(sizeof(WideEntry) / 4) +
+         33u * (uint32_t)(sizeof(SubEntry) / 4);
+}
+
+// Bitonic network over 128 keys, element lane + 32 k in register k.
+__device__ __forceinline__ void warp_sort128(uint64_t (&v)[4], uint32_t lane) {
+#pragma unroll
+  for (uint32_t size = 2; size <= WIDE_ROWS; size <<= 1) {
+#pragma unroll
+    for (uint32_t j = size >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const uint32_t kj = j >> 5;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+          if (k & kj) continue;
+          const uint32_t k2 = k | kj;
+          const bool up = ((lane + 32 * k) & size) == 0u;
+          const uint64_t a = v[k], b = v[k2];
+          const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+          v[k] = up ? lo : hi;
+          v[k2] = up ? hi : lo;
+        }
+      } else {
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+          const uint64_t o = __shfl_xor_sync(FULL, v[k], j);
+          const bool up = ((lane + 32 * k) & size) == 0u;
+          const bool lower = (lane & j) == 0u;
+          v[k] = (lower == up) ? (o < v[k] ? o : v[k]) : (o > v[k] ? o : v[k]);
+        }
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t pick4(const uint64_t (&v)[4], uint32_t k) {
+  return k == 0 ? v[0] : k == 1 ? v[1] : k == 2 ? v[2] : v[3];
+}
+
+__device__ __forceinline__ uint32_t lowest_slot(const uint32_t (&m)[4]) {
+  return m[0] ? __ffs(m[0]) - 1 : m[1] ? 31 + __ffs(m[1]) : m[2] ? 63 + __ffs(m[2]) : 95 + __ffs(m[3]);
+}
+
+template <typename IdxT, typename LabT>
+__device__ void grow_wide(const View& v, const LevelScratch& s, const TreeView& tv, const ct_node& nd, size_t toff,
+                          uint32_t* wsm, uint32_t lane) {
+  const uint32_t C = v.n_classes, F = v.n_features, m = v.max_features;
+  const uint32_t tslot = nd.slot + tv.slot_base;
+  uint32_t* row_s = wsm;
+  uint32_t* lab_s = row_s + WIDE_ROWS;
+  uint32_t* rr_s = lab_s + WIDE_ROWS;
+  uint32_t* cnt = rr_s + WIDE_ROWS;
+  uint32_t* T = cnt + C;
+  WideEntry* wstack = reinterpret_cast<WideEntry*>(wsm + subtree_stacks_word(C));
+  SubEntry* stack1 = reinterpret_cast<SubEntry*>(wstack + WIDE_STACK);
+  const unsigned lt = lanemask_lt();
+  const uint32_t n0 = nd.n;
+  const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+  uint32_t rowr[4], labr[4], rrr[4];
+  uint64_t kk[4];
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) {
+    const uint32_t slot = lane + 32 * k;
+    const bool have = slot < n0;
+    rowr[k] = have ? (uint32_t)l0[slot] : 0u;
+    labr[k] = have ? label_of<LabT>(v, rowr[k]) : NONE;
+    row_s[slot] = rowr[k];
+    lab_s[slot] = labr[k];
+    kk[k] = have ? ((uint64_t)rowr[k] << 7) | slot : ~0ull;
+  }
+  warp_sort128(kk, lane);  // position e holds the slot of rank e by row id
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k)
+    if (lane + 32 * k < n0) rr_s[(uint32_t)kk[k] & 127u] = lane + 32 * k;
+  __syncwarp();
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k) rrr[k] = lane + 32 * k < n0 ? rr_s[lane + 32 * k] : 0u;
+  WideEntry cur{};
+#pragma unroll
+  for (uint32_t k = 0; k < 4; ++k)
+    cur.m[k] = n0 >= 32 * (k + 1) ? FULL : (n0 > 32 * k ? (1u << (n0 - 32 * k)) - 1u : 0u);
+  cur.raw = nd.raw_id;
+  cur.key = nd.key;
+  int wsp = 0;
+  while (true) {
+    bool in[4];
+    uint32_t n = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      in[k] = (cur.m[k] >> lane) & 1u;
+      n += __popc(cur.m[k]);
+    }
+    // class totals of the node
+    for (uint32_t c = lane; c < C; c += 32) T[c] = 0;
+    __syncwarp();
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) {
+      const uint32_t c = in[k] ? labr[k] : NONE;
+      const unsigned grp = __match_any_sync(FULL, c);
+      if (in[k] && (grp & lt) == 0u) T[c] += __popc(grp);
+      __syncwarp();
+    }
+    uint32_t tsum = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) tsum += in[k] ? T[labr[k]] : 0u;
+    const int64_t sr0 = (int64_t)warp_sum_u32(tsum);
+    const double nn = (double)n;
+    double best = dinf();
+    uint32_t bf = NONE, bp = 0, bm[4] = {0u, 0u, 0u, 0u};
+    float bil = 0.f, bir = 0.f, bthr = 0.f;
+    uint32_t taken = 0;
+    uint32_t f_nx = feature_perm(0, F, cur.key, v.feistel_h);
+    float x_nx[4];
+#pragma unroll
+    for (uint32_t k = 0; k < 4; ++k) x_nx[k] = in[k] ? v.x_fm[(size_t)f_nx * v.n_rows + rowr[k]] : 0.f;
+    for (uint32_t i = 0; i < F && taken < m; ++i) {
+      const uint32_t f = f_nx;
+      const float* xf = v.x_fm + (size_t)f * v.n_rows;
+      uint32_t ord[4];
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) ord[k] = f32_order(x_nx[k]);
+      if (i + 1 < F) {
+        f_nx = feature_perm(i + 1, F, cur.key, v.feistel_h);
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) x_nx[k] = in[k] ? v.x_fm[(size_t)f_nx * v.n_rows + rowr[k]] : 0.f;
+      }
+      uint32_t lmin = 0xffffffffu, lmax = 0u;
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        if (in[k]) {
+          lmin = min(lmin, ord[k]);
+          lmax = max(lmax, ord[k]);
+        }
+      if (__reduce_min_sync(FULL, lmin) == __reduce_max_sync(FULL, lmax)) continue;
+      ++taken;
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k)
+        kk[k] = in[k] ? ((uint64_t)ord[k] << 32) | ((uint64_t)rrr[k] << 7) | (lane + 32 * k) : ~0ull;
+      warp_sort128(kk, lane);  // position lane + 32 k
+      for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
+      __syncwarp();
+      int64_t sl = 0, sr = sr0;
+      double bsc = dinf();
+      uint32_t bpos = NONE;
+      float bgl = 0.f, bgr = 0.f;
+#pragma unroll
+      for (uint32_t k = 0; k < 4; ++k) {
+        const uint32_t p = lane + 32 * k;
+        const bool valid = p < n;
+        const uint32_t slot = (uint32_t)kk[k] & 127u;
+        const uint32_t c = valid ? lab_s[slot] : NONE;
+        const float x = f32_unorder((uint32_t)(kk[k] >> 32));
+        float xn = __shfl_down_sync(FULL, x, 1);
+        const float first_next = __shfl_sync(FULL, k + 1 < 4 ? f32_unorder((uint32_t)(kk[k + 1 < 4 ? k + 1 : k] >> 32)) : 0.f, 0);
+        if (lane == 31) xn = first_next;
+        const unsigned grp = __match_any_sync(FULL, c);
+        const int32_t kr = valid ? (int32_t)(cnt[c] + __popc(grp & lt)) : 0;
+        const int32_t tc = valid ? (int32_t)T[c] : 0;
+        __syncwarp();
+        if (valid && (grp & lt) == 0u) cnt[c] += __popc(grp);
+        __syncwarp();
+        const int32_t il = warp_incl_scan_i32(valid ? 2 * kr + 1 : 0);
+        const int32_t ir = warp_incl_scan_i32(valid ? 1 - 2 * (tc - kr) : 0);
+        const int64_t SL = sl + il, SR = sr + ir;
+        sl += __shfl_sync(FULL, il, 31);
+        sr += __shfl_sync(FULL, ir, 31);
+        if (valid && p + 1 < n && is_candidate_sorted(x, xn)) {
+          const double nl = (double)(p + 1);
+          const double nr = __dsub_rn(nn, nl);
+          const double gl = gini_part(SL, nl, nn);
+          const double gr = gini_part(SR, nr, nn);
+          const double sc = __dadd_rn(gl, gr);
+          if (sc < bsc) {
+            bsc = sc;
+            bpos = p;
+            bgl = __double2float_rn(gl);
+            bgr = __double2float_rn(gr);
+          }
+        }
+      }
+      warp_argmin2(bsc, bpos, bgl, bgr);
+      if (bsc < dinf() && (bsc < best || (bsc == best && f < bf))) {
+        best = bsc;
+        bf = f;
+        bp = bpos;
+        bil = bgl;
+        bir = bgr;
+        uint32_t wb[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+          const uint32_t p = lane + 32 * k;
+          const uint32_t slot = (uint32_t)kk[k] & 127u;
+          const uint32_t bit = (p < n && p <= bpos) ? (1u << (slot & 31u)) : 0u;
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) wb[q] |= (slot >> 5) == q ? bit : 0u;
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) bm[q] = __reduce_or_sync(FULL, wb[q]);
+        const uint32_t s0 = (uint32_t)__shfl_sync(FULL, pick4(kk, bpos >> 5), bpos & 31u) & 127u;
+        const uint32_t s1 = (uint32_t)__shfl_sync(FULL, pick4(kk, (bpos + 1) >> 5), (bpos + 1) & 31u) & 127u;
+        bthr = midpoint(xf[row_s[s0]], xf[row_s[s1]]);
+      }
+    }
+    bool split = bf != NONE;
+    uint32_t c0 = 0;
+    if (split && lane == 0) {
+      c0 = atomicAdd(&tv.n_nodes[tslot], 2u);
+      if (c0 + 2ull > tv.capacity) {
+        atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+        split = false;
+      }
+    }
+    split = __shfl_sync(FULL, split, 0);
+    c0 = __shfl_sync(FULL, c0, 0);
+    if (!split) {
+      if (lane == 0) {
+        tv.left[toff + cur.raw] = 0;
+        tv.right[toff + cur.raw] = 0;
+        tv.feature[toff + cur.raw] = 0;
+        tv.threshold[toff + cur.raw] = 0.f;
+        tv.value[toff + cur.raw] = lab_s[lowest_slot(cur.m)];
+      }
+    } else {
+      if (lane == 0) {
+        tv.left[toff + cur.raw] = c0;
+        tv.right[toff + cur.raw] = c0 + 1;
+        tv.feature[toff + cur.raw] = bf;
+        tv.threshold[toff + cur.raw] = bthr;
+        tv.value[toff + cur.raw] = 0;
+      }
+      const float imps[2] = {bil, bir};
+      const uint64_t pkey = cur.key;
+      for (int side = 0; side < 2; ++side) {
+        uint32_t cm[4];
+#pragma unroll
+        for (uint32_t q = 0; q < 4; ++q) cm[q] = side ? cur.m[q] & ~bm[q] : bm[q];
+        const uint32_t nc = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]) + __popc(cm[3]);
+        const uint32_t raw = c0 + (uint32_t)side;
+        if (imps[side] == 0.0f || nc < v.mss) {
+          if (lane == 0) {
+            tv.left[toff + raw] = 0;
+            tv.right[toff + raw] = 0;
+            tv.feature[toff + raw] = 0;
+            tv.threshold[toff + raw] = 0.f;
+            tv.value[toff + raw] = lab_s[lowest_slot(cm)];
+          }
+        } else if (nc <= 32) {
+          // lane i takes the child's i-th slot (slot order = feature-0 order)
+          uint32_t row = 0, lab = NONE;
+          uint32_t before = 0;
+#pragma unroll
+          for (uint32_t q = 0; q < 4; ++q) {
+            const uint32_t c = __popc(cm[q]);
+            if (lane >= before && lane < before + c) {
+              const uint32_t slot = 32 * q + __fns(cm[q], 0, (int)(lane - before + 1));
+              row = row_s[slot];
+              lab = lab_s[slot];
+            }
+            before += c;
+          }
+          const SubEntry e{nc >= 32 ? FULL : ((1u << nc) - 1u), raw, child_key(pkey, side)};
+          grow_small<IdxT, LabT>(v, s, tv, tslot, toff, row, lab, e, stack1, lane);
+        } else if (wsp < (int)WIDE_STACK) {
+          if (lane == 0) {
+            WideEntry e{};
+#pragma unroll
+            for (uint32_t q = 0; q < 4; ++q) e.m[q] = cm[q];
+            e.raw = raw;
+            e.key = child_key(pkey, side);
+            wstack[wsp] = e;
+          }
+          ++wsp;
+        } else {
+          if (lane == 0) atomicOr(&s.ctr->error, DEV_ERR_INTERNAL);
+        }
+      }
+    }
+    __syncwarp();
+    if (wsp == 0) break;
+    --wsp;
+    cur = wstack[wsp];
+    __syncwarp();
+  }
+}
+
+
+
+// Subtree roots of at most 32 rows (the others return at once).
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
+  __shared__ SubEntry stack_all[WARPS_PER_BLOCK][33];
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
+  const ct_node nd = small[w];
+  if (nd.n > 32) return;
+  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+  const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+  const bool have = lane < nd.n;
+  const uint32_t row = have ? (uint32_t)l0[lane] : 0u;
+  const uint32_t lab = have ? label_of<LabT>(v, row) : NONE;
+  const SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
+  grow_small<IdxT, LabT>(v, s, tv, nd.slot + tv.slot_base, toff, row, lab, cur, stack_all[threadIdx.x >> 5], lane);
+}
+
+// Subtree roots of 33..128 rows (the others return at once).
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_subtree_wide(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
+  extern __shared__ __align__(16) uint32_t sub_smem[];
+  const uint32_t w = global_warp();
+  const uint32_t lane = lane_id();
+  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
+  const ct_node nd = small[w];
+  if (nd.n <= 32) return;
+  uint32_t* wsm = sub_smem + (threadIdx.x >> 5) * subtree_warp_words(v.n_classes);
+  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+  grow_wide<IdxT, LabT>(v, s, tv, nd, toff, wsm, lane);
 }
 
 __global__ void k_reset_step(Counters* c, uint32_t n_nodes) {
@@ -941,15 +1275,22 @@ int launch_children(const View& v, uint32_t ib, uint32_t lb, const ct_node* node
 }
 
 int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
-                    const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
+                    bool wide, const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
   if (cap_small == 0) return CT_OK;
   Prof* pf = current_prof();
   pf->begin(CT_K_SUBTREE);
 #define CALL(I, L) k_subtree<I, L><<<blocks_for_warps(cap_small), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, cap_small)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
+  if (wide) {
+    const size_t smem = (size_t)WARPS_PER_BLOCK * subtree_warp_words(v.n_classes) * sizeof(uint32_t);
+#define CALL(I, L) \
+  k_subtree_wide<I, L><<<blocks_for_warps(cap_small), THREADS_PER_BLOCK, smem, st>>>(v, small, s, tv, cap_small)
+    CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  }
   pf->end();
-  pf->launched(CT_K_SUBTREE);
+  pf->launched(CT_K_SUBTREE, wide ? 2 : 1);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

@@ -165,8 +165,8 @@ class RandomForestClassifier:
                  autotune=False):
         if fit_mode not in ("batched", "plain"):
             raise ValueError("fit_mode must be 'batched' or 'plain'")
-        if not 0 <= int(subtree_cutoff) <= 32:
-            raise ValueError("subtree_cutoff must be in [0, 32]")
+        if not 0 <= int(subtree_cutoff) <= 128:
+            raise ValueError("subtree_cutoff must be in [0, 128]")
         # nodes of at most subtree_cutoff rows are grown whole by one warp
         # (same trees; 0 keeps every node in the level steps)
         self.subtree_cutoff = int(subtree_cutoff)

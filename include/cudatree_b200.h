@@ -115,8 +115,8 @@ typedef struct ct_fit_options {
   uint32_t mode;            /* CT_FIT_PLAIN or CT_FIT_BATCHED                       */
   uint32_t bfs_threshold;   /* plain: nodes with n <= this go to the BFS queue
                                (random_tree.py:616-622); 0 = reference formula     */
-  uint32_t subtree_cutoff;  /* batched: nodes with n <= this are grown whole by one
-                               warp (<= 32; 0 disables)                             */
+  uint32_t subtree_cutoff;  /* nodes with n <= this are grown whole by one warp
+                               (<= 128; 0 disables); the trees do not change        */
   uint32_t scan_piece;      /* elements per split-scan work item (0 = default)      */
   uint32_t reserved[4];
 } ct_fit_options;
@@ -218,7 +218,8 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
 /* Autotuner: fits n_trees sample trees (first tree 0) with each candidate
  * option set of the given mode and returns the fastest in *best (its time in
  * *best_ms).  Every candidate grows the same trees, so the choice changes
- * speed only.  Batched: scan piece length x warp-subtree cutoff; plain: the
+ * speed only.  Batched: scan piece length (1024, 2048, 4096) x warp-subtree
+ * cutoff (0, 32, 128); plain: the
  * depth-first/breadth-first switch, which the reference sets with an offline
  * regression (estimate_threshold.py, random_forest.py:278-289).  The
  * workspace must hold ct_autotune_workspace_size bytes; lists and trees as

@@ -112,17 +112,18 @@ def test_compact_nodes_match_packed_and_oracle(cuda_device, n, f, c, seed):
 
 @pytest.mark.parametrize("mss", [1, 3])
 def test_warp_subtrees_grow_the_same_trees(cuda_device, mss):
-    """Nodes of at most subtree_cutoff rows are grown whole by one warp; the
-    trees must equal those of the level steps alone (cutoff 0) and the
-    oracle's, for deep trees (noise labels), ties and min_samples_split."""
+    """Nodes of at most subtree_cutoff rows are grown whole by one warp (one
+    row per lane up to 32, four rows per lane up to 128); the trees must equal
+    those of the level steps alone (cutoff 0) and the oracle's, for deep trees
+    (noise labels), ties and min_samples_split."""
     rng = np.random.default_rng(1031)  # labels independent of x
     x, _ = _synthetic(1500, 24, 5, 31)
     y = rng.integers(0, 5, size=1500)
     forests = {}
-    for cut in (0, 8, 32):
+    for cut in (0, 8, 32, 64, 128):
         forests[cut] = RandomForestClassifier(n_estimators=4, min_samples_split=mss, seed=77,
                                               subtree_cutoff=cut).fit(x, y)
-    for cut in (8, 32):
+    for cut in (8, 32, 64, 128):
         for a, b in zip(forests[cut]._trees, forests[0]._trees):
             np.testing.assert_array_equal(a.left_children, b.left_children)
             np.testing.assert_array_equal(a.feature_idx_array, b.feature_idx_array)
@@ -130,6 +131,7 @@ def test_warp_subtrees_grow_the_same_trees(cuda_device, mss):
             np.testing.assert_array_equal(a.values_array, b.values_array)
     ref = O.fit_forest(x, y, n_estimators=4, min_samples_split=mss, seed=77)
     _assert_same_trees(forests[32]._trees, ref.trees)
+    _assert_same_trees(forests[128]._trees, ref.trees)
 
 
 def test_nan_samples_are_rejected(cuda_device):
@@ -148,8 +150,8 @@ def test_autotune_keeps_the_trees(cuda_device):
     """The autotuner only picks among options that grow the same trees."""
     x, y = _synthetic(4000, 12, 4, 9)
     tuned = RandomForestClassifier(n_estimators=6, seed=5, autotune=True).fit(x, y)
-    assert tuned._tuned is not None and tuned._tuned["scan_piece"] in (1024, 2048, 4096, 8192)
-    assert tuned._tuned["subtree_cutoff"] in (0, 16, 32)
+    assert tuned._tuned is not None and tuned._tuned["scan_piece"] in (1024, 2048, 4096)
+    assert tuned._tuned["subtree_cutoff"] in (0, 32, 128)
     ref = RandomForestClassifier(n_estimators=6, seed=5).fit(x, y)
     for a, b in zip(tuned._trees, ref._trees):
         np.testing.assert_array_equal(a.left_children, b.left_children)
