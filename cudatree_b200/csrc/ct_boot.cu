@@ -8,6 +8,8 @@
 // set of marked rows.  The compaction is the tiled stable partition of
 // ct_partition.cu with the right (out-of-bag) part dropped; all slots of a
 // call are compacted by one launch.
+#include <algorithm>
+
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -34,6 +36,24 @@ __global__ void k_count_marks(const uint8_t* mark, uint32_t n, uint32_t* out) {
 
 __global__ void k_set_u32(uint32_t* p, uint32_t v, uint32_t count) {
   for (uint32_t i = threadIdx.x; i < count; i += blockDim.x) p[i] = v;
+}
+
+template <typename IdxT, typename LabT>
+__global__ void k_pack_presort(const IdxT* __restrict__ in, const LabT* __restrict__ labels, IdxT* __restrict__ out,
+                               uint64_t count, uint32_t shift) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t r = in[i];
+    out[i] = (IdxT)(r | ((uint32_t)__ldg(labels + r) << shift));
+  }
+}
+
+template <typename IdxT, typename LabT>
+void launch_pack_presort(const ct_problem* p, void* out, uint32_t shift, cudaStream_t st) {
+  const uint64_t count = (uint64_t)p->n_rows * p->n_features;
+  const uint32_t blocks = (uint32_t)std::min<uint64_t>((count + 255) / 256, 148u * 16u);
+  k_pack_presort<IdxT, LabT><<<blocks, 256, 0, st>>>(reinterpret_cast<const IdxT*>(p->presort),
+                                                     reinterpret_cast<const LabT*>(p->labels),
+                                                     reinterpret_cast<IdxT*>(out), count, shift);
 }
 
 struct BootPlan {
@@ -101,20 +121,22 @@ size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_
 }
 
 // Compacts slots [slot_lo, slot_lo + n_slots) for trees tree_lo.., one launch
-// per phase.  Error bits accumulate in the workspace's word [1]; the caller
-// zeroes it once and reads it after.
+// per phase.  src is the [F][N] presort, or its packed copy (entries
+// row | label << s, row ids under row_mask).  Error bits accumulate in the
+// workspace's word [1]; the caller zeroes it once and reads it after.
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
-                   uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st) {
+                   const void* src, uint32_t row_mask, uint32_t* n_in_dev, void* ws, size_t wsb,
+                   cudaStream_t st) {
   const uint32_t N = p->n_rows, F = p->n_features;
   CT_ARG_CHECK(n_slots >= 1 && slot_lo + n_slots <= l->n_slots, "slot out of range");
   CT_ARG_CHECK(l->stride >= N, "list stride smaller than n_rows");
-  CT_ARG_CHECK(p->presort != nullptr, "presort is NULL");
+  CT_ARG_CHECK(src != nullptr, "presort is NULL");
   const size_t ib = p->index_bytes;
   const size_t slot_bytes = (size_t)F * l->stride * ib;
   char* dst = reinterpret_cast<char*>(l->si0) + slot_lo * slot_bytes;
   if (!p->bootstrap) {
     for (uint32_t s = 0; s < n_slots; ++s)
-      CT_CUDA_TRY(cudaMemcpy2DAsync(dst + s * slot_bytes, (size_t)l->stride * ib, p->presort, (size_t)N * ib,
+      CT_CUDA_TRY(cudaMemcpy2DAsync(dst + s * slot_bytes, (size_t)l->stride * ib, src, (size_t)N * ib,
                                     (size_t)N * ib, F, cudaMemcpyDeviceToDevice, st));
     k_set_u32<<<1, 256, 0, st>>>(n_in_dev + slot_lo, N, n_slots);
     CT_CUDA_TRY(cudaGetLastError());
@@ -141,7 +163,7 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
                    (size_t)slot_lo * mark_bit_words(N);
   launch_pack_marks(mark, bits, N, n_slots, st);
   BootPlan b;
-  b.presort = p->presort;
+  b.presort = src;
   b.si0 = dst;
   b.bits = bits;
   b.segs = L.segs;
@@ -167,12 +189,28 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
   w.ticket = L.words;
   w.error = L.words + 1;
   w.n_features = F;
+  w.row_mask = row_mask;
   return launch_seg_partition((uint32_t)ib, w, 0, (uint64_t)tiles_per * n_slots, st);
+}
+
+// The presort with each row's label above its row id (entry row | label <<
+// shift), [F][N] at out; out must not overlap the presort.
+int pack_presort(const ct_problem* p, void* out, uint32_t shift, cudaStream_t st) {
+  CT_ARG_CHECK(p->presort != nullptr, "presort is NULL");
+  if (p->index_bytes == 2) {
+    if (p->label_bytes == 1) launch_pack_presort<uint16_t, uint8_t>(p, out, shift, st);
+    else launch_pack_presort<uint16_t, uint16_t>(p, out, shift, st);
+  } else {
+    if (p->label_bytes == 1) launch_pack_presort<uint32_t, uint8_t>(p, out, shift, st);
+    else launch_pack_presort<uint32_t, uint16_t>(p, out, shift, st);
+  }
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
 }
 
 int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree, uint32_t* n_in_dev,
                       void* ws, size_t wsb, cudaStream_t st) {
-  return bootstrap_many(p, l, slot, 1, tree, n_in_dev, ws, wsb, st);
+  return bootstrap_many(p, l, slot, 1, tree, p->presort, 0xffffffffu, n_in_dev, ws, wsb, st);
 }
 
 }  // namespace ct

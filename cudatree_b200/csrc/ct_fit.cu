@@ -23,7 +23,9 @@ namespace ct {
 
 size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots);
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
-                   uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
+                   const void* src, uint32_t row_mask, uint32_t* n_in_dev, void* ws, size_t wsb,
+                   cudaStream_t st);
+int pack_presort(const ct_problem* p, void* out, uint32_t shift, cudaStream_t st);
 
 namespace {
 
@@ -41,7 +43,7 @@ __global__ void k_root_hist(View v, const uint32_t* n_in, uint32_t slot_lo, uint
   const uint32_t n = n_in[slot];
   const IdxT* lst = list_ptr<IdxT>(v, 0, slot, 0);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    atomicAdd(&hist[label_of<LabT>(v, lst[i])], 1u);
+    atomicAdd(&hist[entry_label<LabT>(v, lst[i])], 1u);
   __syncthreads();
   for (uint32_t c = threadIdx.x; c < C; c += blockDim.x)
     if (hist[c]) atomicAdd(&hist_out[(size_t)blockIdx.y * C + c], hist[c]);
@@ -76,7 +78,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
       tv.right[off] = 0;
       tv.feature[off] = 0;
       tv.threshold[off] = 0.f;
-      tv.value[off] = n ? label_of<LabT>(v, lst[0]) : 0u;
+      tv.value[off] = n ? entry_label<LabT>(v, lst[0]) : 0u;
     } else {
       const uint32_t idx = atomicAdd(&ctr->n_next, 1u);
       if (idx < cap) {
@@ -107,10 +109,11 @@ void begin_level(Counters* c, cudaStream_t st) {
   current_prof()->launched(CT_K_CHILDREN);
 }
 
-// Algorithmic bytes of one level, from the device counters of the level.
-void account_level(const ct_problem* p, const Counters& h) {
+// Algorithmic bytes of one level, from the device counters of the level
+// (a scanned entry that carries its label needs no label read).
+void account_level(const ct_problem* p, const View& view, const Counters& h) {
   Prof* pf = current_prof();
-  const double w = p->index_bytes, l = p->label_bytes, v = sizeof(float);
+  const double w = p->index_bytes, l = view.lab_shift ? 0.0 : p->label_bytes, v = sizeof(float);
   pf->stats.bytes[CT_K_SCAN] += (double)h.scan_elems * (w + l + v);
   pf->stats.bytes[CT_K_MARK] += (double)h.split_total * (w + 1.0);
   pf->stats.bytes[CT_K_PARTITION] += (double)h.split_total * p->n_features * (2.0 * w + 1.0);
@@ -273,7 +276,7 @@ int level_loop(const ct_problem* p, const View& v, const FitLayout& L, const Tre
     CT_CUDA_TRY(cudaGetLastError());
     CT_TRY(step(p, v, L, tv, cur, n, total, st));
     CT_TRY(read_counters(L, &h, st));
-    account_level(p, h);
+    account_level(p, v, h);
     if (L.subtree_cut) L.small_bound = h.n_small;
     n = h.n_next;
     total = h.next_total;
@@ -305,14 +308,37 @@ uint32_t default_bfs_threshold(const ct_problem* p) {
   return (uint32_t)v;
 }
 
+// The fit's view: list entries carry their row's label when it fits
+// (fit_label_shift).  The packed presort that seeds the lists goes to slot 0
+// of buffer 1, which no step writes before the first partition.
+View fit_view(const ct_problem* p, const ct_lists* l) {
+  View v = make_view(p, l);
+  if (const uint32_t sh = fit_label_shift(p)) {
+    v.lab_shift = sh;
+    v.row_mask = (1u << sh) - 1u;
+  }
+  return v;
+}
+
+int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const void** src, cudaStream_t st) {
+  *src = p->presort;
+  if (v.lab_shift) {
+    CT_TRY(pack_presort(p, l->si1, v.lab_shift, st));
+    *src = l->si1;
+  }
+  return CT_OK;
+}
+
 int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
                 const FitLayout& L, const ct_tree_buffers* trees, cudaStream_t st) {
-  View v = make_view(p, l);
+  View v = fit_view(p, l);
   TreeView tv = tree_view(trees, 0);
   CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
   CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
   current_prof()->begin(CT_K_BOOTSTRAP);
-  CT_TRY(bootstrap_many(p, l, 0, n_trees, first_tree, L.n_in, L.boot_ws, L.boot_bytes, st));
+  const void* src = nullptr;
+  CT_TRY(seed_source(p, l, v, &src, st));
+  CT_TRY(bootstrap_many(p, l, 0, n_trees, first_tree, src, v.row_mask, L.n_in, L.boot_ws, L.boot_bytes, st));
   current_prof()->end();
   for (uint32_t s = 0; s < n_trees; ++s) account_bootstrap(p);
   CT_TRY(check_boot_error(L, st));
@@ -331,7 +357,7 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
 int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
               const ct_fit_options* o, const FitLayout& L, const ct_tree_buffers* trees,
               cudaStream_t st) {
-  View v = make_view(p, l);
+  View v = fit_view(p, l);
   const uint32_t C = p->n_classes;
   const uint32_t thr = o->bfs_threshold ? o->bfs_threshold : default_bfs_threshold(p);
   struct Pending {
@@ -343,7 +369,9 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
     TreeView tv = tree_view(trees, t);
     CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
     current_prof()->begin(CT_K_BOOTSTRAP);
-    CT_TRY(bootstrap_many(p, l, 0, 1, first_tree + t, L.n_in, L.boot_ws, L.boot_bytes, st));
+    const void* src = nullptr;  // packed again per tree: the previous tree's steps wrote buffer 1
+    CT_TRY(seed_source(p, l, v, &src, st));
+    CT_TRY(bootstrap_many(p, l, 0, 1, first_tree + t, src, v.row_mask, L.n_in, L.boot_ws, L.boot_bytes, st));
     current_prof()->end();
     account_bootstrap(p);
     CT_TRY(check_boot_error(L, st));
@@ -371,7 +399,7 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
       begin_level(L.s.ctr, st);
       CT_TRY(step(p, v, L, tv, 0, 1, cur.nd.n, st));
       CT_TRY(read_counters(L, &h, st));
-      account_level(p, h);
+      account_level(p, v, h);
       if (L.subtree_cut) L.small_bound = h.n_small;
       std::vector<ct_node> kids(h.n_next);
       std::vector<uint32_t> ktot((size_t)h.n_next * C);

@@ -123,6 +123,7 @@ struct PartWork {
   uint32_t* ticket;
   uint32_t* error;
   uint32_t n_features;
+  uint32_t row_mask;      // list entry -> row id of its mark bit (see View::row_mask)
 };
 
 // View of the problem + lists passed by value to kernels.
@@ -142,6 +143,12 @@ struct View {
   uint32_t max_features;
   uint32_t mss;
   int feistel_h;
+  // List entries.  Lists a caller passes in hold plain row ids (row_mask all
+  // ones, lab_shift 0).  The fit's own lists hold row | label << lab_shift
+  // whenever both fit one entry (fit_label_shift), so a kernel that reads an
+  // entry has the row's label without a gather into `labels`.
+  uint32_t row_mask;
+  uint32_t lab_shift;
 };
 
 // Packed mark table: bit r of a slot's words is row r's left flag.  The
@@ -162,9 +169,10 @@ __device__ __forceinline__ IdxT* list_ptr(const View& v, uint32_t buf, uint32_t 
   IdxT* base = reinterpret_cast<IdxT*>(buf ? v.si1 : v.si0);
   return base + ((size_t)slot * v.n_features + f) * v.stride;
 }
+__device__ __forceinline__ uint32_t entry_row(const View& v, uint32_t e) { return e & v.row_mask; }
 template <typename LabT>
-__device__ __forceinline__ uint32_t label_of(const View& v, uint32_t row) {
-  return (uint32_t)reinterpret_cast<const LabT*>(v.labels)[row];
+__device__ __forceinline__ uint32_t entry_label(const View& v, uint32_t e) {
+  return v.lab_shift ? e >> v.lab_shift : (uint32_t)reinterpret_cast<const LabT*>(v.labels)[e];
 }
 
 // Raw tree arrays (fit mode).
@@ -309,6 +317,9 @@ PartWork level_part_work(const View& v, const LevelScratch& s);
 int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
 
 View make_view(const ct_problem* p, const ct_lists* l);
+// Bits of a row id when a row id and a label fit one list entry together
+// (the shift of the label), else 0.
+uint32_t fit_label_shift(const ct_problem* p);
 
 // One request of a multi-request predict launch (ct_predict.cu): blocks
 // [block0, block0 + tiles * ceil(n_trees / group)) of the launch are its,

@@ -78,7 +78,7 @@ k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t sca
         f = feature_perm(i, v.n_features, nd.key, v.feistel_h);
         const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
         const float* xf = v.x_fm + (size_t)f * v.n_rows;
-        usable = xf[lst[0]] != xf[lst[nd.n - 1]];
+        usable = xf[entry_row(v, lst[0])] != xf[entry_row(v, lst[nd.n - 1])];
       }
       const unsigned mask = __ballot_sync(FULL, usable);
       const uint32_t rank = __popc(mask & lanemask_lt());
@@ -146,7 +146,7 @@ k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t 
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r)
-      cs[r] = (base + r * 32 + lane < hi) ? label_of<LabT>(v, rows[r]) : NONE;
+      cs[r] = (base + r * 32 + lane < hi) ? entry_label<LabT>(v, rows[r]) : NONE;
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const unsigned grp = __match_any_sync(FULL, cs[r]);
@@ -234,8 +234,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const bool valid = lo + r * 32 + lane < hi;
-      cs[r] = valid ? label_of<LabT>(v, rows[r]) : NONE;
-      xs[r] = valid ? xf[rows[r]] : 0.f;
+      cs[r] = valid ? entry_label<LabT>(v, rows[r]) : NONE;
+      xs[r] = valid ? xf[entry_row(v, rows[r])] : 0.f;
     }
   }
   for (uint32_t base = lo; base < hi; base += B) {
@@ -244,8 +244,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const bool valid = base + B + r * 32 + lane < hi;
-      cs_n[r] = valid ? label_of<LabT>(v, rows_n[r]) : NONE;
-      xs_n[r] = valid ? xf[rows_n[r]] : 0.f;
+      cs_n[r] = valid ? entry_label<LabT>(v, rows_n[r]) : NONE;
+      xs_n[r] = valid ? xf[entry_row(v, rows_n[r])] : 0.f;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
@@ -262,7 +262,7 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       float xn = __shfl_down_sync(FULL, x, 1);
       const float first_next = (r + 1 < SCAN_BATCH) ? __shfl_sync(FULL, xs[r + 1 < SCAN_BATCH ? r + 1 : r], 0) : x_e;
       if (lane == 31) xn = first_next;
-      if (valid && p + 1 == hi && p + 1 < n) xn = xf[lst[p + 1]];  // next piece's first element
+      if (valid && p + 1 == hi && p + 1 < n) xn = xf[entry_row(v, lst[p + 1])];  // next piece's first element
       const unsigned grp = __match_any_sync(FULL, c);
       uint32_t k = 0;
       int64_t tc = 0;
@@ -361,7 +361,7 @@ k_split_reduce(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
       r.pos = bp;
       r.imp_left = il;
       r.imp_right = ir;
-      r.threshold = midpoint(xf[lst[bp]], xf[lst[bp + 1]]);
+      r.threshold = midpoint(xf[entry_row(v, lst[bp])], xf[entry_row(v, lst[bp + 1])]);
     } else {
       r.score = dinf();
       r.feature = NONE;
@@ -407,7 +407,7 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       tv.right[off + nd.raw_id] = 0;
       tv.feature[off + nd.raw_id] = 0;
       tv.threshold[off + nd.raw_id] = 0.f;
-      tv.value[off + nd.raw_id] = label_of<LabT>(v, l0[0]);
+      tv.value[off + nd.raw_id] = entry_label<LabT>(v, l0[0]);
     }
   }
   split = __shfl_sync(FULL, split, 0);
@@ -508,8 +508,8 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
     cls[r] = NONE;
     if (p < hi) {
       const bool left = p <= sr.pos;
-      mk[rows[r]] = left ? 1 : 0;
-      if (left) cls[r] = label_of<LabT>(v, rows[r]);
+      mk[entry_row(v, rows[r])] = left ? 1 : 0;
+      if (left) cls[r] = entry_label<LabT>(v, rows[r]);
     }
   }
 #pragma unroll
@@ -557,7 +557,7 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
         tv.right[off] = 0;
         tv.feature[off] = 0;
         tv.threshold[off] = 0.f;
-        tv.value[off] = label_of<LabT>(v, l0[0]);
+        tv.value[off] = entry_label<LabT>(v, l0[0]);
       }
       continue;
     }
@@ -842,8 +842,9 @@ __device__ void grow_wide(const View& v, const LevelScratch& s, const TreeView& 
   for (uint32_t k = 0; k < 4; ++k) {
     const uint32_t slot = lane + 32 * k;
     const bool have = slot < n0;
-    rowr[k] = have ? (uint32_t)l0[slot] : 0u;
-    labr[k] = have ? label_of<LabT>(v, rowr[k]) : NONE;
+    const uint32_t e = have ? (uint32_t)l0[slot] : 0u;
+    rowr[k] = have ? entry_row(v, e) : 0u;
+    labr[k] = have ? entry_label<LabT>(v, e) : NONE;
     row_s[slot] = rowr[k];
     lab_s[slot] = labr[k];
     kk[k] = have ? ((uint64_t)rowr[k] << 7) | slot : ~0ull;
@@ -1078,8 +1079,9 @@ k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv
   const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
   const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
   const bool have = lane < nd.n;
-  const uint32_t row = have ? (uint32_t)l0[lane] : 0u;
-  const uint32_t lab = have ? label_of<LabT>(v, row) : NONE;
+  const uint32_t e = have ? (uint32_t)l0[lane] : 0u;
+  const uint32_t row = have ? entry_row(v, e) : 0u;
+  const uint32_t lab = have ? entry_label<LabT>(v, e) : NONE;
   const SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
   grow_small<IdxT, LabT>(v, s, tv, nd.slot + tv.slot_base, toff, row, lab, cur, stack_all[threadIdx.x >> 5], lane);
 }
@@ -1318,6 +1320,7 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   w.ticket = &s.ctr->ticket;
   w.error = &s.ctr->error;
   w.n_features = v.n_features;
+  w.row_mask = v.row_mask;
   return w;
 }
 
@@ -1343,7 +1346,15 @@ View make_view(const ct_problem* p, const ct_lists* l) {
   v.max_features = p->max_features;
   v.mss = p->min_samples_split;
   v.feistel_h = feistel_half_bits(p->n_features);
+  v.row_mask = 0xffffffffu;
+  v.lab_shift = 0;
   return v;
+}
+
+uint32_t fit_label_shift(const ct_problem* p) {
+  const uint32_t row_bits = p->n_rows > 1 ? 32u - (uint32_t)__builtin_clz(p->n_rows - 1) : 1u;
+  const uint32_t lab_bits = p->n_classes > 1 ? 32u - (uint32_t)__builtin_clz(p->n_classes - 1) : 0u;
+  return (row_bits <= 31 && row_bits + lab_bits <= 8 * p->index_bytes) ? row_bits : 0u;
 }
 
 int check_problem(const ct_problem* p) {

@@ -5,7 +5,9 @@
 //
 // A segment is one node's range [0, n) in every feature list.  Left rows
 // (mark != 0) keep their order at [0, nl), right rows keep theirs at
-// [nl, n).  Two kernels by segment size:
+// [nl, n).  Entries move unchanged; an entry's row id (its mark bit) is
+// entry & row_mask, since fit lists carry the label above the row id.
+// Two kernels by segment size:
 //
 //   k_part_small  n <= SMALL_SEG: one warp per segment loops over all
 //                 features; ranks are popc of a ballot.  For n <= 16 a warp
@@ -77,7 +79,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < R; ++r) {
         if (f_lo + r * per >= f_hi) break;
         const uint32_t f = f_lo + r * per + sub;
-        const bool left = valid[r] && left_bit(sg.bits, rows[r]);
+        const bool left = valid[r] && left_bit(sg.bits, rows[r] & w.row_mask);
         const unsigned lm = __ballot_sync(FULL, left) & gmask;
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (p - rl);
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const uint32_t f = f_lo + r;
         if (f >= f_hi) break;
         const bool valid = lane < n;
-        const bool left = valid && left_bit(sg.bits, rows[r]);
+        const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
         const unsigned lm = __ballot_sync(FULL, left);
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (lane - rl);
@@ -119,7 +121,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
           if (r >= rounds) break;
           const uint32_t p = r * 32 + lane;
           const bool valid = p < n;
-          const bool left = valid && left_bit(sg.bits, rows[r]);
+          const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
           const unsigned lm = __ballot_sync(FULL, left);
           const uint32_t rl = run + __popc(lm & lt);
           const uint32_t dst = left ? rl : nl + (p - rl);
@@ -268,7 +270,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
 #pragma unroll
       for (uint32_t r = 0; r < ROUNDS; ++r) {
         const uint32_t q = wlo + r * 32 + lane;
-        const bool left = q < cnt && left_bit(sg.bits, (uint32_t)rows[q < cnt ? q : 0]);
+        const bool left = q < cnt && left_bit(sg.bits, (uint32_t)rows[q < cnt ? q : 0] & w.row_mask);
         lmask[r] = __ballot_sync(FULL, left);
         wc += __popc(lmask[r]);
       }

@@ -183,7 +183,9 @@ int ct_partition_nodes(const ct_problem* p, const ct_lists* lists, const ct_node
 /* -------------------------------------------------------- forest fit --- */
 /* Grows trees first_tree .. first_tree+n_trees-1 into slots 0..n_trees-1 of
  * `trees` (replaces RandomForestClassifier.fit's tree loop + RandomClassifierTree.fit,
- * random_forest.py:292-336, random_tree.py:461-676).  Lists must hold n_trees slots. */
+ * random_forest.py:292-336, random_tree.py:461-676).  Lists must hold n_trees slots
+ * (one for CT_FIT_PLAIN); they are the fit's scratch, and while it runs their
+ * entries may carry each row's label above its row id. */
 int ct_fit_workspace_size(const ct_problem* p, uint32_t n_trees, const ct_fit_options* opt,
                           size_t* bytes);
 int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint32_t n_trees,

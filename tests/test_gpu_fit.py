@@ -49,6 +49,22 @@ def test_fit_matches_oracle(cuda_device, name, bootstrap, mode):
     np.testing.assert_array_equal(forest.predict_proba(x), O.predict_proba(ref, x))
 
 
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+@pytest.mark.parametrize("n,f,c", [(4096, 8, 16), (4097, 8, 16), (66000, 6, 3), (2000, 5, 1)])
+def test_label_carrying_lists_match_oracle(cuda_device, n, f, c, mode):
+    """The fit's lists carry each row's label above its row id when both fit
+    one index entry.  4,096 rows (12 bits) and 16 classes (4 bits) fill a
+    16-bit entry; 4,097 rows need 13 bits, so those lists hold plain row ids;
+    66,000 rows take 32-bit entries (17 + 2 bits); one class needs no label
+    bits.  Every form grows the oracle's trees."""
+    x, y = _synthetic(n, f, max(c, 1), 11)
+    forest = RandomForestClassifier(n_estimators=2, bootstrap=True, seed=5, fit_mode=mode)
+    forest.fit(x, y, bfs_threshold=1000)
+    ref = O.fit_forest(x, y, n_estimators=2, bootstrap=True, seed=5)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
+
+
 def test_plain_equals_batched_large(cuda_device):
     x, y = _synthetic(70000, 12, 5, 9)  # uint32 indices
     a = RandomForestClassifier(n_estimators=4, seed=7, fit_mode="plain").fit(x, y)
