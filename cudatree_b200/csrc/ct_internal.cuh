@@ -164,6 +164,26 @@ __device__ __forceinline__ bool left_bit(const uint32_t* bits, uint32_t row) {
 }
 void launch_pack_marks(const uint8_t* mark, uint32_t* bits, uint32_t n_rows, uint32_t n_slots, cudaStream_t st);
 
+// L2 cache policies.  The index lists stream through once per level (251 MB
+// at covtype size, twice L2), while x and the mark bits are gathered at
+// random: list traffic is marked evict-first so the gathered arrays keep
+// their lines.
+__device__ __forceinline__ uint64_t l2_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
+  float v;
+  asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
 template <typename IdxT>
 __device__ __forceinline__ IdxT* list_ptr(const View& v, uint32_t buf, uint32_t slot, uint32_t f) {
   IdxT* base = reinterpret_cast<IdxT*>(buf ? v.si1 : v.si0);

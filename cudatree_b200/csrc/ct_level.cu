@@ -142,7 +142,7 @@ k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t 
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t p = base + r * 32 + lane;
-      rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+      rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r)
@@ -222,20 +222,21 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   constexpr uint32_t B = 32 * SCAN_BATCH;
   uint32_t rows_n[SCAN_BATCH], cs[SCAN_BATCH];
   float xs[SCAN_BATCH];
+  const uint64_t keep = l2_evict_last();
   {
     uint32_t rows[SCAN_BATCH];
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t p = lo + r * 32 + lane;
-      rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+      rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
       const uint32_t q = p + B;
-      rows_n[r] = q < hi ? (uint32_t)lst[q] : 0u;
+      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const bool valid = lo + r * 32 + lane < hi;
       cs[r] = valid ? entry_label<LabT>(v, rows[r]) : NONE;
-      xs[r] = valid ? xf[entry_row(v, rows[r])] : 0.f;
+      xs[r] = valid ? ld_keep(xf + entry_row(v, rows[r]), keep) : 0.f;
     }
   }
   for (uint32_t base = lo; base < hi; base += B) {
@@ -245,12 +246,12 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const bool valid = base + B + r * 32 + lane < hi;
       cs_n[r] = valid ? entry_label<LabT>(v, rows_n[r]) : NONE;
-      xs_n[r] = valid ? xf[entry_row(v, rows_n[r])] : 0.f;
+      xs_n[r] = valid ? ld_keep(xf + entry_row(v, rows_n[r]), keep) : 0.f;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t q = base + 2 * B + r * 32 + lane;
-      rows_n[r] = q < hi ? (uint32_t)lst[q] : 0u;
+      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
     }
     const float x_e = __shfl_sync(FULL, xs_n[0], 0);  // first value of the next batch
 #pragma unroll
@@ -500,7 +501,7 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
 #pragma unroll
   for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
     const uint32_t p = lo + r * 32 + lane;
-    rows[r] = p < hi ? (uint32_t)lst[p] : 0u;
+    rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
   }
 #pragma unroll
   for (uint32_t r = 0; r < PART_ROUNDS; ++r) {

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < R; ++r) {
         const uint32_t f = f_lo + r * per + sub;
         valid[r] = f < f_hi && p < n;
-        rows[r] = valid[r] ? (uint32_t)in[(size_t)f * sg.in_fstride + p] : 0u;
+        rows[r] = valid[r] ? (uint32_t)__ldcs(in + (size_t)f * sg.in_fstride + p) : 0u;
       }
 #pragma unroll
       for (uint32_t r = 0; r < R; ++r) {
@@ -84,14 +84,14 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (p - rl);
         if (valid[r] && (left || sg.keep_right) && dst < n)
-          out[(size_t)f * sg.out_fstride + dst] = (IdxT)rows[r];
+          __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
       }
     } else if (n <= 32) {
       uint32_t rows[FEAT_BLOCK];
 #pragma unroll
       for (uint32_t r = 0; r < FEAT_BLOCK; ++r) {
         const uint32_t f = f_lo + r;
-        rows[r] = (f < f_hi && lane < n) ? (uint32_t)in[(size_t)f * sg.in_fstride + lane] : 0u;
+        rows[r] = (f < f_hi && lane < n) ? (uint32_t)__ldcs(in + (size_t)f * sg.in_fstride + lane) : 0u;
       }
 #pragma unroll
       for (uint32_t r = 0; r < FEAT_BLOCK; ++r) {
@@ -102,7 +102,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const unsigned lm = __ballot_sync(FULL, left);
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (lane - rl);
-        if (valid && (left || sg.keep_right) && dst < n) out[(size_t)f * sg.out_fstride + dst] = (IdxT)rows[r];
+        if (valid && (left || sg.keep_right) && dst < n) __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
       }
     } else {
       const uint32_t rounds = ceil_div(n, 32);
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
 #pragma unroll
         for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
           const uint32_t p = r * 32 + lane;
-          rows[r] = (r < rounds && p < n) ? (uint32_t)fin[p] : 0u;
+          rows[r] = (r < rounds && p < n) ? (uint32_t)__ldcs(fin + p) : 0u;
         }
         uint32_t run = 0;
 #pragma unroll
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
           const unsigned lm = __ballot_sync(FULL, left);
           const uint32_t rl = run + __popc(lm & lt);
           const uint32_t dst = left ? rl : nl + (p - rl);
-          if (valid && (left || sg.keep_right) && dst < n) fout[dst] = (IdxT)rows[r];
+          if (valid && (left || sg.keep_right) && dst < n) __stcs(fout + dst, (IdxT)rows[r]);
           run += __popc(lm);
         }
       }
@@ -156,12 +156,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
       : "memory");
   return done != 0;
 }
-// Global -> shared bulk copy; src 16-byte aligned, bytes a multiple of 16.
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// Global -> shared bulk copy; src 16-byte aligned, bytes a multiple of 16;
+// pol is the L2 policy of the source lines.
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar, uint64_t pol) {
   asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
           smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(pol)
       : "memory");
 }
 
@@ -175,7 +176,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 
 template <typename IdxT, uint32_t TILE>
 __device__ __forceinline__ void issue_tile(const IdxT* seg_in, uint32_t n, uint32_t j, unsigned char* buf,
-                                           uint64_t* bar, uint32_t* off_out) {
+                                           uint64_t* bar, uint32_t* off_out, uint64_t pol) {
   const uint32_t lo = j * TILE;
   const uint32_t cnt = min(TILE, n - lo);
   const uintptr_t a = reinterpret_cast<uintptr_t>(seg_in + lo);
@@ -183,7 +184,7 @@ __device__ __forceinline__ void issue_tile(const IdxT* seg_in, uint32_t n, uint3
   const uintptr_t e1 = (a + (uintptr_t)cnt * sizeof(IdxT) + 15) & ~uintptr_t(15);
   *off_out = (uint32_t)((a - a0) / sizeof(IdxT));
   mbar_expect_tx(bar, (uint32_t)(e1 - a0));
-  bulk_g2s(buf, reinterpret_cast<const void*>(a0), (uint32_t)(e1 - a0), bar);
+  bulk_g2s(buf, reinterpret_cast<const void*>(a0), (uint32_t)(e1 - a0), bar, pol);
 }
 
 template <typename IdxT, uint32_t ROUNDS>
@@ -205,6 +206,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   const unsigned lt = lanemask_lt();
   const uint32_t nbig = live(w, w.n_big, w.cap_big);
   const uint64_t chains = (uint64_t)nbig * w.n_features;
+  const uint64_t stream_pol = l2_evict_first();  // list tiles are read once
   if (threadIdx.x == 0) {
     for (uint32_t i = 0; i < RING; ++i) mbar_init(&bars[i], 1);
     mbar_fence_init();
@@ -230,13 +232,14 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
     const uint32_t ntiles = ceil_div(n, TILE);
     if (threadIdx.x == 0)
       for (uint32_t j = 0; j < RING - 1 && j < ntiles; ++j)
-        issue_tile<IdxT, TILE>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING]);
+        issue_tile<IdxT, TILE>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING],
+                               stream_pol);
     uint32_t carry = 0;
     for (uint32_t j = 0; j < ntiles; ++j, ++g) {
       const uint32_t b = g % RING;
       if (threadIdx.x == 0 && j + RING - 1 < ntiles) {  // refill the buffer freed by tile j-1
         const uint32_t bn = (g + RING - 1) % RING;
-        issue_tile<IdxT, TILE>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn]);
+        issue_tile<IdxT, TILE>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn], stream_pol);
       }
       bool ok = true;
       {
@@ -292,7 +295,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
         if (q < cnt && (left || sg.keep_right)) {
           const uint32_t p = lo + q;
           const uint32_t dst = left ? rl : sg.nl + (p - rl);
-          if (dst < n) out[dst] = rows[q];
+          if (dst < n) __stcs(out + dst, rows[q]);
         }
         run += __popc(lmask[r]);
       }
