@@ -12,7 +12,7 @@
 //   k_split_reduce min-impurity reduction + threshold
 //                  (reference reduce_2d / find_min_imp / get_thresholds)
 //   k_plan         node record, child ids, partition work list
-//   k_fill_mark    mark table + left class totals (reference fill_table)
+//   k_fill_mark    mark bits + left class totals (reference fill_table)
 //   (partition)    stable partition of every feature's node range: plan and
 //                  mark table here, the kernels in ct_partition.cu
 //                  (reference scan_reshuffle, dfs_module.cu:224-307)
@@ -165,13 +165,16 @@ k_scan_carry(LevelScratch s, uint32_t C) {
   if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
   const ScanPiece pc = s.pieces[pi];
   if (pc.npieces <= 1 || pc.j != 0) return;
-  for (uint32_t c = lane; c < C; c += 32) {
+  // per class, an exclusive prefix over the segment's pieces, 32 pieces per round
+  for (uint32_t c = 0; c < C; ++c) {
     uint32_t run = 0;
-    for (uint32_t j = 0; j < pc.npieces; ++j) {
+    for (uint32_t j0 = 0; j0 < pc.npieces; j0 += 32) {
+      const uint32_t j = j0 + lane;
       uint32_t* h = s.carry + (size_t)(pc.carry + j) * C + c;
       const uint32_t t = (j + 1 < pc.npieces) ? *h : 0u;
-      *h = run;
-      run += t;
+      const uint32_t incl = (uint32_t)warp_incl_scan_i32((int32_t)t);
+      if (j < pc.npieces) *h = run + incl - t;
+      run += __shfl_sync(FULL, incl, 31);
     }
   }
 }
@@ -491,12 +494,14 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
   const SplitRec sr = s.splits[pp.split];
   const ct_node nd = nodes[sr.node];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, sr.feature) + nd.start;
-  uint8_t* mk = v.mark + (size_t)nd.slot * v.n_rows;
+  uint32_t* bw = v.bits + (size_t)nd.slot * v.bit_words;
   for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
   __syncwarp();
   const uint32_t lo = pp.j * PART_PIECE;
   const uint32_t hi = min(lo + PART_PIECE, nd.n);
-  // all the piece's index loads first, then the mark writes and label gathers
+  // all the piece's index loads first, then the mark bits: every row of a
+  // split node is set (left) or cleared (right) once per step, by an atomic
+  // on its 32-row word, so no byte table is packed afterwards
   uint32_t rows[PART_ROUNDS], cls[PART_ROUNDS];
 #pragma unroll
   for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
@@ -509,7 +514,9 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
     cls[r] = NONE;
     if (p < hi) {
       const bool left = p <= sr.pos;
-      mk[entry_row(v, rows[r])] = left ? 1 : 0;
+      const uint32_t row = entry_row(v, rows[r]);
+      if (left) atomicOr(bw + (row >> 5), 1u << (row & 31));
+      else atomicAnd(bw + (row >> 5), ~(1u << (row & 31)));
       if (left) cls[r] = entry_label<LabT>(v, rows[r]);
     }
   }
@@ -1157,8 +1164,6 @@ void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s_a
   k_plan<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, tv);
   k_fill_mark<IdxT, LabT><<<blocks_for_warps(caps.part), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s);
   pf->launched(CT_K_MARK, 2);
-  launch_pack_marks(v.mark, v.bits, v.n_rows, v.n_slots, st);
-  pf->launched(CT_K_MARK);
   pf->end();
   pf->begin(CT_K_PARTITION);
   const PartWork w = level_part_work(v, s);

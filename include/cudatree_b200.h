@@ -61,8 +61,10 @@ typedef struct ct_problem {
  * sorted_indices_gpu_, random_tree.py:466-467).  Slot s, buffer b, feature f
  * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark
  * holds the [n_slots][n_rows] byte mark table (reference mark_table,
- * random_forest.py:168) followed, at the next 256-byte boundary, by its
- * packed [n_slots][bit_words] uint32 copy; ct_mark_bytes gives the size. */
+ * random_forest.py:168; the bootstrap's in-bag marks) followed, at the next
+ * 256-byte boundary, by the packed [n_slots][bit_words] uint32 left flags
+ * that the partition reads (a split's mark fill sets and clears them
+ * directly); ct_mark_bytes gives the size. */
 /* The partition and compaction kernels copy index tiles with 16-byte TMA
  * bulk copies and may read up to 15 bytes past the last element of the
  * si0/si1 buffers and of the presort: allocate them with >= 16 bytes of
