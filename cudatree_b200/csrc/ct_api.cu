@@ -105,7 +105,7 @@ int ct_bootstrap_compact(const ct_problem* p, const ct_lists* lists, uint32_t sl
       CT_CUDA_TRY(cudaMemcpyAsync(words, workspace, sizeof(words), cudaMemcpyDeviceToHost, st));
       CT_CUDA_TRY(cudaStreamSynchronize(st));
       if (words[1]) {
-        set_last_error("bootstrap compaction: a bounded wait for a tile copy gave up");
+        set_last_error("bootstrap compaction flagged a device error");
         return CT_ERR_TIMEOUT;
       }
     }

@@ -194,7 +194,7 @@ int check_boot_error(const FitLayout& L, cudaStream_t st) {
   CT_CUDA_TRY(cudaMemcpyAsync(w, L.boot_ws, sizeof(w), cudaMemcpyDeviceToHost, st));
   CT_CUDA_TRY(cudaStreamSynchronize(st));
   if (w[1]) {
-    set_last_error("bootstrap compaction look-back wait gave up");
+    set_last_error("bootstrap compaction flagged a device error");
     return CT_ERR_TIMEOUT;
   }
   return CT_OK;

@@ -181,7 +181,7 @@ k_scan_carry(LevelScratch s, uint32_t C) {
 
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
 k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
              LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
