@@ -285,28 +285,44 @@ class RandomForestClassifier:
         n, f = self.n_samples, self.n_features
         return 2 * f * n * self.index_bytes + n + 2 * n * 20
 
-    def trees_in_flight(self, mode: str) -> int:
+    def trees_in_flight(self, mode: str, query_free: bool = False) -> int:
+        """Trees grown by one batched call: all of them when their lists and
+        workspace take at most half of the device, else as many as fit in 70 %
+        of the free memory.  The free-memory query is skipped when the forest
+        is small against the device: it took 1-77 ms per call on B200."""
         if mode == "plain":
             return 1
         prob = self._problem()
         opts = self._fit_options(_lib.CT_FIT_BATCHED, 0)
-        free, _ = torch.cuda.mem_get_info()
-        budget = int(free * 0.7)
-        k = self.n_estimators
-        while k > 1:
+
+        def need(k):
             ws = C.c_size_t()
             _lib.call("ct_fit_workspace_size", C.byref(prob), k, C.byref(opts), C.byref(ws))
-            if k * self._slot_bytes() + ws.value <= budget:
-                break
+            return k * self._slot_bytes() + ws.value
+
+        k = self.n_estimators
+        total = torch.cuda.get_device_properties(_device()).total_memory
+        if not query_free and need(k) <= total // 2:
+            return k
+        free, _ = torch.cuda.mem_get_info()
+        budget = int(free * 0.7)
+        while k > 1 and need(k) > budget:
             k = max(1, k // 2)
         return k
 
     def _fit_trees(self, first: int, count: int, mode: str, bfs_threshold: int):
+        try:
+            return self._fit_trees_k(first, count, mode, bfs_threshold, self.trees_in_flight(mode))
+        except torch.OutOfMemoryError:  # another tenant holds memory: size the batch from the free memory
+            torch.cuda.empty_cache()
+            return self._fit_trees_k(first, count, mode, bfs_threshold, self.trees_in_flight(mode, query_free=True))
+
+    def _fit_trees_k(self, first: int, count: int, mode: str, bfs_threshold: int, in_flight: int):
         dev = _device()
         prob = self._problem()
         n, f = self.n_samples, self.n_features
         mode_id = _lib.CT_FIT_PLAIN if mode == "plain" else _lib.CT_FIT_BATCHED
-        k = min(self.trees_in_flight(mode), count)
+        k = min(in_flight, count)
         slots = 1 if mode == "plain" else k
         per_call = 1 if mode == "plain" else k
         si0 = _dev_bytes(slots * f * n * self.index_bytes, dev)

@@ -65,6 +65,16 @@ def test_label_carrying_lists_match_oracle(cuda_device, n, f, c, mode):
     np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
 
 
+def test_bootstrap_of_more_than_128_trees_matches_oracle(cuda_device):
+    """The bootstrap compacts at most 128 trees per pass over the presort:
+    140 trees in flight take two passes, and every tree is the oracle's."""
+    x, y = _synthetic(600, 5, 3, 13)
+    forest = RandomForestClassifier(n_estimators=140, bootstrap=True, seed=21, fit_mode="batched")
+    forest.fit(x, y)
+    ref = O.fit_forest(x, y, n_estimators=140, bootstrap=True, seed=21)
+    _assert_same_trees(forest._trees, ref.trees)
+
+
 def test_plain_equals_batched_large(cuda_device):
     x, y = _synthetic(70000, 12, 5, 9)  # uint32 indices
     a = RandomForestClassifier(n_estimators=4, seed=7, fit_mode="plain").fit(x, y)
