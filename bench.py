@@ -34,7 +34,7 @@ WORKLOAD = ("covtype-shaped synthetic 581012x54 f32 (10 Gaussian + 44 one-hot), 
             "100 trees, bootstrap, max_features=7, uint32 indices, fully grown")
 N_TREES = 100
 MAX_FEATURES = 7
-PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.86
+PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.85
 
 
 def peaks():
@@ -531,7 +531,7 @@ def run_ours(args, world, rank, local):
         "roofline": {"bound": "hbm", "kernel": "k_partition", "achieved": round(p_gbs, 1) if p_gbs else None,
                      "peak": peak, "unit": "GB/s", "frac": round(p_gbs / peak, 4) if p_gbs else None,
                      "peak_kind": peak_kind, "traffic": round(traffic) if traffic else None,
-                     "traffic_unit": "DRAM bytes per launch (ncu ratio 0.86 x algorithmic, 16-tree capture)",
+                     "traffic_unit": f"DRAM bytes per launch (ncu ratio {PARTITION_DRAM_PER_ALGORITHMIC_BYTE} x algorithmic, 16-tree capture)",
                      "algorithmic_bytes_per_launch": round(stats["bytes"][pi] / p_launches) if p_launches else None,
                      "algorithmic_bytes_per_element": "n_features x (2 x index_bytes + 1)"},
         "scan_roofline": {"kernel": "k_split_scan (+hist/carry)",
