@@ -99,7 +99,6 @@ struct PartSeg {
   uint32_t out_fstride;
   uint32_t n;
   uint32_t nl;            // number of left rows
-  uint32_t keep_right;    // 0: right rows are dropped (compaction)
   uint32_t status;        // first status slot (tiled segments)
 };
 struct PartTile {
@@ -162,7 +161,6 @@ __host__ __device__ __forceinline__ size_t mark_bits_offset(uint32_t n_rows, uin
 __device__ __forceinline__ bool left_bit(const uint32_t* bits, uint32_t row) {
   return (__ldg(bits + (row >> 5)) >> (row & 31)) & 1u;
 }
-void launch_pack_marks(const uint8_t* mark, uint32_t* bits, uint32_t n_rows, uint32_t n_slots, cudaStream_t st);
 
 // L2 cache policies.  The index lists stream through once per level (251 MB
 // at covtype size, twice L2), while x and the mark bits are gathered at

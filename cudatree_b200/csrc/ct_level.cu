@@ -450,7 +450,6 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       sg.out_fstride = v.stride;
       sg.n = nd.n;
       sg.nl = r.pos + 1;
-      sg.keep_right = 1;
       sg.status = tbase;
       (big ? s.big_segs : s.small_segs)[gidx] = sg;
     }

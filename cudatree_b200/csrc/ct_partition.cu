@@ -1,7 +1,6 @@
-// Stable partition of index-list segments by a per-row mark byte, for every
+// Stable partition of index-list segments by a per-row mark bit, for every
 // feature (reference scan_reshuffle, dfs_module.cu:224-307 and
-// bfs_module.cu:266-377; and, with the right part dropped, the bootstrap
-// compaction of bootstrap_reshuffle.cu:9-59).
+// bfs_module.cu:266-377).
 //
 // A segment is one node's range [0, n) in every feature list.  Left rows
 // (mark != 0) keep their order at [0, nl), right rows keep theirs at
@@ -83,7 +82,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const unsigned lm = __ballot_sync(FULL, left) & gmask;
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (p - rl);
-        if (valid[r] && (left || sg.keep_right) && dst < n)
+        if (valid[r] && dst < n)
           __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
       }
     } else if (n <= 32) {
@@ -102,7 +101,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         const unsigned lm = __ballot_sync(FULL, left);
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (lane - rl);
-        if (valid && (left || sg.keep_right) && dst < n) __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
+        if (valid && dst < n) __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
       }
     } else {
       const uint32_t rounds = ceil_div(n, 32);
@@ -125,7 +124,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
           const unsigned lm = __ballot_sync(FULL, left);
           const uint32_t rl = run + __popc(lm & lt);
           const uint32_t dst = left ? rl : nl + (p - rl);
-          if (valid && (left || sg.keep_right) && dst < n) __stcs(fout + dst, (IdxT)rows[r]);
+          if (valid && dst < n) __stcs(fout + dst, (IdxT)rows[r]);
           run += __popc(lm);
         }
       }
@@ -292,7 +291,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
         const uint32_t q = wlo + r * 32 + lane;
         const bool left = (lmask[r] >> lane) & 1u;
         const uint32_t rl = run + __popc(lmask[r] & lt);
-        if (q < cnt && (left || sg.keep_right)) {
+        if (q < cnt) {
           const uint32_t p = lo + q;
           const uint32_t dst = left ? rl : sg.nl + (p - rl);
           if (dst < n) __stcs(out + dst, rows[q]);
@@ -302,29 +301,6 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
       carry += total;
       __syncthreads();  // tile buffer and s_wcnt free for reuse
     }
-  }
-}
-
-__global__ void k_pack_marks(const uint8_t* __restrict__ mark, uint32_t* __restrict__ bits, uint32_t n_rows,
-                             uint32_t words, uint32_t n_slots) {
-  const uint64_t total = (uint64_t)words * n_slots;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint32_t slot = (uint32_t)(i / words), wd = (uint32_t)(i - (uint64_t)slot * words);
-    const uint8_t* m = mark + (size_t)slot * n_rows + (size_t)wd * 32;
-    const uint32_t lim = wd * 32 < n_rows ? min(32u, n_rows - wd * 32) : 0u;
-    uint32_t v = 0;
-    if (lim == 32 && (reinterpret_cast<uintptr_t>(m) & 3u) == 0) {
-      // eight aligned words, four mark bytes (each 0 or 1) per word
-#pragma unroll
-      for (uint32_t k = 0; k < 8; ++k) {
-        const uint32_t q = __ldg(reinterpret_cast<const uint32_t*>(m) + k);
-        const uint32_t b4 = (q & 1u) | ((q >> 7) & 2u) | ((q >> 14) & 4u) | ((q >> 21) & 8u);
-        v |= b4 << (4 * k);
-      }
-    } else {
-      for (uint32_t k = 0; k < lim; ++k) v |= (m[k] ? 1u : 0u) << k;
-    }
-    bits[i] = v;
   }
 }
 
@@ -367,13 +343,6 @@ int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
 }
 
 }  // namespace
-
-void launch_pack_marks(const uint8_t* mark, uint32_t* bits, uint32_t n_rows, uint32_t n_slots, cudaStream_t st) {
-  const uint32_t words = mark_bit_words(n_rows);
-  const uint64_t total = (uint64_t)words * n_slots;
-  const uint32_t blocks = (uint32_t)std::min<uint64_t>((total + 255) / 256, 148u * 16u);
-  k_pack_marks<<<blocks, 256, 0, st>>>(mark, bits, n_rows, words, n_slots);
-}
 
 int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
                          cudaStream_t st) {
