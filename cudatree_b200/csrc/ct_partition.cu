@@ -191,6 +191,55 @@ constexpr uint32_t ring_buf_bytes() {
   return BIG_WARPS * 32 * ROUNDS * sizeof(IdxT) + 128;
 }
 
+// One tile of a chain: the left flags of the CTA's BIG_WARPS * 32 * ROUNDS
+// positions, the CTA's prefix of left counts, and the stable stores; returns
+// the tile's left count.  WHOLE: the tile is full, so no position is guarded.
+template <typename IdxT, uint32_t ROUNDS, bool WHOLE>
+__device__ __forceinline__ uint32_t part_tile(const IdxT* rows, uint32_t cnt, uint32_t lo, const PartSeg& sg,
+                                              uint32_t row_mask, IdxT* out, uint32_t n, uint32_t carry,
+                                              uint32_t* s_wcnt) {
+  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+  const unsigned lt = lanemask_lt();
+  const uint32_t wlo = warp * (32 * ROUNDS);
+  unsigned lmask[ROUNDS];
+  IdxT e[ROUNDS];
+  uint32_t wc = 0;
+#pragma unroll
+  for (uint32_t r = 0; r < ROUNDS; ++r) {
+    const uint32_t q = wlo + r * 32 + lane;
+    const bool in = WHOLE || q < cnt;
+    e[r] = rows[in ? q : 0];
+    const bool left = in && left_bit(sg.bits, (uint32_t)e[r] & row_mask);
+    lmask[r] = __ballot_sync(FULL, left);
+    wc += __popc(lmask[r]);
+  }
+  if (lane == 0) s_wcnt[warp] = wc;
+  __syncthreads();
+  // the warps' left counts: lane k of every warp holds warp k's, scanned over 8 lanes
+  static_assert(BIG_WARPS == 8, "the count prefix scans 8 lanes");
+  uint32_t v = s_wcnt[lane & 7u];
+#pragma unroll
+  for (uint32_t d = 1; d < 8; d <<= 1) {
+    const uint32_t o = __shfl_up_sync(FULL, v, d, 8);
+    if ((lane & 7u) >= d) v += o;
+  }
+  const uint32_t total = __shfl_sync(FULL, v, 7);
+  const uint32_t woff = warp ? __shfl_sync(FULL, v, warp - 1) : 0u;
+  uint32_t run = carry + woff;
+#pragma unroll
+  for (uint32_t r = 0; r < ROUNDS; ++r) {
+    const uint32_t q = wlo + r * 32 + lane;
+    const bool left = (lmask[r] >> lane) & 1u;
+    const uint32_t rl = run + __popc(lmask[r] & lt);
+    if (WHOLE || q < cnt) {
+      const uint32_t dst = left ? rl : sg.nl + (lo + q - rl);
+      if (dst < n) __stcs(out + dst, e[r]);
+    }
+    run += __popc(lmask[r]);
+  }
+  return total;
+}
+
 template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
 __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   constexpr uint32_t TILE = BIG_WARPS * 32 * ROUNDS;
@@ -201,8 +250,6 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   __shared__ uint32_t s_off[RING];
   __shared__ uint32_t s_chain;
   __shared__ uint32_t s_wcnt[BIG_WARPS];
-  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
-  const unsigned lt = lanemask_lt();
   const uint32_t nbig = live(w, w.n_big, w.cap_big);
   const uint64_t chains = (uint64_t)nbig * w.n_features;
   const uint64_t stream_pol = l2_evict_first();  // list tiles are read once
@@ -266,39 +313,8 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
       const uint32_t lo = j * TILE;
       const uint32_t cnt = min(TILE, n - lo);
       const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
-      const uint32_t wlo = warp * (32 * ROUNDS);
-      unsigned lmask[ROUNDS];
-      uint32_t wc = 0;
-#pragma unroll
-      for (uint32_t r = 0; r < ROUNDS; ++r) {
-        const uint32_t q = wlo + r * 32 + lane;
-        const bool left = q < cnt && left_bit(sg.bits, (uint32_t)rows[q < cnt ? q : 0] & w.row_mask);
-        lmask[r] = __ballot_sync(FULL, left);
-        wc += __popc(lmask[r]);
-      }
-      if (lane == 0) s_wcnt[warp] = wc;
-      __syncthreads();
-      uint32_t woff = 0, total = 0;
-#pragma unroll
-      for (uint32_t k = 0; k < (uint32_t)BIG_WARPS; ++k) {
-        const uint32_t v = s_wcnt[k];
-        woff += k < warp ? v : 0u;
-        total += v;
-      }
-      uint32_t run = carry + woff;
-#pragma unroll
-      for (uint32_t r = 0; r < ROUNDS; ++r) {
-        const uint32_t q = wlo + r * 32 + lane;
-        const bool left = (lmask[r] >> lane) & 1u;
-        const uint32_t rl = run + __popc(lmask[r] & lt);
-        if (q < cnt) {
-          const uint32_t p = lo + q;
-          const uint32_t dst = left ? rl : sg.nl + (p - rl);
-          if (dst < n) __stcs(out + dst, rows[q]);
-        }
-        run += __popc(lmask[r]);
-      }
-      carry += total;
+      carry += cnt == TILE ? part_tile<IdxT, ROUNDS, true>(rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt)
+                           : part_tile<IdxT, ROUNDS, false>(rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt);
       __syncthreads();  // tile buffer and s_wcnt free for reuse
     }
   }
