@@ -54,8 +54,9 @@ __global__ void k_root_hist(View v, const uint32_t* n_in, uint32_t slot_lo, uint
 template <typename IdxT, typename LabT>
 __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t seed, uint32_t tree_lo,
                        TreeView tv, const uint32_t* hist_in, ct_node* out, uint32_t* out_tot, uint32_t cap,
-                       Counters* ctr) {
+                       Counters* ctr, uint64_t* out_mask) {
   __shared__ uint32_t s_idx;
+  __shared__ unsigned long long s_mask;
   const uint32_t slot = slot_lo + blockIdx.x;
   const uint32_t C = v.n_classes;
   const uint32_t n = n_in[slot];
@@ -94,6 +95,18 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
   if (s_idx != NONE)
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x)
       out_tot[(size_t)s_idx * C + c] = hist_in[(size_t)blockIdx.x * C + c];
+  if (out_mask && s_idx != NONE) {  // features constant over the tree's in-bag rows (feature 0 excepted)
+    if (threadIdx.x == 0) s_mask = 0;
+    __syncthreads();
+    const uint32_t f = threadIdx.x;
+    if (f > 0 && f < v.n_features && f < 64) {
+      const IdxT* lf = list_ptr<IdxT>(v, 0, slot, f);
+      const float* xf = v.x_fm + (size_t)f * v.n_rows;
+      if (xf[entry_row(v, lf[0])] == xf[entry_row(v, lf[n - 1])]) atomicOr(&s_mask, 1ull << f);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) out_mask[s_idx] = s_mask;
+  }
 }
 
 __global__ void k_begin_level(Counters* c) {
@@ -102,6 +115,7 @@ __global__ void k_begin_level(Counters* c) {
   c->small_total = 0;
   c->split_total = 0;
   c->scan_elems = 0;
+  c->part_elems = 0;
 }
 
 void begin_level(Counters* c, cudaStream_t st) {
@@ -116,7 +130,7 @@ void account_level(const ct_problem* p, const View& view, const Counters& h) {
   const double w = p->index_bytes, l = view.lab_shift ? 0.0 : p->label_bytes, v = sizeof(float);
   pf->stats.bytes[CT_K_SCAN] += (double)h.scan_elems * (w + l + v);
   pf->stats.bytes[CT_K_MARK] += (double)h.split_total * (w + 1.0);
-  pf->stats.bytes[CT_K_PARTITION] += (double)h.split_total * p->n_features * (2.0 * w + 1.0);
+  pf->stats.bytes[CT_K_PARTITION] += (double)h.part_elems * (2.0 * w + 1.0);  // chains actually partitioned
   pf->stats.steps += 1;
 }
 
@@ -132,6 +146,7 @@ struct FitLayout {
   uint32_t* n_in;
   ct_node* list[2];
   uint32_t* tot[2];
+  uint64_t* mask[2];     // constant-feature masks of the lists (batched form, n_features <= 64), else NULL
   LevelScratch s;
   void* boot_ws;
   size_t boot_bytes;
@@ -155,9 +170,12 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
   L->small_bound = 0;
   L->n_in = a.take<uint32_t>(slots);
+  // the plain form moves nodes through the host, so only the batched form keeps masks
+  const bool masks = o->mode == CT_FIT_BATCHED && p->n_features <= 64;
   for (int i = 0; i < 2; ++i) {
     L->list[i] = a.take<ct_node>(L->cap_list);
     L->tot[i] = a.take<uint32_t>((size_t)L->cap_list * p->n_classes);
+    L->mask[i] = masks ? a.take<uint64_t>(L->cap_list) : nullptr;
   }
   L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, slots);
   L->boot_ws = a.take<char>(L->boot_bytes);
@@ -218,7 +236,7 @@ int launch_root(const View& v, const FitLayout& L, uint32_t slot_lo, uint32_t n_
   const uint32_t blocks = std::min<uint32_t>(ceil_div(v.n_rows, 256 * 8), 256);
   k_root_hist<IdxT, LabT><<<dim3(blocks, n_slots), 256, C * sizeof(uint32_t), st>>>(v, L.n_in, slot_lo, hist);
   k_root<IdxT, LabT><<<n_slots, 128, 0, st>>>(v, L.n_in, slot_lo, seed, tree_lo, tv, hist, L.list[cur],
-                                                L.tot[cur], L.cap_list, L.s.ctr);
+                                                L.tot[cur], L.cap_list, L.s.ctr, L.mask[cur]);
   current_prof()->launched(CT_K_CHILDREN, 2);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
@@ -257,11 +275,14 @@ int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView&
     const ct_node* nodes = L.list[cur] + lo;
     const uint32_t* tot = L.tot[cur] + (size_t)lo * C;
     const LevelBounds b{cn, total};
+    LevelScratch s = L.s;
+    s.node_mask = L.mask[cur] ? L.mask[cur] + lo : nullptr;
+    s.next_mask = L.mask[1 - cur];
     if (L.subtree_cut && L.small_bound + 2ull * cn > L.cap_small) CT_TRY(flush_subtrees(p, v, L, tv, st));
     CT_TRY(launch_reset_step(L.s.ctr, cn, st));
-    CT_TRY(launch_split(v, ib, lb, nodes, tot, L.s, b, L.scan_piece, st));
-    CT_TRY(launch_partition(v, ib, lb, nodes, L.s, b, tv, st));
-    CT_TRY(launch_children(v, ib, lb, nodes, tot, L.s, b, tv, L.list[1 - cur], L.tot[1 - cur], L.cap_list,
+    CT_TRY(launch_split(v, ib, lb, nodes, tot, s, b, L.scan_piece, st));
+    CT_TRY(launch_partition(v, ib, lb, nodes, s, b, tv, st));
+    CT_TRY(launch_children(v, ib, lb, nodes, tot, s, b, tv, L.list[1 - cur], L.tot[1 - cur], L.cap_list,
                            L.subtree_cut, L.small, L.cap_small, st));
     if (L.subtree_cut) L.small_bound += 2ull * cn;
   }

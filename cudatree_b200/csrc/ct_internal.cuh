@@ -88,6 +88,7 @@ struct Counters {
   unsigned long long small_total;
   unsigned long long split_total;  // samples in nodes partitioned this level
   unsigned long long scan_elems;   // (node, feature) elements scanned this level
+  unsigned long long part_elems;   // (node, feature) elements partitioned this level
 };
 
 // One stable-partition segment: a node range in every feature list.
@@ -100,6 +101,7 @@ struct PartSeg {
   uint32_t n;
   uint32_t nl;            // number of left rows
   uint32_t status;        // first status slot (tiled segments)
+  uint64_t skip;          // features whose lists are left as they are (constant in the node)
 };
 struct PartTile {
   uint32_t seg;
@@ -229,7 +231,15 @@ struct LevelScratch {
   PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
+  // Constant-feature masks of a batched fit (n_features <= 64), else NULL:
+  // bit f of node_mask[i] says that feature f is constant in node i of the
+  // step, so its lists are not partitioned and k_select does not read them;
+  // k_children writes the next list's masks to next_mask.  Feature 0 is never
+  // in a mask (leaf labels and subtrees read its lists).
+  const uint64_t* node_mask = nullptr;
+  uint64_t* next_mask = nullptr;
 };
+__device__ __forceinline__ bool masked(uint64_t m, uint32_t f) { return f < 64 && ((m >> f) & 1u); }
 
 // Per-kernel-group launch counts and CUDA-event timing of one fit.
 struct Prof {

@@ -68,6 +68,7 @@ k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t sca
   if (w >= min(s.ctr->n_nodes, s.cap_nodes)) return;
   const ct_node nd = nodes[w];
   const uint32_t m = v.max_features;
+  const uint64_t cmask = s.node_mask ? s.node_mask[w] : 0ull;  // constant features (lists not current)
   uint32_t taken = 0;
   if (nd.n >= 2) {
     for (uint32_t i0 = 0; i0 < v.n_features && taken < m; i0 += 32) {
@@ -76,9 +77,11 @@ k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t sca
       uint32_t f = 0;
       if (i < v.n_features) {
         f = feature_perm(i, v.n_features, nd.key, v.feistel_h);
-        const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
-        const float* xf = v.x_fm + (size_t)f * v.n_rows;
-        usable = xf[entry_row(v, lst[0])] != xf[entry_row(v, lst[nd.n - 1])];
+        if (!masked(cmask, f)) {
+          const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+          const float* xf = v.x_fm + (size_t)f * v.n_rows;
+          usable = xf[entry_row(v, lst[0])] != xf[entry_row(v, lst[nd.n - 1])];
+        }
       }
       const unsigned mask = __ballot_sync(FULL, usable);
       const uint32_t rank = __popc(mask & lanemask_lt());
@@ -424,6 +427,8 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
     atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
+    const uint64_t skip = s.node_mask ? s.node_mask[w] : 0ull;
+    atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * (v.n_features - (uint32_t)__popcll(skip)));
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
     if (big) {
       gidx = atomicAdd(&s.ctr->n_big_segs, 1u);
@@ -451,6 +456,7 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       sg.n = nd.n;
       sg.nl = r.pos + 1;
       sg.status = tbase;
+      sg.skip = s.node_mask ? s.node_mask[w] : 0ull;
       (big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
@@ -595,6 +601,24 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
     for (uint32_t c = lane; c < C; c += 32) {
       const uint32_t left = s.split_left[(size_t)w * C + c];
       next_tot[(size_t)idx * C + c] = side ? tot[(size_t)sr.node * C + c] - left : left;
+    }
+    if (s.next_mask) {
+      // the child's constant features: the parent's, and those whose values
+      // agree at the child's first and last positions (the child's lists of
+      // the others were just partitioned)
+      const uint64_t pm = s.node_mask[sr.node];
+      uint64_t cm = pm;
+      for (uint32_t f0 = 0; f0 < v.n_features; f0 += 32) {
+        const uint32_t f = f0 + lane;
+        bool cst = false;
+        if (f > 0 && f < v.n_features && !masked(pm, f)) {
+          const IdxT* lst = list_ptr<IdxT>(v, ch.buf, ch.slot, f) + ch.start;
+          const float* xf = v.x_fm + (size_t)f * v.n_rows;
+          cst = xf[entry_row(v, lst[0])] == xf[entry_row(v, lst[ch.n - 1])];
+        }
+        cm |= (uint64_t)__ballot_sync(FULL, cst) << f0;
+      }
+      if (lane == 0) s.next_mask[idx] = cm;
     }
   }
 }

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
 #pragma unroll
       for (uint32_t r = 0; r < R; ++r) {
         const uint32_t f = f_lo + r * per + sub;
-        valid[r] = f < f_hi && p < n;
+        valid[r] = f < f_hi && p < n && !masked(sg.skip, f);
         rows[r] = valid[r] ? (uint32_t)__ldcs(in + (size_t)f * sg.in_fstride + p) : 0u;
       }
 #pragma unroll
@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < FEAT_BLOCK; ++r) {
         const uint32_t f = f_lo + r;
         if (f >= f_hi) break;
+        if (masked(sg.skip, f)) continue;
         const bool valid = lane < n;
         const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
         const unsigned lm = __ballot_sync(FULL, left);
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
     } else {
       const uint32_t rounds = ceil_div(n, 32);
       for (uint32_t f = f_lo; f < f_hi; ++f) {
+        if (masked(sg.skip, f)) continue;
         const IdxT* fin = in + (size_t)f * sg.in_fstride;
         IdxT* fout = out + (size_t)f * sg.out_fstride;
         uint32_t rows[PART_ROUNDS];
@@ -272,6 +274,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
     const uint32_t si = c / w.n_features;
     const uint32_t f = c - si * w.n_features;
     const PartSeg sg = w.big[si];
+    if (masked(sg.skip, f)) continue;  // constant in the node: its lists are never read again
     const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
     IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
     const uint32_t n = sg.n;
