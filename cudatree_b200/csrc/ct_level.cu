@@ -136,10 +136,32 @@ k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t 
   const ct_node nd = nodes[pc.node];
   const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
-  for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
-  __syncwarp();
   const uint32_t lo = pc.j * scan_piece;
   const uint32_t hi = min(lo + scan_piece, nd.n);
+  if (C <= 8 && scan_piece <= 32 * 255) {
+    // each lane counts its (at most 255) positions in 8-bit fields of one
+    // register, one field per class; one warp sum per class at the end
+    uint64_t pk = 0;
+    for (uint32_t base = lo; base < hi; base += 32 * SCAN_BATCH) {
+      uint32_t rows[SCAN_BATCH];
+#pragma unroll
+      for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
+        const uint32_t p = base + r * 32 + lane;
+        rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
+      }
+#pragma unroll
+      for (uint32_t r = 0; r < SCAN_BATCH; ++r)
+        if (base + r * 32 + lane < hi) pk += 1ull << (8 * entry_label<LabT>(v, rows[r]));
+    }
+    uint32_t* out = s.carry + (size_t)pc.carry * C;
+    for (uint32_t c = 0; c < C; ++c) {
+      const uint32_t t = warp_sum_u32((uint32_t)(pk >> (8 * c)) & 0xffu);
+      if (lane == 0) out[c] = t;
+    }
+    return;
+  }
+  for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
+  __syncwarp();
   for (uint32_t base = lo; base < hi; base += 32 * SCAN_BATCH) {
     uint32_t rows[SCAN_BATCH], cs[SCAN_BATCH];
 #pragma unroll
