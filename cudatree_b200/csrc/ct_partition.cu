@@ -195,7 +195,7 @@ constexpr uint32_t ring_buf_bytes() {
 
 // One tile of a chain: the left flags of the CTA's BIG_WARPS * 32 * ROUNDS
 // positions, the CTA's prefix of left counts, and the stable stores; returns
-// the tile's left count.  WHOLE: the tile is full, so no position is guarded.
+// the tile's left count.  WHOLE: the tile is full, so positions need no range check.
 template <typename IdxT, uint32_t ROUNDS, bool WHOLE>
 __device__ __forceinline__ uint32_t part_tile(const IdxT* rows, uint32_t cnt, uint32_t lo, const PartSeg& sg,
                                               uint32_t row_mask, IdxT* out, uint32_t n, uint32_t carry,
