@@ -33,6 +33,8 @@ def restore_forest(trees, dtype_labels, compt_table=None, n_features=None, param
     the restored forest keeps its label table and can predict."""
     f = RandomForestClassifier(len(trees), **(params or {}))
     f._trees = list(trees)
+    for t in f._trees:
+        t.forest = f
     f.dtype_labels = np.dtype(dtype_labels)
     if compt_table is not None:
         f.compt_table = np.asarray(compt_table)
