@@ -120,15 +120,17 @@ PROTOTYPES = {
                          C.POINTER(FitOptions), C.POINTER(TreeBuffers), P, C.c_size_t, P]),
     "ct_fit_stats": (C.c_int, [C.c_void_p]),
     "ct_tree_canonicalize": (C.c_int, [P, P, P, P, P, C.c_uint32, P, P, P, P, P]),
-    "ct_predict": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
+    "ct_predict": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
     "ct_autotune_workspace_size": (C.c_int, [P, C.c_uint32, C.c_uint32, P]),
     "ct_autotune": (C.c_int, [P, P, C.c_uint32, C.c_uint32, P, P, C.c_size_t, P, P, P]),
     "ct_transpose_rows": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P]),
     "ct_fetch_trees_scratch": (C.c_size_t, [C.c_uint64, C.c_uint32]),
     "ct_fetch_trees": (C.c_int, [P, C.c_uint32, P, P, C.c_size_t, P, P, P, P, P, P]),
+    "ct_check_forest": (C.c_int, [P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32]),
     "ct_compact_fits": (C.c_int, [C.c_uint32, C.c_uint32]),
     "ct_compact_forest": (C.c_int, [P, C.c_uint32, C.c_uint32, C.c_uint32, P, P]),
-    "ct_predict_compact": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),
+    "ct_predict_compact": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P,
+                                     P]),
     "ct_server_create": (C.c_int, [P, P]),
     "ct_server_destroy": (C.c_int, [P]),
     "ct_server_add_forest": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P]),

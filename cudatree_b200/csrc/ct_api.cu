@@ -29,9 +29,9 @@ size_t fetch_trees_scratch(uint64_t total_nodes, uint32_t n_trees);
 int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* counts, void* scratch,
                 size_t scratch_bytes, uint32_t* ol, uint32_t* orr, uint16_t* of, float* ot, uint32_t* ov,
                 cudaStream_t st);
-int predict(const void* nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees, const float* x,
-            uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
-            cudaStream_t st);
+int predict(const void* nodes, uint32_t n_nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees,
+            const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes,
+            uint32_t* pred, cudaStream_t st);
 uint32_t compact_feature_bits(uint32_t n_features);
 bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes);
 int compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features, uint32_t max_tree_nodes,
@@ -43,14 +43,6 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
 }  // namespace ct
 
 using namespace ct;
-
-#define CT_GUARD(body)                                   \
-  try {                                                  \
-    body                                                 \
-  } catch (const std::exception& e) {                    \
-    set_last_error(std::string("exception: ") + e.what()); \
-    return CT_ERR_INTERNAL;                              \
-  }
 
 extern "C" {
 
@@ -271,10 +263,10 @@ int ct_fetch_trees(const ct_tree_buffers* trees, uint32_t n_trees, const uint32_
                               out_threshold, out_value, (cudaStream_t)stream);)
 }
 
-int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,
-               uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
-               void* stream) {
-  CT_GUARD(return predict(nodes, 0, tree_offset, n_trees, x, n_rows, n_features, n_classes, votes, pred,
+int ct_predict(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset, uint32_t n_trees,
+               const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes,
+               uint32_t* pred, void* stream) {
+  CT_GUARD(return predict(nodes, n_nodes, 0, tree_offset, n_trees, x, n_rows, n_features, n_classes, votes, pred,
                           (cudaStream_t)stream);)
 }
 
@@ -287,11 +279,19 @@ int ct_compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_
   CT_GUARD(return compact_forest(nodes, n_nodes, n_features, max_tree_nodes, out, (cudaStream_t)stream);)
 }
 
-int ct_predict_compact(const ct_compact_node* nodes, const uint32_t* tree_offset, uint32_t n_trees, const float* x,
-                       uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
-                       void* stream) {
-  CT_GUARD(return predict(nodes, compact_feature_bits(n_features), tree_offset, n_trees, x, n_rows, n_features,
-                          n_classes, votes, pred, (cudaStream_t)stream);)
+int ct_check_forest(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset, uint32_t n_trees,
+                    uint32_t n_features, uint32_t n_classes) {
+  CT_ARG_CHECK(nodes && tree_offset, "check forest: NULL argument");
+  CT_ARG_CHECK(n_trees >= 1 && n_nodes >= n_trees, "check forest: empty forest");
+  CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "check forest: n_classes out of range");
+  CT_GUARD(return check_forest_host(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes);)
+}
+
+int ct_predict_compact(const ct_compact_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
+                       uint32_t n_trees, const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
+                       uint32_t* votes, uint32_t* pred, void* stream) {
+  CT_GUARD(return predict(nodes, n_nodes, compact_feature_bits(n_features), tree_offset, n_trees, x, n_rows,
+                          n_features, n_classes, votes, pred, (cudaStream_t)stream);)
 }
 
 }  // extern "C"

@@ -36,6 +36,21 @@ const std::string& last_error_text();  // this thread's last error
       return CT_ERR_ARG;                        \
     }                                           \
   } while (0)
+// Body of an extern "C" entry point: no C++ exception (std::bad_alloc from a
+// message string, std::system_error from a lock) crosses the C ABI; it
+// becomes CT_ERR_INTERNAL with the exception's text as the last error.
+#define CT_GUARD(...)                                              \
+  try {                                                            \
+    __VA_ARGS__                                                    \
+  } catch (const std::exception& e) {                              \
+    try {                                                          \
+      ::ct::set_last_error(std::string("exception: ") + e.what()); \
+    } catch (...) {                                                \
+    }                                                              \
+    return CT_ERR_INTERNAL;                                        \
+  } catch (...) {                                                  \
+    return CT_ERR_INTERNAL;                                        \
+  }
 
 // Device-side error bits (Counters::error).
 enum : uint32_t { DEV_ERR_TIMEOUT = 1u, DEV_ERR_CAPACITY = 2u, DEV_ERR_INTERNAL = 4u };
@@ -375,6 +390,11 @@ uint32_t predict_group_size(uint32_t n_trees, uint64_t n_nodes, size_t node_byte
 uint32_t compact_feature_bits(uint32_t n_features);
 bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes);
 void compact_host(const ct_packed_node* in, uint32_t n, uint32_t fbits, ct_compact_node* out);
+// CT_ERR_ARG unless every tree [off[t], off[t + 1] or n_nodes) is non-empty,
+// every inner node's children (left, left + 1; local indices) come after it
+// inside its tree, features are < n_features and leaf classes < n_classes.
+int check_forest_host(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* off, uint32_t n_trees,
+                      uint32_t n_features, uint32_t n_classes);
 int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
                   size_t smem, bool any_grouped, cudaStream_t st);
 int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st,

@@ -214,12 +214,84 @@ __global__ void k_vote_rows(const uint32_t* __restrict__ votes, uint32_t n_rows,
   if ((threadIdx.x & 31) == 0 && pred) pred[row] = c;
 }
 
+// A packed node whose child or feature does not fit the compact fields
+// becomes an inner node with child 0, which the forest check rejects.
 __global__ void k_compact(const ct_packed_node* __restrict__ in, uint32_t n, uint32_t fbits,
                           uint2* __restrict__ out) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const uint4 p = __ldg(reinterpret_cast<const uint4*>(in) + i);
-    out[i] = p.z ? make_uint2(p.x, (p.z << fbits) | p.y) : make_uint2(p.w, 0u);
+    const bool fits = (p.z >> (32 - fbits)) == 0u && (p.y >> fbits) == 0u;
+    out[i] = p.z ? make_uint2(p.x, fits ? (p.z << fbits) | p.y : 1u) : make_uint2(p.w, 0u);
   }
+}
+
+// Forest check before a walk (bits of *err): 1 tree offsets not strictly
+// increasing inside [0, n_nodes); 2 an inner node whose left child is not
+// after it or whose right child (left + 1) is past its tree; 4 a feature
+// index >= n_features; 8 a leaf class >= n_classes.  A forest that passes
+// walks every tree in at most its node count of steps (the local index
+// strictly increases) and reads only its own nodes, x columns and vote bins.
+template <typename Form>
+__global__ void k_check_forest(const void* __restrict__ nodes, uint32_t n_nodes, const uint32_t* __restrict__ off,
+                               uint32_t n_trees, uint32_t fbits, uint32_t n_features, uint32_t n_classes,
+                               uint32_t* err) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  uint32_t bad = 0;
+  for (uint32_t t = tid; t < n_trees; t += stride) {
+    const uint32_t b = __ldg(off + t), e = t + 1 < n_trees ? __ldg(off + t + 1) : n_nodes;
+    if (!(b < e && e <= n_nodes)) bad |= 1u;
+  }
+  const uint32_t first = __ldg(off);
+  for (uint32_t i = tid; i < n_nodes; i += stride) {
+    if (i < first) continue;  // before the first tree: never visited
+    uint32_t lo = 0, hi = n_trees;  // the tree t with off[t] <= i < off[t + 1]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) / 2;
+      if (__ldg(off + mid) <= i) lo = mid; else hi = mid;
+    }
+    const uint32_t b = __ldg(off + lo), e = lo + 1 < n_trees ? __ldg(off + lo + 1) : n_nodes;
+    if (i < b || i >= e) {  // only when the offsets are out of order (bit 1 is set then)
+      bad |= 1u;
+      continue;
+    }
+    const typename Form::Raw nd = Form::load(nodes, i);
+    if (Form::inner(nd)) {
+      const uint32_t l = Form::left(nd, fbits);
+      if (l <= i - b || (uint64_t)l + 1 >= (uint64_t)(e - b)) bad |= 2u;
+      if (Form::feature(nd, fbits) >= n_features) bad |= 4u;
+    } else if (Form::value(nd) >= n_classes) {
+      bad |= 8u;
+    }
+  }
+  if (bad) atomicOr(err, bad);
+}
+
+const char* forest_error_text(uint32_t bad) {
+  if (bad & 1u) return "tree offsets are not strictly increasing inside the node array";
+  if (bad & 2u) return "an inner node's children are not after it inside its tree";
+  if (bad & 4u) return "a node's feature index is out of range";
+  return "a leaf's class id is out of range";
+}
+
+// Checks the forest on the device before a walk.  The check's error word is
+// the first word of pred, the caller's output (n_rows >= 1), so nothing is
+// allocated; the walk overwrites it.
+template <typename Form>
+int check_forest_device(const void* nodes, uint32_t n_nodes, const uint32_t* off, uint32_t n_trees, uint32_t fbits,
+                        uint32_t n_features, uint32_t n_classes, uint32_t* pred, cudaStream_t st) {
+  CT_CUDA_TRY(cudaMemsetAsync(pred, 0, sizeof(uint32_t), st));
+  const uint32_t work = std::max(n_nodes, n_trees);
+  k_check_forest<Form><<<std::min<uint32_t>(ceil_div(work, 256), 148 * 8), 256, 0, st>>>(
+      nodes, n_nodes, off, n_trees, fbits, n_features, n_classes, pred);
+  CT_CUDA_TRY(cudaGetLastError());
+  uint32_t bad = 0;
+  CT_CUDA_TRY(cudaMemcpyAsync(&bad, pred, sizeof(bad), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (bad) {
+    set_last_error(std::string("predict: malformed forest: ") + forest_error_text(bad));
+    return CT_ERR_ARG;
+  }
+  return CT_OK;
 }
 
 // Raise a kernel's dynamic shared-memory limit once per device.
@@ -269,6 +341,32 @@ uint32_t compact_feature_bits(uint32_t n_features) {
 bool compact_fits(uint32_t n_features, uint64_t max_tree_nodes) {
   const uint32_t b = compact_feature_bits(n_features);
   return (1u << b) >= n_features && max_tree_nodes <= (1ull << (32 - b));
+}
+
+int check_forest_host(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* off, uint32_t n_trees,
+                      uint32_t n_features, uint32_t n_classes) {
+  uint32_t bad = 0;
+  for (uint32_t t = 0; t < n_trees && !bad; ++t) {
+    const uint32_t b = off[t], e = t + 1 < n_trees ? off[t + 1] : n_nodes;
+    if (!(b < e && e <= n_nodes)) {
+      bad |= 1u;
+      break;
+    }
+    for (uint32_t i = b; i < e; ++i) {
+      const ct_packed_node& nd = nodes[i];
+      if (nd.left != 0) {
+        if (nd.left <= i - b || (uint64_t)nd.left + 1 >= (uint64_t)(e - b)) bad |= 2u;
+        if (nd.feature >= n_features) bad |= 4u;
+      } else if (nd.value >= n_classes) {
+        bad |= 8u;
+      }
+    }
+  }
+  if (bad) {
+    set_last_error(std::string("malformed forest: ") + forest_error_text(bad));
+    return CT_ERR_ARG;
+  }
+  return CT_OK;
 }
 
 void compact_host(const ct_packed_node* in, uint32_t n, uint32_t fbits, ct_compact_node* out) {
@@ -344,28 +442,26 @@ int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_block
 }
 
 // fbits == 0: packed nodes; else compact nodes with that many feature bits.
-int predict(const void* nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees, const float* x,
-            uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes, uint32_t* pred,
-            cudaStream_t st) {
-  CT_ARG_CHECK(nodes && tree_off && x, "predict: NULL input");
+int predict(const void* nodes, uint32_t n_nodes, uint32_t fbits, const uint32_t* tree_off, uint32_t n_trees,
+            const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes, uint32_t* votes,
+            uint32_t* pred, cudaStream_t st) {
+  CT_ARG_CHECK(nodes && tree_off && x && pred, "predict: NULL input or output");
   CT_ARG_CHECK(((uintptr_t)nodes & (fbits ? 7u : 15u)) == 0, "predict: nodes must be aligned to the node size");
   CT_ARG_CHECK(n_trees >= 1 && n_features >= 1, "predict: empty forest or no features");
+  CT_ARG_CHECK(n_nodes >= n_trees, "predict: fewer nodes than trees");
   CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "predict: n_classes out of range");
   CT_ARG_CHECK(!fbits || fbits == compact_feature_bits(n_features), "predict: compact form of another feature count");
   if (n_rows == 0) return CT_OK;
+  if (fbits)
+    CT_TRY(check_forest_device<CompactForm>(nodes, n_nodes, tree_off, n_trees, fbits, n_features, n_classes, pred, st));
+  else
+    CT_TRY(check_forest_device<PackedForm>(nodes, n_nodes, tree_off, n_trees, 0, n_features, n_classes, pred, st));
   const uint32_t rpb = predict_rows_per_block(n_classes, n_features);
   const uint32_t tiles = ceil_div(n_rows, rpb);
-  // Tree groups need the vote table; without one every block walks all
-  // trees.  The forest's size is estimated from the last tree's offset (one
-  // 4-byte read, only for batches large enough to amortize it).
+  // Tree groups need the vote table; without one every block walks all trees.
   uint32_t group = n_trees;
-  if (votes && n_trees >= 16 && n_rows >= 1024) {
-    uint32_t last_off = 0;
-    CT_CUDA_TRY(cudaMemcpyAsync(&last_off, tree_off + n_trees - 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CT_CUDA_TRY(cudaStreamSynchronize(st));
-    group = predict_group_size(n_trees, (uint64_t)last_off * n_trees / (n_trees - 1),
-                               fbits ? CompactForm::BYTES : PackedForm::BYTES);
-  }
+  if (votes && n_trees >= 16 && n_rows >= 1024)
+    group = predict_group_size(n_trees, n_nodes, fbits ? CompactForm::BYTES : PackedForm::BYTES);
   const uint32_t groups = ceil_div(n_trees, group);
   const size_t smem = predict_tile_smem(rpb, n_classes, n_features);
   if (groups > 1) CT_CUDA_TRY(cudaMemsetAsync(votes, 0, (size_t)n_rows * n_classes * sizeof(uint32_t), st));

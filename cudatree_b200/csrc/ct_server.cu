@@ -328,6 +328,7 @@ class Server {
     CT_ARG_CHECK(nodes && off && id && n_nodes && n_trees, "server: empty forest");
     CT_ARG_CHECK(n_features <= cfg.max_features, "server: forest has more features than max_features");
     CT_ARG_CHECK(n_classes >= 1 && n_classes <= CT_MAX_CLASSES, "server: n_classes out of range");
+    CT_TRY(check_forest_host(nodes, n_nodes, off, n_trees, n_features, n_classes));
     if (!st) st = upload_st;
     Forest f;
     f.n_nodes = n_nodes;
@@ -831,73 +832,91 @@ int ct_server_create(const ct_server_config* cfg, void** handle) {
 }
 
 int ct_server_destroy(void* handle) {
-  delete reinterpret_cast<Server*>(handle);
-  return CT_OK;
+  CT_GUARD({
+    delete reinterpret_cast<Server*>(handle);
+    return CT_OK;
+  })
 }
 
 int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
                          uint32_t n_trees, uint32_t n_features, uint32_t n_classes, uint32_t* forest_id) {
   CT_ARG_CHECK(handle, "NULL server");
-  return reinterpret_cast<Server*>(handle)->add_forest(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes,
-                                                        forest_id);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->add_forest(nodes, n_nodes, tree_offset, n_trees, n_features, n_classes,
+                                                          forest_id);
+  })
 }
 
 int ct_server_forest_info(void* handle, uint32_t forest_id, uint32_t* n_nodes, uint32_t* n_trees,
                           uint32_t* n_features, uint32_t* n_classes) {
   CT_ARG_CHECK(handle, "NULL server");
-  return reinterpret_cast<Server*>(handle)->forest_info(forest_id, n_nodes, n_trees, n_features, n_classes);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->forest_info(forest_id, n_nodes, n_trees, n_features, n_classes);
+  })
 }
 
 int ct_server_read_forest(void* handle, uint32_t forest_id, ct_packed_node* nodes, uint32_t* tree_offset) {
   CT_ARG_CHECK(handle, "NULL server");
-  return reinterpret_cast<Server*>(handle)->read_forest(forest_id, nodes, tree_offset);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->read_forest(forest_id, nodes, tree_offset);
+  })
 }
 
 int ct_server_remove_forest(void* handle, uint32_t forest_id) {
   CT_ARG_CHECK(handle, "NULL server");
-  return reinterpret_cast<Server*>(handle)->remove_forest(forest_id);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->remove_forest(forest_id);
+  })
 }
 
 int ct_server_submit(void* handle, ct_request* req) {
   CT_ARG_CHECK(handle, "NULL server");
-  return reinterpret_cast<Server*>(handle)->submit(req);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->submit(req);
+  })
 }
 
 int ct_server_wait(void* handle, ct_request* req, double timeout_s) {
   CT_ARG_CHECK(handle && req, "NULL argument");
-  return reinterpret_cast<Server*>(handle)->wait(req, timeout_s);
+  CT_GUARD({
+    return reinterpret_cast<Server*>(handle)->wait(req, timeout_s);
+  })
 }
 
 int ct_server_replay(void* handle, ct_request* reqs, uint32_t n, double timeout_s, ct_server_stats* stats) {
   CT_ARG_CHECK(handle && (reqs || n == 0), "NULL argument");
-  Server* s = reinterpret_cast<Server*>(handle);
-  s->reset_stats();
-  const double t0 = now_s();
-  for (uint32_t i = 0; i < n; ++i) {
-    const double due = t0 + reqs[i].arrival_s;
-    while (now_s() < due) {
-      const double left = due - now_s();
-      if (left > 200e-6) std::this_thread::sleep_for(std::chrono::duration<double>(left - 100e-6));
+  CT_GUARD({
+    Server* s = reinterpret_cast<Server*>(handle);
+    s->reset_stats();
+    const double t0 = now_s();
+    for (uint32_t i = 0; i < n; ++i) {
+      const double due = t0 + reqs[i].arrival_s;
+      while (now_s() < due) {
+        const double left = due - now_s();
+        if (left > 200e-6) std::this_thread::sleep_for(std::chrono::duration<double>(left - 100e-6));
+      }
+      const int st = s->submit(&reqs[i]);
+      if (st != CT_OK && st != CT_ERR_OOM) return st;
     }
-    const int st = s->submit(&reqs[i]);
-    if (st != CT_OK && st != CT_ERR_OOM) return st;
-  }
-  int worst = CT_OK;
-  for (uint32_t i = 0; i < n; ++i) {
-    if (!reqs[i].pending_) continue;
-    const int st = s->wait(&reqs[i], timeout_s);
-    if (st == CT_ERR_TIMEOUT) return st;
-    if (st != CT_OK) worst = st;
-  }
-  if (stats) s->stats(stats);
-  (void)worst;
-  return CT_OK;
+    int worst = CT_OK;
+    for (uint32_t i = 0; i < n; ++i) {
+      if (!reqs[i].pending_) continue;
+      const int st = s->wait(&reqs[i], timeout_s);
+      if (st == CT_ERR_TIMEOUT) return st;
+      if (st != CT_OK) worst = st;
+    }
+    if (stats) s->stats(stats);
+    (void)worst;
+    return CT_OK;
+  })
 }
 
 int ct_server_get_stats(void* handle, ct_server_stats* out) {
   CT_ARG_CHECK(handle && out, "NULL argument");
-  reinterpret_cast<Server*>(handle)->stats(out);
-  return CT_OK;
+  CT_GUARD({
+    reinterpret_cast<Server*>(handle)->stats(out);
+    return CT_OK;
+  })
 }
 
 }  // extern "C"

@@ -141,7 +141,8 @@ def unpack_trees(packed, offsets, n_features, dtype_labels):
 
 def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_votes, compact=False):
     """Walk the forest on the device: packed nodes (ct_predict) or, with
-    compact=True, a device tensor of 8-byte compact nodes (ct_predict_compact)."""
+    compact=True, a device tensor of 8-byte compact nodes (ct_predict_compact).
+    The library checks the forest before it walks it."""
     dev = _device()
     x = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
     if x.ndim != 2 or x.shape[1] != n_features:
@@ -154,8 +155,9 @@ def _predict_packed(packed, offsets, n_trees, x, n_features, n_classes, want_vot
     xd = torch.from_numpy(x).to(dev)
     votes = torch.empty((n, n_classes), dtype=torch.int32, device=dev)  # also the tree-group vote table
     pred = torch.empty((n,), dtype=torch.int32, device=dev)
-    _lib.call("ct_predict_compact" if compact else "ct_predict", _ptr(nodes), _ptr(offs), n_trees, _ptr(xd), n,
-              n_features, n_classes, _ptr(votes), _ptr(pred), _stream())
+    n_nodes = nodes.numel() * nodes.element_size() // (8 if compact else 16)
+    _lib.call("ct_predict_compact" if compact else "ct_predict", _ptr(nodes), n_nodes, _ptr(offs), n_trees, _ptr(xd),
+              n, n_features, n_classes, _ptr(votes), _ptr(pred), _stream())
     return (votes if want_votes else pred).cpu().numpy().view(np.uint32)
 
 

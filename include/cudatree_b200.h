@@ -166,9 +166,10 @@ int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* no
  * buffers of its own): the scratch is a static 16 MiB array per device
  * instead of a caller workspace.  total_samples must be >= the sum of the
  * nodes' n; batches whose scratch exceeds 16 MiB are rejected with
- * CT_ERR_ARG.  The first call on a device looks up the array's device
- * address and should come before any stream capture; calls that overlap on
- * the same device race on the shared array and must be serialized. */
+ * CT_ERR_ARG.  Every call looks up the array's device address (no
+ * allocation); the first call on a device may load the library's device
+ * code and should come before any stream capture.  Calls that overlap on the
+ * same device race on the shared array and must be serialized. */
 int ct_split_nodes_noalloc(const ct_problem* p, const ct_lists* lists, const ct_node* nodes,
                            const uint32_t* totals, uint32_t n_nodes, uint64_t total_samples,
                            ct_split_result* out, void* stream);
@@ -259,7 +260,14 @@ int ct_fetch_trees(const ct_tree_buffers* trees, uint32_t n_trees, const uint32_
  * predict.cu (base_tree.py:44-81, predict.cu:12-69) and the host vote
  * (random_forest.py:339-377).  x [n_rows][n_features] float32 row-major;
  * votes [n_rows][n_classes] uint32 (may be NULL); pred [n_rows] uint32 class
- * ids (may be NULL).  All device pointers; nodes 16-byte aligned. */
+ * ids.  All device pointers; nodes 16-byte aligned; n_nodes nodes in all
+ * (tree t ends where tree t+1 starts, the last tree at n_nodes).  Before the
+ * walk the forest is checked on the device (its error word is pred[0], so
+ * nothing is allocated): tree offsets strictly increasing inside the array,
+ * every inner node's children after it inside its tree, features below
+ * n_features, leaf classes below n_classes; a forest that fails returns
+ * CT_ERR_ARG and is never walked.  The reference trusts its arrays
+ * (predict.cu:50-67). */
 typedef struct ct_packed_node {
   float threshold;
   uint32_t feature;
@@ -267,9 +275,16 @@ typedef struct ct_packed_node {
   uint32_t value;  /* leaf class id                                           */
 } ct_packed_node;
 
-int ct_predict(const ct_packed_node* nodes, const uint32_t* tree_offset, uint32_t n_trees,
-               const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
-               uint32_t* votes, uint32_t* pred, void* stream);
+int ct_predict(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
+               uint32_t n_trees, const float* x, uint32_t n_rows, uint32_t n_features,
+               uint32_t n_classes, uint32_t* votes, uint32_t* pred, void* stream);
+
+/* The forest check of ct_predict on host arrays (no device work): CT_OK, or
+ * CT_ERR_ARG with the reason as the last error.  For callers that load
+ * forests from files or other processes before uploading them; the
+ * reference has no check (restore_forest, random_forest.py:18-23). */
+int ct_check_forest(const ct_packed_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
+                    uint32_t n_trees, uint32_t n_features, uint32_t n_classes);
 
 /* Compact forest: the same trees in 8-byte nodes, which halve the bytes a
  * walk step reads (the walk is bound by them).  With b = feature bits (the
@@ -284,13 +299,15 @@ typedef struct ct_compact_node {
 /* 1 when trees of up to max_tree_nodes nodes fit the compact form. */
 int ct_compact_fits(uint32_t n_features, uint32_t max_tree_nodes);
 /* Device packed -> device compact (stream ordered); CT_ERR_ARG when the
- * trees do not fit. */
+ * trees do not fit.  A node whose child or feature does not fit the compact
+ * fields becomes one that ct_predict_compact's forest check rejects. */
 int ct_compact_forest(const ct_packed_node* nodes, uint32_t n_nodes, uint32_t n_features,
                       uint32_t max_tree_nodes, ct_compact_node* out, void* stream);
-/* ct_predict on the compact form (nodes 8-byte aligned); same results. */
-int ct_predict_compact(const ct_compact_node* nodes, const uint32_t* tree_offset, uint32_t n_trees,
-                       const float* x, uint32_t n_rows, uint32_t n_features, uint32_t n_classes,
-                       uint32_t* votes, uint32_t* pred, void* stream);
+/* ct_predict on the compact form (nodes 8-byte aligned); same check, same
+ * results. */
+int ct_predict_compact(const ct_compact_node* nodes, uint32_t n_nodes, const uint32_t* tree_offset,
+                       uint32_t n_trees, const float* x, uint32_t n_rows, uint32_t n_features,
+                       uint32_t n_classes, uint32_t* votes, uint32_t* pred, void* stream);
 
 /* ----------------------------------------------------------- serving --- */
 /* No counterpart in the reference (its predict re-uploads X and every tree
@@ -354,7 +371,8 @@ typedef struct ct_server_stats {
 int ct_server_create(const ct_server_config* cfg, void** handle);
 int ct_server_destroy(void* handle);
 /* Copies a packed forest (host arrays, layout of ct_predict) into the forest
- * pool; CT_ERR_OOM when the pool has no room. */
+ * pool; CT_ERR_OOM when the pool has no room.  The forest is checked on the
+ * host first, as ct_predict checks it (CT_ERR_ARG when malformed). */
 int ct_server_add_forest(void* handle, const ct_packed_node* nodes, uint32_t n_nodes,
                          const uint32_t* tree_offset, uint32_t n_trees, uint32_t n_features,
                          uint32_t n_classes, uint32_t* forest_id);

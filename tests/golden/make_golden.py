@@ -11,6 +11,11 @@
 * ``oracle_forests.npz`` — canonical forests (node arrays in breadth-first
   order) of small seeded fits, which the GPU tests compare node for node and
   the CPU tests use to detect drift of the oracle.
+* ``covtype_trees.json`` — node counts and SHA-256 digests of the first
+  trees of the oracle forest at the benchmark's full covtype-shaped size
+  (581,012 x 54, 7 classes, max_features 7, bootstrap, seed 1000): the GPU
+  parity test checks its trees against them, and a CPU test regrows them to
+  catch drift of the oracle.
 """
 from __future__ import annotations
 
@@ -102,8 +107,26 @@ def oracle_forests():
     np.savez_compressed(OUT / "oracle_forests.npz", **arrays)
 
 
+COVTYPE = {"make": "covtype_like", "seed": 1000, "max_features": 7, "bootstrap": True, "trees": 3}
+
+
+def covtype_trees():
+    import json
+
+    from tests import oracle_jobs
+    c = COVTYPE
+    with oracle_jobs.pool(c["trees"]) as ex:
+        trees = [f.result() for f in oracle_jobs.submit_forest(ex, c["make"], None, c["trees"], c["seed"],
+                                                                c["max_features"], c["bootstrap"])]
+    rec = dict(c, workload="covtype-shaped synthetic 581012x54 f32, 7 classes",
+               digests=[{"tree": i, "n_nodes": t.n_nodes, "sha256": oracle_jobs.oracle_digest(t)}
+                        for i, t in enumerate(trees)])
+    (OUT / "covtype_trees.json").write_text(json.dumps(rec, indent=1) + "\n")
+
+
 if __name__ == "__main__":
     reference_chain_nodes()
     oracle_forests()
+    covtype_trees()
     for p in sorted(OUT.glob("*.npz")):
         print(p.name, p.stat().st_size, "bytes")

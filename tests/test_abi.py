@@ -43,7 +43,7 @@ def test_struct_layouts_match_header_sizes():
 
 def test_argument_errors_are_reported_without_gpu():
     lib = _lib.load()
-    st = lib.ct_predict(None, None, 0, None, 0, 0, 0, None, None, None)
+    st = lib.ct_predict(None, 0, None, 0, None, 0, 0, 0, None, None, None)
     assert st == 1
     assert "NULL" in _lib.last_error()
     prob = _lib.Problem(1, 1, 1, 10, 4, 3, 3, 1, 9, 1, 0, 0)  # uint16 index width is 2 or 4 only
@@ -156,3 +156,51 @@ def test_compact_labels_matches_np_unique():
         assert t.dtype == t2.dtype
         np.testing.assert_array_equal(t, t2)
         np.testing.assert_array_equal(i, i2)
+
+
+def _check(packed, offsets, n_features=4, n_classes=3):
+    packed = np.ascontiguousarray(packed)
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint32)
+    return _lib.load().ct_check_forest(packed.ctypes.data, packed.shape[0], offsets.ctypes.data,
+                                       offsets.shape[0], n_features, n_classes)
+
+
+def _forest():
+    """Two breadth-first trees: a stump (3 nodes) and a depth-2 tree (5 nodes)."""
+    from cudatree_b200.random_forest import PACKED_DTYPE
+    p = np.zeros(8, dtype=PACKED_DTYPE)
+    p["left"] = [1, 0, 0, 1, 3, 0, 0, 0]
+    p["feature"] = [2, 0, 0, 0, 3, 0, 0, 0]
+    p["value"] = [0, 1, 2, 0, 0, 2, 0, 1]
+    return p, np.array([0, 3], np.uint32)
+
+
+@pytest.mark.parametrize("case", ["ok", "cycle", "self_loop", "child_past_tree", "bad_feature", "bad_class",
+                                  "offsets_out_of_order", "offset_past_end"])
+def test_malformed_forests_are_rejected_before_any_walk(case):
+    """The forest check that ct_predict runs on the device and
+    ct_server_add_forest runs on the host, through ct_check_forest: children
+    must come after their node inside its tree (so every walk ends), features
+    and leaf classes must be in range, tree offsets strictly increasing."""
+    p, off = _forest()
+    if case == "cycle":
+        p["left"][4] = 1  # node 4 of tree 1 points back to its grandparent
+    elif case == "self_loop":
+        p["left"][3] = 0 + 0  # root becomes a leaf: still valid ...
+        p["left"][4] = 1  # ... and node 1 (local) points to itself
+    elif case == "child_past_tree":
+        p["left"][0] = 2  # right child would be node 3: the next tree's root
+    elif case == "bad_feature":
+        p["feature"][4] = 4
+    elif case == "bad_class":
+        p["value"][7] = 3
+    elif case == "offsets_out_of_order":
+        off = np.array([3, 0], np.uint32)
+    elif case == "offset_past_end":
+        off = np.array([0, 8], np.uint32)
+    st = _check(p, off)
+    if case == "ok":
+        assert st == 0, _lib.last_error()
+    else:
+        assert st == 1, case
+        assert "malformed forest" in _lib.last_error()

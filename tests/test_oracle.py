@@ -134,3 +134,21 @@ def test_candidate_shortcut_matches_double_test():
         d = (xn - x).astype(np.float32)
     fast = np.where(~(xn > x), False, np.where(d > np.float32(1e-4), True, exact))
     np.testing.assert_array_equal(fast, exact)
+
+
+def test_covtype_full_size_oracle_trees_match_fixture():
+    """The oracle's first three trees of the benchmark forest (581,012 x 54
+    covtype-shaped, 7 classes, max_features 7, bootstrap, seed 1000) against
+    the node counts and digests committed in tests/golden/covtype_trees.json:
+    the GPU parity test pins its trees to the same digests."""
+    import json
+    from pathlib import Path
+
+    from tests import oracle_jobs
+    fx = json.loads((Path(__file__).resolve().parent / "golden" / "covtype_trees.json").read_text())
+    with oracle_jobs.pool(fx["trees"]) as ex:
+        trees = [f.result() for f in oracle_jobs.submit_forest(ex, fx["make"], None, fx["trees"], fx["seed"],
+                                                                fx["max_features"], fx["bootstrap"])]
+    for d, t in zip(fx["digests"], trees):
+        assert t.n_nodes == d["n_nodes"], d["tree"]
+        assert oracle_jobs.oracle_digest(t) == d["sha256"], d["tree"]

@@ -56,3 +56,23 @@ def test_noalloc_rejects_batches_beyond_the_static_scratch(cuda_device):
                                             nodes.shape[0], 1 << 34, out.data_ptr(), G.stream())
     assert st == 1
     assert "static scratch" in _lib.last_error()
+
+
+def test_noalloc_understated_total_samples_then_recovers(cuda_device):
+    """total_samples sizes every scratch list.  Passed 1 for a batch of 10,000
+    rows, the device capacity checks stop the split search (no record past a
+    list's end is written or read) and the call returns CT_ERR_CAPACITY; the
+    next call with the right total, which reuses the same static scratch,
+    matches ct_split_nodes field for field."""
+    gp, gl, groups, nodes, totals, keys, _ = _grouped_case(*BATCHES[0])
+    nd = G.to_dev(nodes)
+    td = G.to_dev(totals.astype(np.uint32))
+    out = G.dev_bytes(nodes.shape[0] * 32)
+    st = _lib.load().ct_split_nodes_noalloc(C.byref(gp.prob), C.byref(gl.lists), nd.data_ptr(), td.data_ptr(),
+                                            nodes.shape[0], 1, out.data_ptr(), G.stream())
+    assert st == 7
+    assert "work lists overflowed" in _lib.last_error()
+    ref, _, _ = G.split_nodes(gp, gl, nodes, totals)
+    got = _noalloc(gp, gl, nodes, totals)
+    for field in ("score", "feature", "pos", "imp_left", "imp_right", "threshold", "n_selected"):
+        np.testing.assert_array_equal(got[field], ref[field], err_msg=field)
