@@ -27,6 +27,21 @@ namespace {
 
 constexpr uint32_t SCAN_BATCH = 4;  // rounds of 32 whose loads are issued together
 
+// Candidate queue of the split scan: per warp, in shared memory after the
+// warp's class counts and class totals.
+struct ScanCand {
+  int64_t sl;   // left sum of squared class counts at pos
+  int64_t sr;   // right sum
+  uint32_t pos;
+  float t;      // approximate SL / n_L + SR / n_R
+};
+constexpr uint32_t SCAN_QCAP = 64;
+constexpr float SCAN_KEEP = 1.0f - 1.0f / 262144.0f;  // keep band 1 - 2^-18 (see k_split_scan)
+__host__ __device__ __forceinline__ uint32_t scan_count_words(uint32_t C) { return (2 * C + 1) & ~1u; }
+__host__ __device__ __forceinline__ uint32_t scan_warp_words(uint32_t C) {
+  return scan_count_words(C) + SCAN_QCAP * (uint32_t)(sizeof(ScanCand) / 4);
+}
+
 __device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
 __device__ __forceinline__ uint32_t global_warp() {
@@ -205,14 +220,65 @@ k_scan_carry(LevelScratch s, uint32_t C) {
 }
 
 // ------------------------------------------------------------------------
+// Exact fp64 score of the queued candidates whose approximate score is within
+// the keep band of the best approximate score; the lane's best is the
+// lexicographic minimum of (score, position).  Warp-collective: the queue is
+// read after a __syncwarp and may be refilled after the next one.
+__device__ __noinline__ void scan_flush(const ScanCand* q, uint32_t qn, float thr, double nn, uint32_t lane,
+                                           double& best, uint32_t& bpos, float& bil, float& bir) {
+  __syncwarp();
+  for (uint32_t i = lane; i < qn; i += 32) {
+    const ScanCand e = q[i];
+    if (!(e.t >= thr)) continue;
+    const double nl = (double)(e.pos + 1);
+    const double nr = __dsub_rn(nn, nl);
+    const double gl = gini_part(e.sl, nl, nn);
+    const double gr = gini_part(e.sr, nr, nn);
+    const double sc = __dadd_rn(gl, gr);
+    if (sc < best || (sc == best && e.pos < bpos)) {
+      best = sc;
+      bpos = e.pos;
+      bil = __double2float_rn(gl);
+      bir = __double2float_rn(gr);
+    }
+  }
+  __syncwarp();
+}
+
+// Gini scan of one piece of a (node, feature) segment.
+//
+// Per round of 32 positions: the class rank of each position (match over the
+// labels plus the warp's running class counts) gives the exact increments of
+// the left and right sums of squared class counts, 2k + 1 and 1 - 2 (T - k)
+// (the reference's serial recurrence, dfs_module.cu:392-398).  A round with
+// no candidate position (equal or nearly equal neighbouring values,
+// dfs_module.cu:400) only advances the running sums, by two warp reductions.
+// A round with candidates takes inclusive warp scans for the per-position
+// sums SL, SR and scores each candidate approximately in fp32:
+// t = SL / n_L + SR / n_R, the quantity whose maximum is the minimum Gini
+// score (score = 1 - t / n in exact arithmetic).  Only candidates whose t is
+// within the keep band of the largest t seen so far are queued; the queue is
+// scored exactly (fp64, correctly rounded, dfs_module.cu:404-407) when it
+// fills and at the end of the piece, against the final band.
+//
+// Why the result is the exact argmin: t~ (fp32: int64 -> f32 conversions,
+// __fdividef at <= 2 ulp, one add) is within eps = 2^-20 of t relatively.  A
+// candidate q never scored exactly has t~(q) < (1 - 2^-18) t~max, so
+// t(q) < (1 - 2 eps) t(p*) for the position p* of t~max, and its real score
+// exceeds p*'s by more than 2 eps t(p*) / n >= 2 eps / C (t >= n / C by
+// Cauchy-Schwarz), which is > 1.8e-9 for C <= 1024: far beyond the fp64
+// rounding of either score (< 16 * 2^-53).  So q cannot equal or beat p*'s
+// exact score, which is scored; ties among the scored keep the lowest
+// position.
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
+__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)
 k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
              LevelScratch s, uint32_t scan_piece) {
-  extern __shared__ uint32_t smem[];
+  extern __shared__ __align__(8) uint32_t smem[];
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * C;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * scan_warp_words(C);
   uint32_t* T = cnt + C;
+  ScanCand* q = reinterpret_cast<ScanCand*>(cnt + scan_count_words(C));
   const uint32_t pi = global_warp();
   const uint32_t lane = lane_id();
   if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
@@ -243,6 +309,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   double best = dinf();
   uint32_t bpos = NONE;
   float bil = 0.f, bir = 0.f;
+  uint32_t tmax = 0;  // bits of the largest approximate t so far (t >= 0: bits order as values)
+  uint32_t qn = 0;    // queued candidates
   const unsigned lt = lanemask_lt();
   // Software pipeline over batches of SCAN_BATCH rounds: while batch b is
   // scanned, the label/value gathers of batch b+1 and the index loads of
@@ -257,8 +325,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t p = lo + r * 32 + lane;
       rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
-      const uint32_t q = p + B;
-      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
+      const uint32_t q2 = p + B;
+      rows_n[r] = q2 < hi ? (uint32_t)__ldcs(lst + q2) : 0u;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
@@ -278,8 +346,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
-      const uint32_t q = base + 2 * B + r * 32 + lane;
-      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
+      const uint32_t q2 = base + 2 * B + r * 32 + lane;
+      rows_n[r] = q2 < hi ? (uint32_t)__ldcs(lst + q2) : 0u;
     }
     const float x_e = __shfl_sync(FULL, xs_n[0], 0);  // first value of the next batch
 #pragma unroll
@@ -292,9 +360,9 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       const float first_next = (r + 1 < SCAN_BATCH) ? __shfl_sync(FULL, xs[r + 1 < SCAN_BATCH ? r + 1 : r], 0) : x_e;
       if (lane == 31) xn = first_next;
       if (valid && p + 1 == hi && p + 1 < n) xn = xf[entry_row(v, lst[p + 1])];  // next piece's first element
+      const bool cand = valid && p + 1 < n && is_candidate_sorted(x, xn);
       const unsigned grp = __match_any_sync(FULL, c);
-      uint32_t k = 0;
-      int64_t tc = 0;
+      uint32_t k = 0, tc = 0;
       if (valid) {
         k = cnt[c] + __popc(grp & lt);
         tc = T[c];
@@ -302,37 +370,43 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       __syncwarp();
       if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
       __syncwarp();
-      const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
-      const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
-      int64_t il, ir, tl, tr;  // inclusive warp prefix and warp total of each increment
-      if (narrow) {  // |partial sums| <= 32 (2n + 1) < 2^31
-        const int32_t a = warp_incl_scan_i32((int32_t)dl), b = warp_incl_scan_i32((int32_t)dr);
-        il = a;
-        ir = b;
-        tl = __shfl_sync(FULL, a, 31);
-        tr = __shfl_sync(FULL, b, 31);
-      } else {
-        il = warp_incl_scan_i64(dl);
-        ir = warp_incl_scan_i64(dr);
-        tl = __shfl_sync(FULL, il, 31);
-        tr = __shfl_sync(FULL, ir, 31);
-      }
-      const int64_t SL = sl + il;
-      const int64_t SR = sr + ir;
-      sl += tl;
-      sr += tr;
-      if (valid && p + 1 < n && is_candidate_sorted(x, xn)) {
-        const double nl = (double)(p + 1);
-        const double nr = __dsub_rn(nn, nl);
-        const double gl = gini_part(SL, nl, nn);
-        const double gr = gini_part(SR, nr, nn);
-        const double sc = __dadd_rn(gl, gr);
-        if (sc < best) {
-          best = sc;
-          bpos = p;
-          bil = __double2float_rn(gl);
-          bir = __double2float_rn(gr);
+      int64_t SL, SR;
+      if (narrow) {  // |increments| <= 2n + 1, |partial sums| <= 32 (2n + 1) < 2^31
+        const int32_t dl = valid ? 2 * (int32_t)k + 1 : 0;
+        const int32_t dr = valid ? 1 - 2 * ((int32_t)tc - (int32_t)k) : 0;
+        if (__ballot_sync(FULL, cand) == 0u) {
+          sl += __reduce_add_sync(FULL, dl);
+          sr += __reduce_add_sync(FULL, dr);
+          continue;
         }
+        const int32_t a = warp_incl_scan_i32(dl), b = warp_incl_scan_i32(dr);
+        SL = sl + a;
+        SR = sr + b;
+        sl += __shfl_sync(FULL, a, 31);
+        sr += __shfl_sync(FULL, b, 31);
+      } else {
+        const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
+        const int64_t dr = valid ? 1 - 2 * ((int64_t)tc - (int64_t)k) : 0;
+        const int64_t a = warp_incl_scan_i64(dl), b = warp_incl_scan_i64(dr);
+        SL = sl + a;
+        SR = sr + b;
+        sl += __shfl_sync(FULL, a, 31);
+        sr += __shfl_sync(FULL, b, 31);
+      }
+      float t = 0.f;
+      if (cand) t = __fdividef((float)SL, (float)(p + 1)) + __fdividef((float)SR, (float)(n - p - 1));
+      tmax = max(tmax, __reduce_max_sync(FULL, __float_as_uint(t)));
+      const float thr = __uint_as_float(tmax) * SCAN_KEEP;
+      const bool push = cand && t >= thr;
+      const unsigned pm = __ballot_sync(FULL, push);
+      if (pm) {
+        const uint32_t np = __popc(pm);
+        if (qn + np > SCAN_QCAP) {
+          scan_flush(q, qn, thr, nn, lane, best, bpos, bil, bir);
+          qn = 0;
+        }
+        if (push) q[qn + __popc(pm & lt)] = ScanCand{SL, SR, p, t};
+        qn += np;
       }
     }
 #pragma unroll
@@ -341,6 +415,7 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       xs[r] = xs_n[r];
     }
   }
+  scan_flush(q, qn, __uint_as_float(tmax) * SCAN_KEEP, nn, lane, best, bpos, bil, bir);
   warp_argmin2(best, bpos, bil, bir);
   if (lane == 0) {
     PieceBest pb;
@@ -1187,7 +1262,8 @@ void split_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const 
   k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
                                                                                        scan_piece);
   k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
-  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 2 * sm1, st>>>(
+  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK,
+                             (size_t)WARPS_PER_BLOCK * scan_warp_words(v.n_classes) * sizeof(uint32_t), st>>>(
       v, nodes, tot, s, scan_piece);
   pf->end();
   pf->launched(CT_K_SCAN, 3);

@@ -24,14 +24,16 @@ import time
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, forest_format
+from .forest_format import PACKED_DTYPE
 from .random_tree import RandomClassifierTree
 
 
 def restore_forest(trees, dtype_labels, compt_table=None, n_features=None, params=None):
     """Unpickle hook (reference random_forest.py:18-23).  Unlike the reference,
     the restored forest keeps its label table and can predict."""
-    f = RandomForestClassifier(len(trees), **(params or {}))
+    params = dict(params or {})
+    f = RandomForestClassifier(params.pop("n_estimators", len(trees)), **params)
     f._trees = list(trees)
     for t in f._trees:
         t.forest = f
@@ -78,9 +80,6 @@ def default_bfs_threshold(n_labels: int, n_samples: int, max_features: int) -> i
     """Reference random_forest.py:278-289 ("Titan" regression, clamped)."""
     t = int(4746 + 4 * n_labels + 0.0651 * n_samples - 75 * max_features)
     return max(min(t, 50000), 2000)
-
-
-PACKED_DTYPE = np.dtype([("threshold", "<f4"), ("feature", "<u4"), ("left", "<u4"), ("value", "<u4")])
 
 
 def pack_trees(trees):
@@ -194,14 +193,36 @@ class RandomForestClassifier:
 
     # ------------------------------------------------------------ pickling
     def _params(self):
-        return dict(max_features=self.max_features, min_samples_split=self.min_samples_split,
+        return dict(n_estimators=self.n_estimators, max_features=self.max_features,
+                    min_samples_split=self.min_samples_split,
                     bootstrap=self.bootstrap, seed=self.seed, fit_mode=self.fit_mode,
                     subtree_cutoff=self.subtree_cutoff)
 
     def __reduce__(self):
+        """A fitted forest pickles as its flat format (forest_format); an
+        unfitted one as its constructor arguments."""
+        if self._trees:
+            return forest_format.restore_forest_flat, (forest_format.dumps(self),)
         return restore_forest, (self._trees, getattr(self, "dtype_labels", np.dtype(np.uint8)).str,
                                 getattr(self, "compt_table", None), getattr(self, "n_features", None),
                                 self._params())
+
+    def to_bytes(self) -> bytes:
+        """The fitted forest in the versioned flat format (forest_format)."""
+        return forest_format.dumps(self)
+
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "RandomForestClassifier":
+        """A forest stored by to_bytes or save; ValueError when the bytes are
+        not a valid flat forest."""
+        return forest_format.loads(data)
+
+    def save(self, path) -> None:
+        forest_format.save(self, path)
+
+    @classmethod
+    def load(cls, path) -> "RandomForestClassifier":
+        return forest_format.load(path)
 
     # ------------------------------------------------------------- fitting
     def fit_init(self, samples, target):

@@ -145,6 +145,19 @@ class ForestServer:
             self._tables[fid.value] = np.asarray(table)
         return fid.value
 
+    def load_forest(self, source) -> int:
+        """Make a stored forest resident: source is a path or the bytes of the
+        versioned flat format (forest_format), whose node section goes to the
+        forest pool as it is, after the host check."""
+        from . import forest_format
+        if isinstance(source, (bytes, bytearray, memoryview)):
+            data = bytes(source)
+        else:
+            with open(source, "rb") as fh:
+                data = fh.read()
+        packed, offsets, hdr, table = forest_format.decode(data)
+        return self.add_packed(packed, offsets, hdr["n_features"], hdr["n_classes"], table)
+
     def read_forest(self, forest_id: int):
         """(packed nodes, tree offsets, n_features, n_classes) of a resident forest, exactly as added or fitted."""
         nn, nt, nf, nc = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()

@@ -97,3 +97,34 @@ def test_server_refuses_malformed_forests(cuda_device):
         np.testing.assert_array_equal(srv.predict(fid, x[:300]), forest.predict(x[:300]))
     finally:
         srv.close()
+
+
+def test_stored_forest_predicts_as_fitted(cuda_device, tmp_path):
+    """fit -> pickle / flat bytes / file -> restore -> predict and
+    predict_proba equal the fitted forest's and the oracle's, vote for vote;
+    the stored bytes also load straight into a server's forest pool.  The
+    reference's restored forest cannot predict (random_forest.py:18-23,
+    :94, :453-457)."""
+    import pickle
+
+    x, y = _data(4000, 9, 5, 21)
+    labels = np.array(["oak", "elm", "ash", "fir", "yew"])[y]
+    forest = RandomForestClassifier(n_estimators=7, seed=33).fit(x, labels)
+    ref = O.fit_forest(x, labels, n_estimators=7, seed=33)
+    want = forest.predict(x)
+    np.testing.assert_array_equal(want, O.predict(ref, x))
+    forest.save(tmp_path / "f.ctf")
+    restored = [pickle.loads(pickle.dumps(forest)), RandomForestClassifier.from_bytes(forest.to_bytes()),
+                RandomForestClassifier.load(tmp_path / "f.ctf")]
+    for g in restored:
+        np.testing.assert_array_equal(g.predict(x), want)
+        np.testing.assert_array_equal(g.predict_proba(x), forest.predict_proba(x))
+        np.testing.assert_array_equal(g.predict_proba(x), O.predict_proba(ref, x))
+    srv = ForestServer(max_features=16, fit_workers=1, max_fit_rows=1000, max_fit_trees=2)
+    try:
+        fid = srv.load_forest(forest.to_bytes())
+        np.testing.assert_array_equal(srv.predict(fid, x[:1500]), want[:1500])
+        fid2 = srv.load_forest(tmp_path / "f.ctf")
+        np.testing.assert_array_equal(srv.predict(fid2, x[1500:]), want[1500:])
+    finally:
+        srv.close()
