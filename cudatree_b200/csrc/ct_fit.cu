@@ -144,6 +144,7 @@ struct FitLayout {
   ct_node* small;        // small nodes waiting for their warp subtree (kept across levels)
   mutable uint64_t small_bound;  // upper bound of the entries in small
   uint32_t* n_in;
+  uint32_t* fbin;        // two-valued feature bits (feature_flags)
   ct_node* list[2];
   uint32_t* tot[2];
   uint64_t* mask[2];     // constant-feature masks of the lists (batched form, n_features <= 64), else NULL
@@ -170,6 +171,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
   L->small_bound = 0;
   L->n_in = a.take<uint32_t>(slots);
+  L->fbin = a.take<uint32_t>((p->n_features + 31) / 32);
   // the plain form moves nodes through the host, so only the batched form keeps masks
   const bool masks = o->mode == CT_FIT_BATCHED && p->n_features <= 64;
   for (int i = 0; i < 2; ++i) {
@@ -330,14 +332,17 @@ uint32_t default_bfs_threshold(const ct_problem* p) {
 }
 
 // The fit's view: list entries carry their row's label when it fits
-// (fit_label_shift).  The packed presort that seeds the lists goes to slot 0
-// of buffer 1, which no step writes before the first partition.
-View fit_view(const ct_problem* p, const ct_lists* l) {
+// (fit_label_shift), and two-valued features are marked (feature_flags, run
+// at the start of each fit call) for the split scan's boundary search.  The
+// packed presort that seeds the lists goes to slot 0 of buffer 1, which no
+// step writes before the first partition.
+View fit_view(const ct_problem* p, const ct_lists* l, const FitLayout& L) {
   View v = make_view(p, l);
   if (const uint32_t sh = fit_label_shift(p)) {
     v.lab_shift = sh;
     v.row_mask = (1u << sh) - 1u;
   }
+  v.fbin = L.fbin;
   return v;
 }
 
@@ -352,8 +357,9 @@ int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const voi
 
 int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
                 const FitLayout& L, const ct_tree_buffers* trees, cudaStream_t st) {
-  View v = fit_view(p, l);
+  View v = fit_view(p, l, L);
   TreeView tv = tree_view(trees, 0);
+  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, st));
   CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
   CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
   current_prof()->begin(CT_K_BOOTSTRAP);
@@ -378,9 +384,10 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
 int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
               const ct_fit_options* o, const FitLayout& L, const ct_tree_buffers* trees,
               cudaStream_t st) {
-  View v = fit_view(p, l);
+  View v = fit_view(p, l, L);
   const uint32_t C = p->n_classes;
   const uint32_t thr = o->bfs_threshold ? o->bfs_threshold : default_bfs_threshold(p);
+  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, st));
   struct Pending {
     ct_node nd;
     std::vector<uint32_t> tot;

@@ -165,7 +165,14 @@ struct View {
   // entry has the row's label without a gather into `labels`.
   uint32_t row_mask;
   uint32_t lab_shift;
+  // Bit f set: feature f takes at most two distinct values over all rows
+  // (feature_flags), so its split scan needs only the position of the node's
+  // value boundary.  NULL: every feature takes the general scan.
+  const uint32_t* fbin;
 };
+__device__ __forceinline__ bool two_valued(const View& v, uint32_t f) {
+  return v.fbin && ((__ldg(v.fbin + (f >> 5)) >> (f & 31)) & 1u);
+}
 
 // Packed mark table: bit r of a slot's words is row r's left flag.  The
 // words of one tree (N/8 bytes) fit in an SM's L1, unlike the byte table.
@@ -397,6 +404,10 @@ int check_forest_host(const ct_packed_node* nodes, uint32_t n_nodes, const uint3
                       uint32_t n_features, uint32_t n_classes);
 int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_blocks, uint32_t total_rows,
                   size_t smem, bool any_grouped, cudaStream_t st);
+// Bit f of bits ([ceil(n_features / 32)] words, zeroed here): feature f takes
+// at most two distinct values (-0.0 and +0.0 count as one, as in the scan's
+// comparisons).
+int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, cudaStream_t st);
 int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st,
                    uint32_t* nan_flag = nullptr);
 int check_problem(const ct_problem* p);

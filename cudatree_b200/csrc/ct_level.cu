@@ -9,6 +9,8 @@
 //   k_split_scan   Gini scan of one piece: per-element class rank via
 //                  __match_any_sync, int64 warp scans of the sum of squared
 //                  counts, fp64 impurity (reference compute_2d, dfs_module.cu:310-443)
+//   k_scan_two_valued  the same result for pieces of two-valued features:
+//                  a search for the node's value boundary instead of a scan
 //   k_split_reduce min-impurity reduction + threshold
 //                  (reference reduce_2d / find_min_imp / get_thresholds)
 //   k_plan         node record, child ids, partition work list
@@ -26,21 +28,6 @@ namespace ct {
 namespace {
 
 constexpr uint32_t SCAN_BATCH = 4;  // rounds of 32 whose loads are issued together
-
-// Candidate queue of the split scan: per warp, in shared memory after the
-// warp's class counts and class totals.
-struct ScanCand {
-  int64_t sl;   // left sum of squared class counts at pos
-  int64_t sr;   // right sum
-  uint32_t pos;
-  float t;      // approximate SL / n_L + SR / n_R
-};
-constexpr uint32_t SCAN_QCAP = 64;
-constexpr float SCAN_KEEP = 1.0f - 1.0f / 262144.0f;  // keep band 1 - 2^-18 (see k_split_scan)
-__host__ __device__ __forceinline__ uint32_t scan_count_words(uint32_t C) { return (2 * C + 1) & ~1u; }
-__host__ __device__ __forceinline__ uint32_t scan_warp_words(uint32_t C) {
-  return scan_count_words(C) + SCAN_QCAP * (uint32_t)(sizeof(ScanCand) / 4);
-}
 
 __device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000000000000ll); }
 
@@ -220,65 +207,113 @@ k_scan_carry(LevelScratch s, uint32_t C) {
 }
 
 // ------------------------------------------------------------------------
-// Exact fp64 score of the queued candidates whose approximate score is within
-// the keep band of the best approximate score; the lane's best is the
-// lexicographic minimum of (score, position).  Warp-collective: the queue is
-// read after a __syncwarp and may be refilled after the next one.
-__device__ __noinline__ void scan_flush(const ScanCand* q, uint32_t qn, float thr, double nn, uint32_t lane,
-                                           double& best, uint32_t& bpos, float& bil, float& bir) {
-  __syncwarp();
-  for (uint32_t i = lane; i < qn; i += 32) {
-    const ScanCand e = q[i];
-    if (!(e.t >= thr)) continue;
-    const double nl = (double)(e.pos + 1);
-    const double nr = __dsub_rn(nn, nl);
-    const double gl = gini_part(e.sl, nl, nn);
-    const double gr = gini_part(e.sr, nr, nn);
-    const double sc = __dadd_rn(gl, gr);
-    if (sc < best || (sc == best && e.pos < bpos)) {
-      best = sc;
-      bpos = e.pos;
-      bil = __double2float_rn(gl);
-      bir = __double2float_rn(gr);
+// Split scan of one piece of a two-valued feature.  In a node's sorted list
+// such a feature is a run of its low value a followed by a run of its high
+// value b, so the only candidate position is the last a (when a + 1e-5 < b:
+// is_candidate, dfs_module.cu:400), and the left class counts there are the
+// piece's carry plus the classes of the piece's entries up to it.  The piece
+// holding that position (x[lo] == a and x[hi] == b, or hi == n) finds it with
+// a 32-way search over x and scores it with the scan's exact arithmetic; the
+// other pieces report no candidate.  Same result as the general scan, with
+// a few gathers per piece instead of one per position.
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_scan_two_valued(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot, LevelScratch s,
+                  uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  const uint32_t C = v.n_classes;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
+  const uint32_t pi = global_warp();
+  const uint32_t lane = lane_id();
+  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
+  const ScanPiece pc = s.pieces[pi];
+  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
+  if (!two_valued(v, f)) return;  // k_split_scan's piece
+  const ct_node nd = nodes[pc.node];
+  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
+  const float* xf = v.x_fm + (size_t)f * v.n_rows;
+  const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
+  PieceBest* out = s.best + pi;
+  const uint32_t n = nd.n;
+  const uint32_t lo = pc.j * scan_piece;
+  const uint32_t hi = min(lo + scan_piece, n);
+  const float a = xf[entry_row(v, lst[0])];
+  const float b = xf[entry_row(v, lst[n - 1])];
+  PieceBest pb;
+  pb.score = dinf();
+  pb.pos = NONE;
+  pb.il = 0.f;
+  pb.ir = 0.f;
+  pb.pad = 0;
+  const bool owns = is_candidate_sorted(a, b) && xf[entry_row(v, lst[lo])] == a &&
+                    (hi == n || xf[entry_row(v, lst[hi])] == b);
+  if (owns) {
+    // last position with x == a in [lo, e), e = min(hi, n - 1): x[L] == a and
+    // x[R] == b throughout; 32 probes of the interior per round
+    uint32_t L = lo, R = min(hi, n - 1);
+    while (R - L > 1) {
+      const uint32_t k = R - L - 1;
+      const uint32_t q = L + 1 + (uint32_t)(((uint64_t)k * lane) / 32u);  // every interior position when k <= 32
+      const unsigned m = __ballot_sync(FULL, xf[entry_row(v, lst[q])] == a);
+      const uint32_t c = __popc(m);  // probes see a on lanes [0, c): the values are sorted
+      const uint32_t ql = __shfl_sync(FULL, q, c > 0 ? c - 1 : 0);
+      const uint32_t qr = __shfl_sync(FULL, q, c < 32 ? c : 31);
+      if (c > 0) L = ql;
+      if (c < 32) R = qr;
     }
+    const uint32_t p = L;
+    // classes of the entries [lo, p]
+    const uint32_t cnt_n = p - lo + 1;
+    for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
+    __syncwarp();
+    if (C <= 8 && cnt_n <= 32 * 255) {
+      uint64_t pk = 0;  // 8-bit field per class, at most 255 entries per lane
+      for (uint32_t i = lo + lane; i <= p; i += 32) pk += 1ull << (8 * entry_label<LabT>(v, (uint32_t)__ldcs(lst + i)));
+      for (uint32_t c = 0; c < C; ++c) {
+        const uint32_t t = warp_sum_u32((uint32_t)(pk >> (8 * c)) & 0xffu);
+        if (lane == 0) cnt[c] = t;
+      }
+    } else {
+      for (uint32_t i0 = lo; i0 <= p; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t c = i <= p ? entry_label<LabT>(v, (uint32_t)__ldcs(lst + i)) : NONE;
+        const unsigned grp = __match_any_sync(FULL, c);
+        if (c != NONE && (grp >> lane) == 1u) cnt[c] += __popc(grp);
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+    int64_t sl = 0, sr = 0;
+    for (uint32_t c = lane; c < C; c += 32) {
+      const int64_t l = (int64_t)cnt[c] + (carry ? carry[c] : 0u);
+      const int64_t r = (int64_t)tot[(size_t)pc.node * C + c] - l;
+      sl += l * l;
+      sr += r * r;
+    }
+    sl = warp_sum_i64(sl);
+    sr = warp_sum_i64(sr);
+    const double nn = (double)n;
+    const double nl = (double)(p + 1);
+    const double nr = __dsub_rn(nn, nl);
+    const double gl = gini_part(sl, nl, nn);
+    const double gr = gini_part(sr, nr, nn);
+    pb.score = __dadd_rn(gl, gr);
+    pb.pos = p;
+    pb.il = __double2float_rn(gl);
+    pb.ir = __double2float_rn(gr);
   }
-  __syncwarp();
+  if (lane == 0) *out = pb;
 }
 
-// Gini scan of one piece of a (node, feature) segment.
-//
-// Per round of 32 positions: the class rank of each position (match over the
-// labels plus the warp's running class counts) gives the exact increments of
-// the left and right sums of squared class counts, 2k + 1 and 1 - 2 (T - k)
-// (the reference's serial recurrence, dfs_module.cu:392-398).  A round with
-// no candidate position (equal or nearly equal neighbouring values,
-// dfs_module.cu:400) only advances the running sums, by two warp reductions.
-// A round with candidates takes inclusive warp scans for the per-position
-// sums SL, SR and scores each candidate approximately in fp32:
-// t = SL / n_L + SR / n_R, the quantity whose maximum is the minimum Gini
-// score (score = 1 - t / n in exact arithmetic).  Only candidates whose t is
-// within the keep band of the largest t seen so far are queued; the queue is
-// scored exactly (fp64, correctly rounded, dfs_module.cu:404-407) when it
-// fills and at the end of the piece, against the final band.
-//
-// Why the result is the exact argmin: t~ (fp32: int64 -> f32 conversions,
-// __fdividef at <= 2 ulp, one add) is within eps = 2^-20 of t relatively.  A
-// candidate q never scored exactly has t~(q) < (1 - 2^-18) t~max, so
-// t(q) < (1 - 2 eps) t(p*) for the position p* of t~max, and its real score
-// exceeds p*'s by more than 2 eps t(p*) / n >= 2 eps / C (t >= n / C by
-// Cauchy-Schwarz), which is > 1.8e-9 for C <= 1024: far beyond the fp64
-// rounding of either score (< 16 * 2^-53).  So q cannot equal or beat p*'s
-// exact score, which is scored; ties among the scored keep the lowest
-// position.
+// ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)
+__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
 k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
              LevelScratch s, uint32_t scan_piece) {
-  extern __shared__ __align__(8) uint32_t smem[];
+  extern __shared__ uint32_t smem[];
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * scan_warp_words(C);
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * C;
   uint32_t* T = cnt + C;
-  ScanCand* q = reinterpret_cast<ScanCand*>(cnt + scan_count_words(C));
   const uint32_t pi = global_warp();
   const uint32_t lane = lane_id();
   if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
@@ -288,6 +323,7 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const float* xf = v.x_fm + (size_t)f * v.n_rows;
   const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
+  if (two_valued(v, f)) return;  // k_scan_two_valued's piece
   int64_t sl = 0, sr = 0;
   for (uint32_t c = lane; c < C; c += 32) {
     const uint32_t k = carry ? carry[c] : 0u;
@@ -309,8 +345,6 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   double best = dinf();
   uint32_t bpos = NONE;
   float bil = 0.f, bir = 0.f;
-  uint32_t tmax = 0;  // bits of the largest approximate t so far (t >= 0: bits order as values)
-  uint32_t qn = 0;    // queued candidates
   const unsigned lt = lanemask_lt();
   // Software pipeline over batches of SCAN_BATCH rounds: while batch b is
   // scanned, the label/value gathers of batch b+1 and the index loads of
@@ -325,8 +359,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
       const uint32_t p = lo + r * 32 + lane;
       rows[r] = p < hi ? (uint32_t)__ldcs(lst + p) : 0u;
-      const uint32_t q2 = p + B;
-      rows_n[r] = q2 < hi ? (uint32_t)__ldcs(lst + q2) : 0u;
+      const uint32_t q = p + B;
+      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
@@ -346,8 +380,8 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
     }
 #pragma unroll
     for (uint32_t r = 0; r < SCAN_BATCH; ++r) {
-      const uint32_t q2 = base + 2 * B + r * 32 + lane;
-      rows_n[r] = q2 < hi ? (uint32_t)__ldcs(lst + q2) : 0u;
+      const uint32_t q = base + 2 * B + r * 32 + lane;
+      rows_n[r] = q < hi ? (uint32_t)__ldcs(lst + q) : 0u;
     }
     const float x_e = __shfl_sync(FULL, xs_n[0], 0);  // first value of the next batch
 #pragma unroll
@@ -360,9 +394,9 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       const float first_next = (r + 1 < SCAN_BATCH) ? __shfl_sync(FULL, xs[r + 1 < SCAN_BATCH ? r + 1 : r], 0) : x_e;
       if (lane == 31) xn = first_next;
       if (valid && p + 1 == hi && p + 1 < n) xn = xf[entry_row(v, lst[p + 1])];  // next piece's first element
-      const bool cand = valid && p + 1 < n && is_candidate_sorted(x, xn);
       const unsigned grp = __match_any_sync(FULL, c);
-      uint32_t k = 0, tc = 0;
+      uint32_t k = 0;
+      int64_t tc = 0;
       if (valid) {
         k = cnt[c] + __popc(grp & lt);
         tc = T[c];
@@ -370,43 +404,37 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       __syncwarp();
       if (valid && (grp >> lane) == 1u) cnt[c] += __popc(grp);
       __syncwarp();
-      int64_t SL, SR;
-      if (narrow) {  // |increments| <= 2n + 1, |partial sums| <= 32 (2n + 1) < 2^31
-        const int32_t dl = valid ? 2 * (int32_t)k + 1 : 0;
-        const int32_t dr = valid ? 1 - 2 * ((int32_t)tc - (int32_t)k) : 0;
-        if (__ballot_sync(FULL, cand) == 0u) {
-          sl += __reduce_add_sync(FULL, dl);
-          sr += __reduce_add_sync(FULL, dr);
-          continue;
-        }
-        const int32_t a = warp_incl_scan_i32(dl), b = warp_incl_scan_i32(dr);
-        SL = sl + a;
-        SR = sr + b;
-        sl += __shfl_sync(FULL, a, 31);
-        sr += __shfl_sync(FULL, b, 31);
+      const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
+      const int64_t dr = valid ? 1 - 2 * (tc - (int64_t)k) : 0;
+      int64_t il, ir, tl, tr;  // inclusive warp prefix and warp total of each increment
+      if (narrow) {  // |partial sums| <= 32 (2n + 1) < 2^31
+        const int32_t a = warp_incl_scan_i32((int32_t)dl), b = warp_incl_scan_i32((int32_t)dr);
+        il = a;
+        ir = b;
+        tl = __shfl_sync(FULL, a, 31);
+        tr = __shfl_sync(FULL, b, 31);
       } else {
-        const int64_t dl = valid ? 2 * (int64_t)k + 1 : 0;
-        const int64_t dr = valid ? 1 - 2 * ((int64_t)tc - (int64_t)k) : 0;
-        const int64_t a = warp_incl_scan_i64(dl), b = warp_incl_scan_i64(dr);
-        SL = sl + a;
-        SR = sr + b;
-        sl += __shfl_sync(FULL, a, 31);
-        sr += __shfl_sync(FULL, b, 31);
+        il = warp_incl_scan_i64(dl);
+        ir = warp_incl_scan_i64(dr);
+        tl = __shfl_sync(FULL, il, 31);
+        tr = __shfl_sync(FULL, ir, 31);
       }
-      float t = 0.f;
-      if (cand) t = __fdividef((float)SL, (float)(p + 1)) + __fdividef((float)SR, (float)(n - p - 1));
-      tmax = max(tmax, __reduce_max_sync(FULL, __float_as_uint(t)));
-      const float thr = __uint_as_float(tmax) * SCAN_KEEP;
-      const bool push = cand && t >= thr;
-      const unsigned pm = __ballot_sync(FULL, push);
-      if (pm) {
-        const uint32_t np = __popc(pm);
-        if (qn + np > SCAN_QCAP) {
-          scan_flush(q, qn, thr, nn, lane, best, bpos, bil, bir);
-          qn = 0;
+      const int64_t SL = sl + il;
+      const int64_t SR = sr + ir;
+      sl += tl;
+      sr += tr;
+      if (valid && p + 1 < n && is_candidate_sorted(x, xn)) {
+        const double nl = (double)(p + 1);
+        const double nr = __dsub_rn(nn, nl);
+        const double gl = gini_part(SL, nl, nn);
+        const double gr = gini_part(SR, nr, nn);
+        const double sc = __dadd_rn(gl, gr);
+        if (sc < best) {
+          best = sc;
+          bpos = p;
+          bil = __double2float_rn(gl);
+          bir = __double2float_rn(gr);
         }
-        if (push) q[qn + __popc(pm & lt)] = ScanCand{SL, SR, p, t};
-        qn += np;
       }
     }
 #pragma unroll
@@ -415,7 +443,6 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
       xs[r] = xs_n[r];
     }
   }
-  scan_flush(q, qn, __uint_as_float(tmax) * SCAN_KEEP, nn, lane, best, bpos, bil, bir);
   warp_argmin2(best, bpos, bil, bir);
   if (lane == 0) {
     PieceBest pb;
@@ -1262,11 +1289,13 @@ void split_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const 
   k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
                                                                                        scan_piece);
   k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
-  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK,
-                             (size_t)WARPS_PER_BLOCK * scan_warp_words(v.n_classes) * sizeof(uint32_t), st>>>(
+  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 2 * sm1, st>>>(
       v, nodes, tot, s, scan_piece);
+  if (v.fbin)
+    k_scan_two_valued<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, tot, s,
+                                                                                              scan_piece);
   pf->end();
-  pf->launched(CT_K_SCAN, 3);
+  pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
   pf->begin(CT_K_REDUCE);
   k_split_reduce<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s);
   pf->end();
@@ -1451,6 +1480,52 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   return w;
 }
 
+namespace {
+// One block per feature: the row's minimum and maximum, then whether every
+// value equals one of them (float equality: -0.0 == +0.0).
+__global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows, uint32_t* bits) {
+  __shared__ float s_mn[32], s_mx[32];
+  const uint32_t f = blockIdx.x;
+  const float* xr = x_fm + (size_t)f * n_rows;
+  float mn = xr[0], mx = xr[0];
+  for (uint32_t i = threadIdx.x; i < n_rows; i += blockDim.x) {
+    const float x = xr[i];
+    mn = fminf(mn, x);
+    mx = fmaxf(mx, x);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fminf(mn, __shfl_xor_sync(FULL, mn, o));
+    mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
+  }
+  if (lane_id() == 0) {
+    s_mn[threadIdx.x >> 5] = mn;
+    s_mx[threadIdx.x >> 5] = mx;
+  }
+  __syncthreads();
+  mn = s_mn[0];
+  mx = s_mx[0];
+  for (uint32_t w = 1; w < blockDim.x / 32; ++w) {
+    mn = fminf(mn, s_mn[w]);
+    mx = fmaxf(mx, s_mx[w]);
+  }
+  bool ok = true;
+  for (uint32_t i = threadIdx.x; i < n_rows && ok; i += blockDim.x) {
+    const float x = xr[i];
+    ok = (x == mn) || (x == mx);
+  }
+  if (!__syncthreads_and(ok)) return;
+  if (threadIdx.x == 0) atomicOr(bits + (f >> 5), 1u << (f & 31));
+}
+}  // namespace
+
+int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, cudaStream_t st) {
+  CT_CUDA_TRY(cudaMemsetAsync(bits, 0, ((n_features + 31) / 32) * sizeof(uint32_t), st));
+  k_feature_flags<<<n_features, 256, 0, st>>>(x_fm, n_rows, bits);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
 Prof* current_prof() {
   static thread_local Prof prof;
   return &prof;
@@ -1475,6 +1550,7 @@ View make_view(const ct_problem* p, const ct_lists* l) {
   v.feistel_h = feistel_half_bits(p->n_features);
   v.row_mask = 0xffffffffu;
   v.lab_shift = 0;
+  v.fbin = nullptr;
   return v;
 }
 

@@ -249,3 +249,40 @@ def test_per_tree_loop_of_hybridforest(cuda_device):
         np.testing.assert_array_equal(a.left_children, b.left_children)
         np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
         np.testing.assert_array_equal(a.values_array, b.values_array)
+
+
+def _two_valued_data(n, c, seed):
+    """Two-valued features of every kind the boundary search meets, beside
+    continuous ones: {0, 1}; {-0.0, +0.0, 3.5} (two values: -0.0 == +0.0);
+    {1, 1 + 4e-6} (never a candidate: closer than 1e-5); {-2, 7.25} tied to
+    the class; and one constant feature."""
+    rng = np.random.default_rng(seed)
+    y = rng.integers(0, c, size=n)
+    x = np.zeros((n, 9), np.float32)
+    x[:, 0] = rng.normal(size=n) + y
+    x[:, 1] = rng.integers(0, 2, n)
+    x[:, 2] = np.where(rng.random(n) < 0.5, np.where(rng.random(n) < 0.5, -0.0, 0.0), 3.5)
+    x[:, 3] = np.where(rng.random(n) < 0.4, 1.0, np.float32(1.0 + 4e-6))
+    x[:, 4] = np.where((y % 2 == 0) ^ (rng.random(n) < 0.1), -2.0, 7.25)
+    x[:, 5] = 4.0
+    x[:, 6] = rng.normal(size=n)
+    x[:, 7] = (rng.random(n) < 0.03).astype(np.float32)
+    x[:, 8] = np.where(y == 0, 1.0, rng.integers(0, 2, n))
+    return x, y
+
+
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+@pytest.mark.parametrize("n,c,piece", [(700, 3, None), (9000, 5, None), (9000, 12, 1024), (70000, 7, 4096)])
+def test_two_valued_features_match_oracle(cuda_device, n, c, piece, mode):
+    """Features with at most two distinct values take the boundary search
+    (k_scan_two_valued) instead of the full scan; single- and multi-piece
+    nodes, byte-packed (C <= 8) and match (C > 8) class counts, uint16 and
+    uint32 entries grow the oracle's trees."""
+    x, y = _two_valued_data(n, c, 17)
+    forest = RandomForestClassifier(n_estimators=3, max_features=4, seed=29, fit_mode=mode)
+    if piece:
+        forest._tuned = {"scan_piece": piece, "subtree_cutoff": 32}
+    forest.fit(x, y, bfs_threshold=2000)
+    ref = O.fit_forest(x, y, n_estimators=3, max_features=4, seed=29)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
