@@ -15,6 +15,8 @@ LIB_PATH = Path(__file__).resolve().parent / "libcudatree_b200.so"
 CT_OK = 0
 CT_FIT_PLAIN = 0
 CT_FIT_BATCHED = 1
+CT_FIT_PROFILE = 1     # ct_fit_options.flags
+CT_FIT_HOST_LOOP = 2
 MAX_CLASSES = 1024
 MAX_FEATURES = 65536
 
@@ -65,7 +67,8 @@ class TreeBuffers(C.Structure):
 
 class FitOptions(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("bfs_threshold", C.c_uint32), ("subtree_cutoff", C.c_uint32),
-                ("scan_piece", C.c_uint32), ("reserved", C.c_uint32 * 4)]
+                ("scan_piece", C.c_uint32), ("flags", C.c_uint32), ("step_nodes", C.c_uint32),
+                ("graph_samples", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class PackedNode(C.Structure):

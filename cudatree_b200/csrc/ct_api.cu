@@ -149,9 +149,9 @@ int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* no
     CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
     s.result = out;
     CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
-    CT_TRY(launch_reset_step(s.ctr, n_nodes, st));
-    CT_TRY(launch_split(v, p->index_bytes, p->label_bytes, nodes, totals, s, LevelBounds{n_nodes, total},
-                        DEFAULT_SCAN_PIECE, st));
+    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, totals, nullptr, nullptr, nullptr, nullptr}, st));
+    CT_TRY(launch_split(v, p->index_bytes, p->label_bytes, s, LevelBounds{n_nodes, total}, DEFAULT_SCAN_PIECE, false,
+                        st));
     if (selected)
       CT_CUDA_TRY(cudaMemcpyAsync(selected, s.sel, (size_t)n_nodes * p->max_features * sizeof(uint32_t),
                                   cudaMemcpyDeviceToDevice, st));
@@ -185,10 +185,10 @@ int ct_partition_nodes(const ct_problem* p, const ct_lists* lists, const ct_node
     CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
     s.result = const_cast<ct_split_result*>(splits);
     CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
-    CT_TRY(launch_reset_step(s.ctr, n_nodes, st));
+    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, nullptr, nullptr, nullptr, nullptr, nullptr}, st));
     TreeView tv;
     std::memset(&tv, 0, sizeof(tv));
-    CT_TRY(launch_partition(v, p->index_bytes, p->label_bytes, nodes, s, LevelBounds{n_nodes, total}, tv, st));
+    CT_TRY(launch_partition(v, p->index_bytes, p->label_bytes, s, LevelBounds{n_nodes, total}, tv, false, st));
     Counters h;
     CT_CUDA_TRY(cudaMemcpyAsync(&h, s.ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
     CT_CUDA_TRY(cudaStreamSynchronize(st));

@@ -30,6 +30,7 @@ int pack_presort(const ct_problem* p, void* out, uint32_t shift, cudaStream_t st
 namespace {
 
 constexpr uint32_t CHUNK_NODES_MAX = 1u << 20;
+constexpr uint64_t DEFAULT_GRAPH_SAMPLES = 1u << 22;
 
 // Class histogram of every slot's in-bag rows: grid (blocks, slots), one
 // shared-memory histogram per block flushed with global atomics.
@@ -109,14 +110,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
   }
 }
 
-__global__ void k_begin_level(Counters* c) {
-  c->n_next = 0;
-  c->next_total = 0;
-  c->small_total = 0;
-  c->split_total = 0;
-  c->scan_elems = 0;
-  c->part_elems = 0;
-}
+__global__ void k_begin_level(Counters* c) { reset_level_counters(c); }
 
 void begin_level(Counters* c, cudaStream_t st) {
   k_begin_level<<<1, 1, 0, st>>>(c);
@@ -134,6 +128,19 @@ void account_level(const ct_problem* p, const View& view, const Counters& h) {
   pf->stats.steps += 1;
 }
 
+// State of the graph-driven level loop (device memory).
+struct LoopCtl {
+  uint32_t cur;      // list holding the current level
+  uint32_t lo;       // first node of the current chunk
+  uint32_t n_level;  // nodes of the current level
+  uint32_t levels;   // levels finished
+  uint32_t steps;    // steps run
+  uint32_t pad[3];
+  unsigned long long scan_elems;   // totals of the finished levels
+  unsigned long long split_total;
+  unsigned long long part_elems;
+};
+
 struct FitLayout {
   uint32_t n_slots;
   uint32_t cap_list;
@@ -141,6 +148,8 @@ struct FitLayout {
   uint32_t scan_piece;
   uint32_t subtree_cut;  // nodes of at most this many rows are grown by warp subtrees (0: off)
   uint32_t cap_small;
+  bool host_loop;        // batched form: per-level host round trips instead of the loop graph
+  uint64_t graph_samples; // batched form: levels of at most this many samples run in the loop graph
   ct_node* small;        // small nodes waiting for their warp subtree (kept across levels)
   mutable uint64_t small_bound;  // upper bound of the entries in small
   uint32_t* n_in;
@@ -149,6 +158,7 @@ struct FitLayout {
   uint32_t* tot[2];
   uint64_t* mask[2];     // constant-feature masks of the lists (batched form, n_features <= 64), else NULL
   LevelScratch s;
+  struct LoopCtl* ctl;   // state of the graph-driven level loop
   void* boot_ws;
   size_t boot_bytes;
   size_t bytes;
@@ -162,11 +172,15 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   const uint64_t cap_list64 = S / 2 + slots + 2;
   L->n_slots = slots;
   L->cap_list = (uint32_t)std::min<uint64_t>(cap_list64, 0xffffffffull);
-  L->chunk = std::min<uint32_t>(L->cap_list, CHUNK_NODES_MAX);
+  L->chunk = std::min<uint32_t>(L->cap_list, o->step_nodes ? o->step_nodes : CHUNK_NODES_MAX);
   L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
   // the warp subtree packs a row id into 27 bits of its sort key
   L->subtree_cut = p->n_rows < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 128u) : 0u;
   L->cap_small = L->subtree_cut ? 2 * L->chunk : 0u;
+  L->host_loop = (o->flags & CT_FIT_HOST_LOOP) != 0;
+  L->graph_samples = o->graph_samples == 0xffffffffu ? UINT64_MAX
+                     : o->graph_samples               ? o->graph_samples
+                                                      : DEFAULT_GRAPH_SAMPLES;
   Arena a{base, size, 0};
   L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
   L->small_bound = 0;
@@ -183,6 +197,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->boot_ws = a.take<char>(L->boot_bytes);
   LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
   carve_level_scratch(a, v, caps, &L->s);
+  L->ctl = a.take<LoopCtl>(1);
   L->bytes = a.used + 256;
   return base != nullptr && a.ok();
 }
@@ -261,11 +276,24 @@ int root(const ct_problem* p, const View& v, const FitLayout& L, uint32_t slot_l
 // (disjoint) ranges.  Deferring them to one launch lets long subtrees overlap.
 int flush_subtrees(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, cudaStream_t st) {
   if (!L.subtree_cut || L.small_bound == 0) return CT_OK;
-  CT_TRY(launch_subtrees(v, p->index_bytes, p->label_bytes, L.small,
-                         (uint32_t)std::min<uint64_t>(L.small_bound, L.cap_small), L.subtree_cut > 32, L.s, tv, st));
+  CT_TRY(launch_subtrees(v, p->index_bytes, p->label_bytes, L.small, L.cap_small,
+                         (uint32_t)std::min<uint64_t>(L.small_bound, L.cap_small), L.subtree_cut > 32, false, L.s, tv,
+                         st));
   CT_CUDA_TRY(cudaMemsetAsync(&L.s.ctr->n_small, 0, sizeof(uint32_t), st));
   L.small_bound = 0;
   return CT_OK;
+}
+
+// The lists of a step over list[cur][lo..): children go to list[1 - cur].
+StepLists step_lists(const FitLayout& L, int cur, uint32_t lo, uint32_t C) {
+  StepLists sl;
+  sl.nodes = L.list[cur] + lo;
+  sl.tot = L.tot[cur] + (size_t)lo * C;
+  sl.node_mask = L.mask[cur] ? L.mask[cur] + lo : nullptr;
+  sl.next = L.list[1 - cur];
+  sl.next_tot = L.tot[1 - cur];
+  sl.next_mask = L.mask[1 - cur];
+  return sl;
 }
 
 // One step over list[cur][0..n) -> children appended to list[1-cur].
@@ -274,18 +302,12 @@ int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView&
   const uint32_t ib = p->index_bytes, lb = p->label_bytes, C = p->n_classes;
   for (uint32_t lo = 0; lo < n; lo += L.chunk) {
     const uint32_t cn = std::min(L.chunk, n - lo);
-    const ct_node* nodes = L.list[cur] + lo;
-    const uint32_t* tot = L.tot[cur] + (size_t)lo * C;
     const LevelBounds b{cn, total};
-    LevelScratch s = L.s;
-    s.node_mask = L.mask[cur] ? L.mask[cur] + lo : nullptr;
-    s.next_mask = L.mask[1 - cur];
     if (L.subtree_cut && L.small_bound + 2ull * cn > L.cap_small) CT_TRY(flush_subtrees(p, v, L, tv, st));
-    CT_TRY(launch_reset_step(L.s.ctr, cn, st));
-    CT_TRY(launch_split(v, ib, lb, nodes, tot, s, b, L.scan_piece, st));
-    CT_TRY(launch_partition(v, ib, lb, nodes, s, b, tv, st));
-    CT_TRY(launch_children(v, ib, lb, nodes, tot, s, b, tv, L.list[1 - cur], L.tot[1 - cur], L.cap_list,
-                           L.subtree_cut, L.small, L.cap_small, st));
+    CT_TRY(launch_reset_step(L.s, cn, step_lists(L, cur, lo, C), st));
+    CT_TRY(launch_split(v, ib, lb, L.s, b, L.scan_piece, false, st));
+    CT_TRY(launch_partition(v, ib, lb, L.s, b, tv, false, st));
+    CT_TRY(launch_children(v, ib, lb, L.s, b, tv, L.cap_list, L.subtree_cut, L.small, L.cap_small, false, st));
     if (L.subtree_cut) L.small_bound += 2ull * cn;
   }
   return CT_OK;
@@ -305,6 +327,255 @@ int level_loop(const ct_problem* p, const View& v, const FitLayout& L, const Tre
     total = h.next_total;
     cur = 1 - cur;
   }
+  return CT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Graph-driven level loop of the batched form.
+//
+// The host-driven loop above reads the step counters after every level to
+// learn the next level's size: the reference's per-level round trip
+// (random_tree.py:428-431).  Here the loop is one CUDA graph: a conditional
+// WHILE node whose body is one step (one chunk of a level), launched
+// persistently (at most the resident blocks; warps loop over the items).  A
+// kernel at the top of the body points the step's lists at the current
+// chunk; one at the bottom advances to the next chunk or, at the end of a
+// level, swaps the list buffers, adds the level's counts to the totals and
+// sets the loop condition to "the next level has nodes" (0 on a device
+// error).  The warp-subtree launches follow the loop in the same graph.  The
+// host launches the graph and synchronizes once.
+struct LoopLists {
+  ct_node* list[2];
+  uint32_t* tot[2];
+  uint64_t* mask[2];
+};
+
+// The level the loop starts with is the last step's children (the roots, or
+// the host-driven levels' last children): n_next nodes in list ctl->cur,
+// which the host sets before launching the graph.
+__global__ void k_loop_init(LoopCtl* ctl, Counters* c, uint32_t cap_list, cudaGraphConditionalHandle h) {
+  const uint32_t n = c->error ? 0u : min(c->n_next, cap_list);
+  ctl->lo = 0;
+  ctl->n_level = n;
+  ctl->levels = 0;
+  ctl->steps = 0;
+  ctl->scan_elems = 0;
+  ctl->split_total = 0;
+  ctl->part_elems = 0;
+  reset_level_counters(c);
+  c->claim[ITEM_SUBTREE] = 0;
+  c->claim[ITEM_SUBTREE_WIDE] = 0;
+  cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+}
+
+__global__ void k_loop_step(LoopCtl* ctl, Counters* c, StepLists* step, LoopLists ll, uint32_t chunk, uint32_t C) {
+  const uint32_t cur = ctl->cur, lo = ctl->lo;
+  reset_step_counters(c, min(chunk, ctl->n_level - lo));
+  StepLists sl;
+  sl.nodes = ll.list[cur] + lo;
+  sl.tot = ll.tot[cur] + (size_t)lo * C;
+  sl.node_mask = ll.mask[cur] ? ll.mask[cur] + lo : nullptr;
+  sl.next = ll.list[cur ^ 1u];
+  sl.next_tot = ll.tot[cur ^ 1u];
+  sl.next_mask = ll.mask[cur ^ 1u];
+  *step = sl;
+}
+
+__global__ void k_loop_end(LoopCtl* ctl, Counters* c, uint32_t chunk, uint32_t cap_list,
+                           cudaGraphConditionalHandle h) {
+  ctl->steps += 1;
+  if (c->error) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
+  if (ctl->lo + chunk < ctl->n_level) {  // more chunks of this level; the condition stays set
+    ctl->lo += chunk;
+    return;
+  }
+  ctl->scan_elems += c->scan_elems;
+  ctl->split_total += c->split_total;
+  ctl->part_elems += c->part_elems;
+  ctl->levels += 1;
+  const uint32_t n = min(c->n_next, cap_list);
+  ctl->n_level = n;
+  ctl->cur ^= 1u;
+  ctl->lo = 0;
+  reset_level_counters(c);
+  cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
+}
+
+// The instantiated loop graph of the last batched fit on this thread, reused
+// while every kernel argument is the same (same problem, workspace, lists and
+// options).
+struct LoopGraph {
+  std::vector<unsigned char> key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = -1;
+  ct_kernel_stats per_step{};  // launches of one body iteration
+  ct_kernel_stats once{};      // launches outside the loop
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+  }
+  ~LoopGraph() { reset(); }
+};
+thread_local LoopGraph t_loop_graph;
+
+template <typename T>
+void key_add(std::vector<unsigned char>& k, const T& v) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), b, b + sizeof(T));
+}
+
+ct_kernel_stats stats_diff(const ct_kernel_stats& a, const ct_kernel_stats& b) {
+  ct_kernel_stats d{};
+  for (int i = 0; i < CT_NUM_KERNEL_GROUPS; ++i) d.launches[i] = a.launches[i] - b.launches[i];
+  d.total_launches = a.total_launches - b.total_launches;
+  return d;
+}
+
+// Capture one batch of launches into graph g (after `dep` when given); the
+// stream capture is always ended, whatever the launches return.
+template <typename F>
+int capture_into(cudaGraph_t g, const cudaGraphNode_t* dep, cudaStream_t st, F launches) {
+  CT_CUDA_TRY(cudaStreamBeginCaptureToGraph(st, g, dep, nullptr, dep ? 1 : 0, cudaStreamCaptureModeRelaxed));
+  const int rc = launches();
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(st, &out);
+  if (rc != CT_OK) return rc;
+  CT_CUDA_TRY(e);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+// Stream the loop graph is captured on: capture cannot start on the legacy
+// default stream, which callers often pass; the graph runs on the caller's.
+cudaStream_t capture_stream() {
+  static thread_local struct Holder {
+    cudaStream_t st = nullptr;
+    ~Holder() {
+      if (st) cudaStreamDestroy(st);
+    }
+  } h;
+  if (!h.st) cudaStreamCreateWithFlags(&h.st, cudaStreamNonBlocking);
+  return h.st;
+}
+
+int build_loop_graph(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, cudaStream_t st,
+                     LoopGraph& lg) {
+  const uint32_t ib = p->index_bytes, lb = p->label_bytes, C = p->n_classes;
+  const LevelBounds b{L.chunk, (uint64_t)L.n_slots * p->n_rows};
+  const LoopLists ll{{L.list[0], L.list[1]}, {L.tot[0], L.tot[1]}, {L.mask[0], L.mask[1]}};
+  Prof* pf = current_prof();
+  CT_CUDA_TRY(cudaGraphCreate(&lg.graph, 0));
+  cudaGraphConditionalHandle h;
+  CT_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, lg.graph, 0, cudaGraphCondAssignDefault));
+  const ct_kernel_stats s0 = pf->stats;
+  CT_TRY(capture_into(lg.graph, nullptr, st, [&]() -> int {
+    k_loop_init<<<1, 1, 0, st>>>(L.ctl, L.s.ctr, L.cap_list, h);
+    pf->launched(CT_K_CHILDREN);
+    return CT_OK;
+  }));
+  cudaGraphNode_t init = nullptr;
+  size_t n_nodes = 1;
+  CT_CUDA_TRY(cudaGraphGetNodes(lg.graph, &init, &n_nodes));
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t loop = nullptr;
+  CT_CUDA_TRY(cudaGraphAddNode(&loop, lg.graph, &init, 1, &cp));
+  const ct_kernel_stats s1 = pf->stats;
+  CT_TRY(capture_into(cp.conditional.phGraph_out[0], nullptr, st, [&]() -> int {
+    k_loop_step<<<1, 1, 0, st>>>(L.ctl, L.s.ctr, L.s.step, ll, L.chunk, C);
+    pf->launched(CT_K_CHILDREN);
+    CT_TRY(launch_split(v, ib, lb, L.s, b, L.scan_piece, true, st));
+    CT_TRY(launch_partition(v, ib, lb, L.s, b, tv, true, st));
+    CT_TRY(launch_children(v, ib, lb, L.s, b, tv, L.cap_list, L.subtree_cut, L.small, L.cap_small, true, st));
+    k_loop_end<<<1, 1, 0, st>>>(L.ctl, L.s.ctr, L.chunk, L.cap_list, h);
+    pf->launched(CT_K_CHILDREN);
+    return CT_OK;
+  }));
+  const ct_kernel_stats s2 = pf->stats;
+  CT_TRY(capture_into(lg.graph, &loop, st, [&]() -> int {
+    return launch_subtrees(v, ib, lb, L.small, L.cap_small, L.cap_small, L.subtree_cut > 32, true, L.s, tv, st);
+  }));
+  const ct_kernel_stats s3 = pf->stats;
+  lg.per_step = stats_diff(s2, s1);
+  lg.once = stats_diff(s1, s0);
+  const ct_kernel_stats tail = stats_diff(s3, s2);
+  for (int i = 0; i < CT_NUM_KERNEL_GROUPS; ++i) lg.once.launches[i] += tail.launches[i];
+  lg.once.total_launches += tail.total_launches;
+  pf->stats = s0;  // the capture launched nothing; executions are counted after they run
+  CT_CUDA_TRY(cudaGraphInstantiate(&lg.exec, lg.graph, 0));
+  return CT_OK;
+}
+
+// Level loop + warp subtrees of a batched fit as one graph launch, from the
+// level of list `cur` on.
+int graph_level_loop(const ct_problem* p, const View& v, const FitLayout& L, const TreeView& tv, int cur,
+                     cudaStream_t st) {
+  std::vector<unsigned char> key;
+  int dev = -1;
+  CT_CUDA_TRY(cudaGetDevice(&dev));
+  key_add(key, dev);
+  key_add(key, v);
+  key_add(key, L.s);
+  key_add(key, tv);
+  key_add(key, *p);
+  for (int i = 0; i < 2; ++i) {
+    key_add(key, L.list[i]);
+    key_add(key, L.tot[i]);
+    key_add(key, L.mask[i]);
+  }
+  key_add(key, L.ctl);
+  key_add(key, L.small);
+  key_add(key, L.cap_small);
+  key_add(key, L.cap_list);
+  key_add(key, L.chunk);
+  key_add(key, L.n_slots);
+  key_add(key, L.scan_piece);
+  key_add(key, L.subtree_cut);
+  LoopGraph& lg = t_loop_graph;
+  if (!lg.exec || lg.key != key) {
+    lg.reset();
+    cudaStream_t cs = capture_stream();
+    if (!cs) {
+      set_last_error("could not create the loop graph's capture stream");
+      return CT_ERR_CUDA;
+    }
+    const int rc = build_loop_graph(p, v, L, tv, cs, lg);
+    if (rc != CT_OK) {
+      lg.reset();
+      return rc;
+    }
+    lg.key = key;
+    lg.device = dev;
+  }
+  // the loop starts from list `cur` (k_loop_init keeps ctl->cur)
+  CT_CUDA_TRY(cudaMemsetAsync(&L.ctl->cur, 0, sizeof(uint32_t), st));
+  if (cur) CT_CUDA_TRY(cudaMemsetAsync(&L.ctl->cur, 1, 1, st));
+  CT_CUDA_TRY(cudaGraphLaunch(lg.exec, st));
+  LoopCtl ctl;
+  Counters h;
+  CT_CUDA_TRY(cudaMemcpyAsync(&ctl, L.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, st));
+  CT_TRY(read_counters(L, &h, st));
+  Prof* pf = current_prof();
+  for (int i = 0; i < CT_NUM_KERNEL_GROUPS; ++i)
+    pf->stats.launches[i] += lg.once.launches[i] + (uint64_t)ctl.steps * lg.per_step.launches[i];
+  pf->stats.total_launches += lg.once.total_launches + (uint64_t)ctl.steps * lg.per_step.total_launches;
+  Counters tot{};
+  tot.scan_elems = ctl.scan_elems;
+  tot.split_total = ctl.split_total;
+  tot.part_elems = ctl.part_elems;
+  const uint64_t steps = pf->stats.steps;
+  account_level(p, v, tot);
+  pf->stats.steps = steps + ctl.levels;
   return CT_OK;
 }
 
@@ -372,6 +643,31 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
   begin_level(L.s.ctr, st);
   CT_TRY(root(p, v, L, 0, n_trees, first_tree, tv, 0, st));
   Counters h;
+  if (!current_prof()->timing && !L.host_loop) {
+    // Levels holding more than graph_samples samples run from the host (their
+    // kernels dwarf a round trip; one warp per item); the rest, and the
+    // subtrees, run as the loop graph.
+    uint32_t n = 0;
+    uint64_t total = 0;
+    if (L.graph_samples != UINT64_MAX) {
+      CT_TRY(read_counters(L, &h, st));
+      n = h.n_next;
+      total = h.next_total;
+    }
+    int cur = 0;
+    while (n > 0 && total > L.graph_samples) {
+      begin_level(L.s.ctr, st);
+      CT_TRY(step(p, v, L, tv, cur, n, total, st));
+      CT_TRY(read_counters(L, &h, st));
+      account_level(p, v, h);
+      if (L.subtree_cut) L.small_bound = h.n_small;
+      n = h.n_next;
+      total = h.next_total;
+      cur = 1 - cur;
+    }
+    return graph_level_loop(p, v, L, tv, cur, st);
+  }
+  // host-driven: per-level CUDA-event timing (profiled fits) needs the levels as separate launches
   CT_TRY(read_counters(L, &h, st));
   CT_TRY(level_loop(p, v, L, tv, 0, h.n_next, h.next_total, st));
   if (L.small_bound) {
@@ -584,7 +880,7 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
   Prof* pf = current_prof();
   pf->finish();
   pf->stats = ct_kernel_stats{};
-  pf->timing = (o->reserved[0] & 1u) != 0;
+  pf->timing = (o->flags & CT_FIT_PROFILE) != 0;
   pf->st = st;
   const int rc = (o->mode == CT_FIT_PLAIN) ? fit_plain(p, l, first_tree, n_trees, o, L, trees, st)
                                            : fit_batched(p, l, first_tree, n_trees, L, trees, st);

@@ -99,12 +99,44 @@ struct Counters {
   uint32_t n_big_segs;
   uint32_t n_tiles;       // partition tiles of big splits
   uint32_t pad[3];
+  uint32_t claim[16];     // item counters of persistent launches (ITEM_* slots)
   unsigned long long next_total;
   unsigned long long small_total;
   unsigned long long split_total;  // samples in nodes partitioned this level
   unsigned long long scan_elems;   // (node, feature) elements scanned this level
   unsigned long long part_elems;   // (node, feature) elements partitioned this level
 };
+
+// Counters of one step, zeroed at its start (n_nodes set); the level totals
+// (n_next, next_total, small_total, split_total, scan_elems, part_elems) are
+// zeroed once per level by reset_level_counters.
+// Slots of Counters::claim.  The subtree slots are zeroed by a fit's start
+// and its loop graph, not per step (subtrees run after the level loop).
+enum : uint32_t {
+  ITEM_SELECT, ITEM_HIST, ITEM_CARRY, ITEM_SCAN, ITEM_TWO_VALUED, ITEM_REDUCE, ITEM_PLAN, ITEM_FILL,
+  ITEM_CHILDREN, ITEM_STEP_SLOTS, ITEM_SUBTREE = ITEM_STEP_SLOTS, ITEM_SUBTREE_WIDE
+};
+__device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_nodes) {
+  for (uint32_t i = 0; i < ITEM_STEP_SLOTS; ++i) c->claim[i] = 0;
+  c->n_nodes = n_nodes;
+  c->n_scan_pieces = 0;
+  c->n_carry = 0;
+  c->n_splits = 0;
+  c->n_part_pieces = 0;
+  c->n_status = 0;
+  c->ticket = 0;
+  c->n_small_segs = 0;
+  c->n_big_segs = 0;
+  c->n_tiles = 0;
+}
+__device__ __forceinline__ void reset_level_counters(Counters* c) {
+  c->n_next = 0;
+  c->next_total = 0;
+  c->small_total = 0;
+  c->split_total = 0;
+  c->scan_elems = 0;
+  c->part_elems = 0;
+}
 
 // One stable-partition segment: a node range in every feature list.
 struct PartSeg {
@@ -230,6 +262,19 @@ struct TreeView {
   uint32_t enabled;
 };
 
+// The node lists of one level step, in device memory: written by the step's
+// first kernel (k_reset_step, or the graph-driven loop's step kernel) and
+// read by every later kernel of the step, so the step's launches do not
+// depend on which buffer holds the level or where its chunk starts.
+struct StepLists {
+  const ct_node* nodes;       // the step's nodes
+  const uint32_t* tot;        // their class totals [n][n_classes]
+  const uint64_t* node_mask;  // their constant-feature masks, or NULL (see LevelScratch)
+  ct_node* next;              // the next level's list: children are appended
+  uint32_t* next_tot;         // their class totals
+  uint64_t* next_mask;        // their masks, or NULL
+};
+
 // Scratch of one level step, carved from the caller's workspace.
 struct LevelScratch {
   uint32_t cap_nodes;
@@ -253,13 +298,12 @@ struct LevelScratch {
   PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
-  // Constant-feature masks of a batched fit (n_features <= 64), else NULL:
-  // bit f of node_mask[i] says that feature f is constant in node i of the
-  // step, so its lists are not partitioned and k_select does not read them;
-  // k_children writes the next list's masks to next_mask.  Feature 0 is never
-  // in a mask (leaf labels and subtrees read its lists).
-  const uint64_t* node_mask = nullptr;
-  uint64_t* next_mask = nullptr;
+  // The step's lists.  Constant-feature masks exist in a batched fit with
+  // n_features <= 64: bit f of node_mask[i] says that feature f is constant
+  // in node i of the step, so its lists are not partitioned and k_select
+  // does not read them; k_children writes the next list's masks.  Feature 0
+  // is never in a mask (leaf labels and subtrees read its lists).
+  StepLists* step;
 };
 __device__ __forceinline__ bool masked(uint64_t m, uint32_t f) { return f < 64 && ((m >> f) & 1u); }
 
@@ -342,29 +386,41 @@ LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b);
 bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s);
 size_t level_scratch_bytes(const View& v, const LevelCaps& c);
 
-// Level-step launches (ct_level.cu).  Node count of the chunk is in
-// s.ctr->n_nodes (device) and bounded by b.nodes.
-int launch_split(const View& v, uint32_t index_bytes, uint32_t label_bytes, const ct_node* nodes,
-                 const uint32_t* tot, const LevelScratch& s, LevelBounds b, uint32_t scan_piece,
-                 cudaStream_t st);
-int launch_partition(const View& v, uint32_t index_bytes, uint32_t label_bytes,
-                     const ct_node* nodes, const LevelScratch& s, LevelBounds b,
-                     const TreeView& tv, cudaStream_t st);
-int launch_children(const View& v, uint32_t index_bytes, uint32_t label_bytes, const ct_node* nodes,
-                    const uint32_t* tot, const LevelScratch& s, LevelBounds b, const TreeView& tv,
-                    ct_node* next, uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut,
-                    ct_node* small, uint32_t cap_small, cudaStream_t st);
-// Warp subtrees of the small nodes the children step set aside (at most
-// cap_small of them); wide: some may have 33..128 rows.
+// Level-step launches (ct_level.cu).  The step's node count is in
+// s.ctr->n_nodes and its lists in *s.step (both on the device, set by the
+// step's reset kernel); b bounds the step (nodes, samples) and sizes the
+// grids.  Every warp-per-item kernel loops over its items, so with
+// `persistent` a launch takes at most the blocks resident at once: a
+// graph-driven loop, whose launches are fixed at capture, passes the
+// workspace's bounds.
+int launch_split(const View& v, uint32_t index_bytes, uint32_t label_bytes, const LevelScratch& s, LevelBounds b,
+                 uint32_t scan_piece, bool persistent, cudaStream_t st);
+int launch_partition(const View& v, uint32_t index_bytes, uint32_t label_bytes, const LevelScratch& s,
+                     LevelBounds b, const TreeView& tv, bool persistent, cudaStream_t st);
+// Children of the step's splits: appended to the next list (at most
+// cap_next) or, when they have at most small_cut rows, to the subtree list
+// while it has room (cap_small); a child that finds the subtree list full
+// goes to the next list (the level steps grow the same subtrees).
+int launch_children(const View& v, uint32_t index_bytes, uint32_t label_bytes, const LevelScratch& s,
+                    LevelBounds b, const TreeView& tv, uint32_t cap_next, uint32_t small_cut, ct_node* small,
+                    uint32_t cap_small, bool persistent, cudaStream_t st);
+// Warp subtrees of the small nodes the children steps set aside (the count
+// is s.ctr->n_small, at most cap_small; the grid covers `bound` of them and
+// loops over the rest); wide: some may have 33..128 rows.
 int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
-                    bool wide, const LevelScratch& s, const TreeView& tv, cudaStream_t st);
+                    uint32_t bound, bool wide, bool persistent, const LevelScratch& s, const TreeView& tv,
+                    cudaStream_t st);
 // Stable partition of segments (ct_partition.cu).
 int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
                          cudaStream_t st);
 PartWork level_part_work(const View& v, const LevelScratch& s);
 
-// Counter resets between steps (device-side, stream ordered).
-int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st);
+// Start of a step (device-side, stream ordered): per-step counters reset,
+// n_nodes and the step's lists set.
+int launch_reset_step(const LevelScratch& s, uint32_t n_nodes, const StepLists& lists, cudaStream_t st);
+// Blocks of a warp-per-item launch: one warp per item, at most grid_cap
+// blocks (0: no cap).
+uint32_t item_blocks(uint64_t warps, uint32_t grid_cap);
 
 View make_view(const ct_problem* p, const ct_lists* l);
 // Bits of a row id when a row id and a label fit one list entry together

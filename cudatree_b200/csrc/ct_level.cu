@@ -19,6 +19,7 @@
 //                  mark table here, the kernels in ct_partition.cu
 //                  (reference scan_reshuffle, dfs_module.cu:224-307)
 //   k_children     child records for the next step
+#include <algorithm>
 #include <cfloat>
 
 #include "ct_internal.cuh"
@@ -33,6 +34,25 @@ __device__ __forceinline__ double dinf() { return __longlong_as_double(0x7ff0000
 
 __device__ __forceinline__ uint32_t global_warp() {
   return (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+}
+__device__ __forceinline__ uint32_t total_warps() { return (gridDim.x * blockDim.x) >> 5; }
+
+// Items of a warp-per-item launch.  A warp takes item global_warp() first;
+// when the grid does not cover every item (a persistent launch), it then
+// claims the items past the grid in order from a counter, so uneven items
+// balance as they do with one warp per item.  Warp-collective.
+template <typename F>
+__device__ __forceinline__ void for_items(uint32_t count, uint32_t* claim, F item) {
+  const uint32_t nw = total_warps();
+  uint32_t w = global_warp();
+  while (w < count) {
+    item(w);
+    __syncwarp();
+    if (nw >= count) break;
+    uint32_t k = 0;
+    if (lane_id() == 0) k = atomicAdd(claim, 1u);
+    w = nw + __shfl_sync(FULL, k, 0);
+  }
 }
 
 __device__ __forceinline__ uint32_t read_error(const Counters* c) {
@@ -63,14 +83,12 @@ __device__ __forceinline__ void warp_argmin2(double& score, uint32_t& pos, float
 
 // ------------------------------------------------------------------------
 template <typename IdxT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t scan_piece) {
-  const uint32_t w = global_warp();
+__device__ __forceinline__ void select_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                            uint32_t scan_piece, uint32_t w) {
   const uint32_t lane = lane_id();
-  if (w >= min(s.ctr->n_nodes, s.cap_nodes)) return;
-  const ct_node nd = nodes[w];
+  const ct_node nd = lists.nodes[w];
   const uint32_t m = v.max_features;
-  const uint64_t cmask = s.node_mask ? s.node_mask[w] : 0ull;  // constant features (lists not current)
+  const uint64_t cmask = lists.node_mask ? lists.node_mask[w] : 0ull;  // constant features (lists not current)
   uint32_t taken = 0;
   if (nd.n >= 2) {
     for (uint32_t i0 = 0; i0 < v.n_features && taken < m; i0 += 32) {
@@ -123,19 +141,22 @@ k_select(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t sca
   }
 }
 
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_select(View v, LevelScratch s, uint32_t scan_piece) {
+  const uint32_t count = min(s.ctr->n_nodes, s.cap_nodes);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_SELECT], [&](uint32_t w) { select_item<IdxT>(v, sl, s, scan_piece, w); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t scan_piece) {
-  extern __shared__ uint32_t smem[];
+__device__ __forceinline__ void scan_hist_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                               uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
-  const uint32_t pi = global_warp();
   const uint32_t lane = lane_id();
-  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
   const ScanPiece pc = s.pieces[pi];
   if (pc.npieces <= 1 || pc.j + 1 == pc.npieces) return;
-  const ct_node nd = nodes[pc.node];
+  const ct_node nd = lists.nodes[pc.node];
   const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const uint32_t lo = pc.j * scan_piece;
@@ -185,11 +206,18 @@ k_scan_hist(View v, const ct_node* __restrict__ nodes, LevelScratch s, uint32_t 
   for (uint32_t c = lane; c < C; c += 32) out[c] = cnt[c];
 }
 
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_scan_carry(LevelScratch s, uint32_t C) {
-  const uint32_t pi = global_warp();
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_hist(View v, LevelScratch s, uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
+  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_HIST],
+            [&](uint32_t pi) { scan_hist_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+}
+
+__device__ __forceinline__ void scan_carry_item(const LevelScratch& s, uint32_t C, uint32_t pi) {
   const uint32_t lane = lane_id();
-  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
   const ScanPiece pc = s.pieces[pi];
   if (pc.npieces <= 1 || pc.j != 0) return;
   // per class, an exclusive prefix over the segment's pieces, 32 pieces per round
@@ -206,6 +234,11 @@ k_scan_carry(LevelScratch s, uint32_t C) {
   }
 }
 
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_carry(LevelScratch s, uint32_t C) {
+  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  for_items(count, &s.ctr->claim[ITEM_CARRY], [&](uint32_t pi) { scan_carry_item(s, C, pi); });
+}
+
 // ------------------------------------------------------------------------
 // Split scan of one piece of a two-valued feature.  In a node's sorted list
 // such a feature is a run of its low value a followed by a run of its high
@@ -217,19 +250,15 @@ k_scan_carry(LevelScratch s, uint32_t C) {
 // other pieces report no candidate.  Same result as the general scan, with
 // a few gathers per piece instead of one per position.
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_scan_two_valued(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot, LevelScratch s,
-                  uint32_t scan_piece) {
-  extern __shared__ uint32_t smem[];
+__device__ __forceinline__ void two_valued_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                                uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
-  const uint32_t pi = global_warp();
+  const uint32_t* tot = lists.tot;
   const uint32_t lane = lane_id();
-  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
   const ScanPiece pc = s.pieces[pi];
   const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
   if (!two_valued(v, f)) return;  // k_split_scan's piece
-  const ct_node nd = nodes[pc.node];
+  const ct_node nd = lists.nodes[pc.node];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const float* xf = v.x_fm + (size_t)f * v.n_rows;
   const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
@@ -305,25 +334,31 @@ k_scan_two_valued(View v, const ct_node* __restrict__ nodes, const uint32_t* __r
   if (lane == 0) *out = pb;
 }
 
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_two_valued(View v, LevelScratch s, uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
+  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_TWO_VALUED],
+            [&](uint32_t pi) { two_valued_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
-k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
-             LevelScratch s, uint32_t scan_piece) {
-  extern __shared__ uint32_t smem[];
+__device__ __forceinline__ void split_scan_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                                uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * C;
+  const uint32_t* tot = lists.tot;
   uint32_t* T = cnt + C;
-  const uint32_t pi = global_warp();
   const uint32_t lane = lane_id();
-  if (pi >= live_count(s, s.ctr->n_scan_pieces, s.cap_scan)) return;
   const ScanPiece pc = s.pieces[pi];
-  const ct_node nd = nodes[pc.node];
   const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
+  if (two_valued(v, f)) return;  // k_scan_two_valued's piece
+  const ct_node nd = lists.nodes[pc.node];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const float* xf = v.x_fm + (size_t)f * v.n_rows;
   const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
-  if (two_valued(v, f)) return;  // k_scan_two_valued's piece
   int64_t sl = 0, sr = 0;
   for (uint32_t c = lane; c < C; c += 32) {
     const uint32_t k = carry ? carry[c] : 0u;
@@ -455,13 +490,22 @@ k_split_scan(View v, const ct_node* __restrict__ nodes, const uint32_t* __restri
   }
 }
 
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
+k_split_scan(View v, LevelScratch s, uint32_t scan_piece) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * v.n_classes;
+  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_SCAN],
+            [&](uint32_t pi) { split_scan_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_split_reduce(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
-  const uint32_t w = global_warp();
+__device__ __forceinline__ void split_reduce_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                                  uint32_t w) {
   const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_nodes, s.cap_nodes)) return;
   const uint32_t base = s.piece_base[w];
   const uint32_t cnt = s.piece_cnt[w];
   const uint32_t m = v.max_features;
@@ -484,7 +528,7 @@ k_split_reduce(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
     ct_split_result r;
     r.n_selected = s.nsel[w];
     if (best < dinf()) {
-      const ct_node nd = nodes[w];
+      const ct_node nd = lists.nodes[w];
       const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, bf) + nd.start;
       const float* xf = v.x_fm + (size_t)bf * v.n_rows;
       r.score = best;
@@ -505,14 +549,19 @@ k_split_reduce(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
   }
 }
 
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_split_reduce(View v, LevelScratch s) {
+  const uint32_t count = live_count(s, s.ctr->n_nodes, s.cap_nodes);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_REDUCE], [&](uint32_t w) { split_reduce_item<IdxT>(v, sl, s, w); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
-  const uint32_t w = global_warp();
+__device__ __forceinline__ void plan_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                          const TreeView& tv, uint32_t w) {
   const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_nodes, s.cap_nodes)) return;
-  const ct_node nd = nodes[w];
+  const ct_node nd = lists.nodes[w];
   const ct_split_result r = s.result[w];
   uint32_t split = r.feature != NONE;
   uint32_t children = 0;
@@ -551,7 +600,7 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
     atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
-    const uint64_t skip = s.node_mask ? s.node_mask[w] : 0ull;
+    const uint64_t skip = lists.node_mask ? lists.node_mask[w] : 0ull;
     atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * (v.n_features - (uint32_t)__popcll(skip)));
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
     if (big) {
@@ -580,7 +629,7 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
       sg.n = nd.n;
       sg.nl = r.pos + 1;
       sg.status = tbase;
-      sg.skip = s.node_mask ? s.node_mask[w] : 0ull;
+      sg.skip = lists.node_mask ? lists.node_mask[w] : 0ull;
       (big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
@@ -609,19 +658,22 @@ k_plan(View v, const ct_node* __restrict__ nodes, LevelScratch s, TreeView tv) {
   }
 }
 
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_plan(View v, LevelScratch s, TreeView tv) {
+  const uint32_t count = live_count(s, s.ctr->n_nodes, s.cap_nodes);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_PLAN], [&](uint32_t w) { plan_item<IdxT, LabT>(v, sl, s, tv, w); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
-  extern __shared__ uint32_t smem[];
+__device__ __forceinline__ void fill_mark_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                               uint32_t* cnt, uint32_t pi) {
   const uint32_t C = v.n_classes;
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * C;
-  const uint32_t pi = global_warp();
   const uint32_t lane = lane_id();
-  if (pi >= live_count(s, s.ctr->n_part_pieces, s.cap_part)) return;
   const PartPiece pp = s.part[pi];
   const SplitRec sr = s.splits[pp.split];
-  const ct_node nd = nodes[sr.node];
+  const ct_node nd = lists.nodes[sr.node];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, sr.feature) + nd.start;
   uint32_t* bw = v.bits + (size_t)nd.slot * v.bit_words;
   for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
@@ -662,17 +714,26 @@ k_fill_mark(View v, const ct_node* __restrict__ nodes, LevelScratch s) {
     if (cnt[c]) atomicAdd(&out[c], cnt[c]);
 }
 
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_fill_mark(View v, LevelScratch s) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
+  const uint32_t count = live_count(s, s.ctr->n_part_pieces, s.cap_part);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_FILL], [&](uint32_t pi) { fill_mark_item<IdxT, LabT>(v, sl, s, cnt, pi); });
+}
+
 // ------------------------------------------------------------------------
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict__ tot,
-           LevelScratch s, TreeView tv, ct_node* next, uint32_t* next_tot, uint32_t cap_next,
-           uint32_t small_cut, ct_node* small, uint32_t cap_small) {
-  const uint32_t w = global_warp();
+__device__ __forceinline__ void children_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                              const TreeView& tv, uint32_t cap_next, uint32_t small_cut,
+                                              ct_node* small, uint32_t cap_small, uint32_t w) {
   const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_splits, s.cap_nodes)) return;
+  const uint32_t* tot = lists.tot;
+  ct_node* next = lists.next;
+  uint32_t* next_tot = lists.next_tot;
   const SplitRec sr = s.splits[w];
-  const ct_node nd = nodes[sr.node];
+  const ct_node nd = lists.nodes[sr.node];
   const ct_split_result r = s.result[sr.node];
   const uint32_t nl = sr.pos + 1;
   const uint32_t C = v.n_classes;
@@ -699,16 +760,17 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
       continue;
     }
     if (small_cut != 0 && ch.n <= small_cut) {
+      uint32_t placed = 0;
       if (lane == 0) {
         const uint32_t idx = atomicAdd(&s.ctr->n_small, 1u);
         if (idx < cap_small) {
           small[idx] = ch;
           atomicAdd(&s.ctr->small_total, (unsigned long long)ch.n);
-        } else {
-          atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+          placed = 1;
         }
       }
-      continue;
+      if (__shfl_sync(FULL, placed, 0)) continue;
+      // the subtree list is full: the level steps split this child
     }
     uint32_t idx = 0;
     if (lane == 0) {
@@ -726,11 +788,11 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
       const uint32_t left = s.split_left[(size_t)w * C + c];
       next_tot[(size_t)idx * C + c] = side ? tot[(size_t)sr.node * C + c] - left : left;
     }
-    if (s.next_mask) {
+    if (lists.next_mask) {
       // the child's constant features: the parent's, and those whose values
       // agree at the child's first and last positions (the child's lists of
       // the others were just partitioned)
-      const uint64_t pm = s.node_mask[sr.node];
+      const uint64_t pm = lists.node_mask[sr.node];
       uint64_t cm = pm;
       for (uint32_t f0 = 0; f0 < v.n_features; f0 += 32) {
         const uint32_t f = f0 + lane;
@@ -742,9 +804,20 @@ k_children(View v, const ct_node* __restrict__ nodes, const uint32_t* __restrict
         }
         cm |= (uint64_t)__ballot_sync(FULL, cst) << f0;
       }
-      if (lane == 0) s.next_mask[idx] = cm;
+      if (lane == 0) lists.next_mask[idx] = cm;
     }
   }
+}
+
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK)
+k_children(View v, LevelScratch s, TreeView tv, uint32_t cap_next, uint32_t small_cut, ct_node* small,
+           uint32_t cap_small) {
+  const uint32_t count = live_count(s, s.ctr->n_splits, s.cap_nodes);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_CHILDREN], [&](uint32_t w) {
+    children_item<IdxT, LabT>(v, sl, s, tv, cap_next, small_cut, small, cap_small, w);
+  });
 }
 
 // ------------------------------------------------------------------------
@@ -1221,98 +1294,106 @@ __device__ void grow_wide(const View& v, const LevelScratch& s, const TreeView& 
 
 
 
-// Subtree roots of at most 32 rows (the others return at once).
+// Subtree roots of at most 32 rows (the others are skipped).
 template <typename IdxT, typename LabT>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK)
 k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
   __shared__ SubEntry stack_all[WARPS_PER_BLOCK][33];
-  const uint32_t w = global_warp();
   const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
-  const ct_node nd = small[w];
-  if (nd.n > 32) return;
-  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
-  const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
-  const bool have = lane < nd.n;
-  const uint32_t e = have ? (uint32_t)l0[lane] : 0u;
-  const uint32_t row = have ? entry_row(v, e) : 0u;
-  const uint32_t lab = have ? entry_label<LabT>(v, e) : NONE;
-  const SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
-  grow_small<IdxT, LabT>(v, s, tv, nd.slot + tv.slot_base, toff, row, lab, cur, stack_all[threadIdx.x >> 5], lane);
+  const uint32_t count = live_count(s, s.ctr->n_small, cap_small);
+  for_items(count, &s.ctr->claim[ITEM_SUBTREE], [&](uint32_t w) {
+    const ct_node nd = small[w];
+    if (nd.n > 32) return;
+    const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+    const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
+    const bool have = lane < nd.n;
+    const uint32_t e = have ? (uint32_t)l0[lane] : 0u;
+    const uint32_t row = have ? entry_row(v, e) : 0u;
+    const uint32_t lab = have ? entry_label<LabT>(v, e) : NONE;
+    const SubEntry cur{nd.n >= 32 ? FULL : ((1u << nd.n) - 1u), nd.raw_id, nd.key};
+    grow_small<IdxT, LabT>(v, s, tv, nd.slot + tv.slot_base, toff, row, lab, cur, stack_all[threadIdx.x >> 5],
+                           lane);
+  });
 }
 
-// Subtree roots of 33..128 rows (the others return at once).
+// Subtree roots of 33..128 rows (the others are skipped).
 template <typename IdxT, typename LabT>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK)
 k_subtree_wide(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
   extern __shared__ __align__(16) uint32_t sub_smem[];
-  const uint32_t w = global_warp();
   const uint32_t lane = lane_id();
-  if (w >= live_count(s, s.ctr->n_small, cap_small)) return;
-  const ct_node nd = small[w];
-  if (nd.n <= 32) return;
+  const uint32_t count = live_count(s, s.ctr->n_small, cap_small);
   uint32_t* wsm = sub_smem + (threadIdx.x >> 5) * subtree_warp_words(v.n_classes);
-  const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
-  grow_wide<IdxT, LabT>(v, s, tv, nd, toff, wsm, lane);
+  for_items(count, &s.ctr->claim[ITEM_SUBTREE_WIDE], [&](uint32_t w) {
+    const ct_node nd = small[w];
+    if (nd.n <= 32) return;
+    const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
+    grow_wide<IdxT, LabT>(v, s, tv, nd, toff, wsm, lane);
+  });
 }
 
-__global__ void k_reset_step(Counters* c, uint32_t n_nodes) {
-  c->n_nodes = n_nodes;
-  c->n_scan_pieces = 0;
-  c->n_carry = 0;
-  c->n_splits = 0;
-  c->n_part_pieces = 0;
-  c->n_status = 0;
-  c->ticket = 0;
-  c->n_small_segs = 0;
-  c->n_big_segs = 0;
-  c->n_tiles = 0;
-}
-
-inline uint32_t blocks_for_warps(uint64_t warps) {
-  uint64_t b = (warps + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
-  return (uint32_t)(b == 0 ? 1 : b);
+__global__ void k_reset_step(Counters* c, uint32_t n_nodes, StepLists* step, StepLists lists) {
+  reset_step_counters(c, n_nodes);
+  *step = lists;
 }
 
 inline uint32_t clamp32(uint64_t x) { return x > 0xffffffffull ? 0xffffffffu : (uint32_t)x; }
 
+// Blocks of a warp-per-item launch: one warp per item, or, for a launch that
+// must not depend on the item count (persistent), at most the blocks that
+// are resident at once, whose warps then loop over the items.
+template <typename K>
+uint32_t grid_for(K kernel, uint64_t warps, size_t smem, bool persistent) {
+  uint32_t cap = 0;
+  if (persistent) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, THREADS_PER_BLOCK, smem);
+    cap = (uint32_t)std::max(1, sms) * (uint32_t)std::max(1, per);
+  }
+  return item_blocks(warps, cap);
+}
+
 template <typename IdxT, typename LabT>
-void split_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const LevelScratch& s,
-                const LevelCaps& caps, uint32_t scan_piece, cudaStream_t st) {
+void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uint32_t scan_piece, bool persistent,
+                cudaStream_t st) {
   Prof* pf = current_prof();
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
   pf->begin(CT_K_SELECT);
-  k_select<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, scan_piece);
+  k_select<IdxT><<<grid_for(k_select<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s, scan_piece);
   pf->end();
   pf->launched(CT_K_SELECT);
   pf->begin(CT_K_SCAN);
-  k_scan_hist<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s,
-                                                                                       scan_piece);
-  k_scan_carry<<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
-  k_split_scan<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, 2 * sm1, st>>>(
-      v, nodes, tot, s, scan_piece);
+  k_scan_hist<IdxT, LabT><<<grid_for(k_scan_hist<IdxT, LabT>, caps.scan, sm1, persistent), THREADS_PER_BLOCK, sm1,
+                            st>>>(v, s, scan_piece);
+  k_scan_carry<<<grid_for(k_scan_carry, caps.scan, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
+  k_split_scan<IdxT, LabT><<<grid_for(k_split_scan<IdxT, LabT>, caps.scan, 2 * sm1, persistent), THREADS_PER_BLOCK,
+                             2 * sm1, st>>>(v, s, scan_piece);
   if (v.fbin)
-    k_scan_two_valued<IdxT, LabT><<<blocks_for_warps(caps.scan), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, tot, s,
-                                                                                              scan_piece);
+    k_scan_two_valued<IdxT, LabT><<<grid_for(k_scan_two_valued<IdxT, LabT>, caps.scan, sm1, persistent),
+                                    THREADS_PER_BLOCK, sm1, st>>>(v, s, scan_piece);
   pf->end();
   pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
   pf->begin(CT_K_REDUCE);
-  k_split_reduce<IdxT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s);
+  k_split_reduce<IdxT><<<grid_for(k_split_reduce<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
   pf->end();
   pf->launched(CT_K_REDUCE);
 }
 
 template <typename IdxT, typename LabT>
-void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s_all, const LevelCaps& caps,
-                    const TreeView& tv, cudaStream_t st) {
+void partition_impl(const View& v, const LevelScratch& s_all, const LevelCaps& caps, const TreeView& tv,
+                    bool persistent, cudaStream_t st) {
   Prof* pf = current_prof();
   // tile/status capacity of this step: its status words are zeroed, its stride is the column stride
   LevelScratch s = s_all;
   s.cap_status = caps.status;
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
   pf->begin(CT_K_MARK);
-  k_plan<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(v, nodes, s, tv);
-  k_fill_mark<IdxT, LabT><<<blocks_for_warps(caps.part), THREADS_PER_BLOCK, sm1, st>>>(v, nodes, s);
+  k_plan<IdxT, LabT><<<grid_for(k_plan<IdxT, LabT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s,
+                                                                                                            tv);
+  k_fill_mark<IdxT, LabT><<<grid_for(k_fill_mark<IdxT, LabT>, caps.part, sm1, persistent), THREADS_PER_BLOCK, sm1,
+                            st>>>(v, s);
   pf->launched(CT_K_MARK, 2);
   pf->end();
   pf->begin(CT_K_PARTITION);
@@ -1323,14 +1404,12 @@ void partition_impl(const View& v, const ct_node* nodes, const LevelScratch& s_a
 }
 
 template <typename IdxT, typename LabT>
-void children_impl(const View& v, const ct_node* nodes, const uint32_t* tot, const LevelScratch& s,
-                   const LevelCaps& caps, const TreeView& tv, ct_node* next, uint32_t* next_tot,
-                   uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small,
-                   cudaStream_t st) {
+void children_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, const TreeView& tv, uint32_t cap_next,
+                   uint32_t small_cut, ct_node* small, uint32_t cap_small, bool persistent, cudaStream_t st) {
   Prof* pf = current_prof();
   pf->begin(CT_K_CHILDREN);
-  k_children<IdxT, LabT><<<blocks_for_warps(caps.nodes), THREADS_PER_BLOCK, 0, st>>>(
-      v, nodes, tot, s, tv, next, next_tot, cap_next, small_cut, small, cap_small);
+  k_children<IdxT, LabT><<<grid_for(k_children<IdxT, LabT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(
+      v, s, tv, cap_next, small_cut, small, cap_small);
   pf->end();
   pf->launched(CT_K_CHILDREN);
 }
@@ -1373,6 +1452,7 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.big_segs = a.take<PartSeg>(c.nodes);
   t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
+  t.step = a.take<StepLists>(1);
   if (s) *s = t;
   return a.used;
 }
@@ -1395,55 +1475,64 @@ bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScrat
     else { CALL(uint32_t, uint16_t); }                              \
   } while (0)
 
-int launch_split(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes, const uint32_t* tot,
-                 const LevelScratch& s, LevelBounds b, uint32_t scan_piece, cudaStream_t st) {
+uint32_t item_blocks(uint64_t warps, uint32_t grid_cap) {
+  uint64_t b = (warps + WARPS_PER_BLOCK - 1) / WARPS_PER_BLOCK;
+  if (b == 0) b = 1;
+  if (grid_cap && b > grid_cap) b = grid_cap;
+  return (uint32_t)std::min<uint64_t>(b, 0x7fffffffull);
+}
+
+int launch_split(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b, uint32_t scan_piece,
+                 bool persistent, cudaStream_t st) {
   LevelCaps caps = level_caps(v, scan_piece, b);
   caps.scan = min(caps.scan, s.cap_scan);
   caps.carry = min(caps.carry, s.cap_carry);
-#define CALL(I, L) split_impl<I, L>(v, nodes, tot, s, caps, scan_piece, st)
+#define CALL(I, L) split_impl<I, L>(v, s, caps, scan_piece, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
 
-int launch_partition(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes,
-                     const LevelScratch& s, LevelBounds b, const TreeView& tv, cudaStream_t st) {
+int launch_partition(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
+                     const TreeView& tv, bool persistent, cudaStream_t st) {
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
   caps.part = min(caps.part, s.cap_part);
   caps.status = min(caps.status, s.cap_status);
-#define CALL(I, L) partition_impl<I, L>(v, nodes, s, caps, tv, st)
+#define CALL(I, L) partition_impl<I, L>(v, s, caps, tv, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
 
-int launch_children(const View& v, uint32_t ib, uint32_t lb, const ct_node* nodes, const uint32_t* tot,
-                    const LevelScratch& s, LevelBounds b, const TreeView& tv, ct_node* next,
-                    uint32_t* next_tot, uint32_t cap_next, uint32_t small_cut, ct_node* small,
-                    uint32_t cap_small, cudaStream_t st) {
+int launch_children(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b, const TreeView& tv,
+                    uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small, bool persistent,
+                    cudaStream_t st) {
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
-#define CALL(I, L) \
-  children_impl<I, L>(v, nodes, tot, s, caps, tv, next, next_tot, cap_next, small_cut, small, cap_small, st)
+#define CALL(I, L) children_impl<I, L>(v, s, caps, tv, cap_next, small_cut, small, cap_small, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
 
-int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
-                    bool wide, const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
-  if (cap_small == 0) return CT_OK;
+int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small, uint32_t bound,
+                    bool wide, bool persistent, const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
+  if (cap_small == 0 || bound == 0) return CT_OK;
   Prof* pf = current_prof();
   pf->begin(CT_K_SUBTREE);
-#define CALL(I, L) k_subtree<I, L><<<blocks_for_warps(cap_small), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, cap_small)
+  const uint32_t items = std::min(bound, cap_small);
+#define CALL(I, L)                                                                                           \
+  k_subtree<I, L><<<grid_for(k_subtree<I, L>, items, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, \
+                                                                                                cap_small)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   if (wide) {
     const size_t smem = (size_t)WARPS_PER_BLOCK * subtree_warp_words(v.n_classes) * sizeof(uint32_t);
-#define CALL(I, L) \
-  k_subtree_wide<I, L><<<blocks_for_warps(cap_small), THREADS_PER_BLOCK, smem, st>>>(v, small, s, tv, cap_small)
+#define CALL(I, L)                                                                                      \
+  k_subtree_wide<I, L><<<grid_for(k_subtree_wide<I, L>, items, smem, persistent), THREADS_PER_BLOCK, smem, st>>>( \
+      v, small, s, tv, cap_small)
     CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   }
@@ -1453,8 +1542,8 @@ int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* smal
   return CT_OK;
 }
 
-int launch_reset_step(Counters* ctr, uint32_t n_nodes, cudaStream_t st) {
-  k_reset_step<<<1, 1, 0, st>>>(ctr, n_nodes);
+int launch_reset_step(const LevelScratch& s, uint32_t n_nodes, const StepLists& lists, cudaStream_t st) {
+  k_reset_step<<<1, 1, 0, st>>>(s.ctr, n_nodes, s.step, lists);
   current_prof()->launched(CT_K_CHILDREN);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;

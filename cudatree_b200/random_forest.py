@@ -190,6 +190,14 @@ class RandomForestClassifier:
         self.last_fit_timing = {}
         self.last_fit_stats = None
         self.profile = False  # record CUDA-event time per kernel group
+        # batched form: run the levels from the host (one round trip per
+        # level) instead of as one CUDA graph with a device-side loop
+        self.host_level_loop = False
+        # nodes per level step (0: 2^20); a wider level takes several steps
+        self.step_nodes = 0
+        # batched form: levels of at most this many samples run in the loop
+        # graph (0: 2^22; 0xffffffff: all of them)
+        self.graph_samples = 0
 
     # ------------------------------------------------------------ pickling
     def _params(self):
@@ -361,7 +369,7 @@ class RandomForestClassifier:
         tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
                               _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
         opts = self._fit_options(mode_id, bfs_threshold)
-        opts.reserved[0] = 1 if self.profile else 0
+        opts.flags = (_lib.CT_FIT_PROFILE if self.profile else 0) | (_lib.CT_FIT_HOST_LOOP if self.host_level_loop else 0)
         ws = C.c_size_t()
         _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))
         work = _dev_bytes(ws.value, dev)
@@ -437,8 +445,11 @@ class RandomForestClassifier:
     # ---------------------------------------------------------- autotune
     def _fit_options(self, mode_id, bfs_threshold):
         t = self._tuned or {}
-        return _lib.FitOptions(mode_id, int(bfs_threshold), int(t.get("subtree_cutoff", self.subtree_cutoff)),
-                               int(t.get("scan_piece", 0)))
+        o = _lib.FitOptions(mode_id, int(bfs_threshold), int(t.get("subtree_cutoff", self.subtree_cutoff)),
+                            int(t.get("scan_piece", 0)))
+        o.step_nodes = int(self.step_nodes)
+        o.graph_samples = int(self.graph_samples)
+        return o
 
     def _shape_key(self, mode):
         return (mode, self.n_samples, self.n_features, self.n_labels, self._m, self.index_bytes,

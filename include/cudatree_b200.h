@@ -120,8 +120,22 @@ typedef struct ct_fit_options {
   uint32_t subtree_cutoff;  /* nodes with n <= this are grown whole by one warp
                                (<= 128; 0 disables); the trees do not change        */
   uint32_t scan_piece;      /* elements per split-scan work item (0 = default)      */
-  uint32_t reserved[4];
+  uint32_t flags;           /* CT_FIT_PROFILE | CT_FIT_HOST_LOOP                    */
+  uint32_t step_nodes;      /* nodes per level step (0 = 2^20): a wider level takes
+                               several steps; the workspace grows with it           */
+  uint32_t graph_samples;   /* batched: levels of at most this many samples run in
+                               the loop graph, larger ones from the host (0 = 2^22,
+                               0xffffffff = every level in the graph)               */
+  uint32_t reserved;
 } ct_fit_options;
+/* ct_fit_options.flags.  CT_FIT_PROFILE: CUDA events around each kernel
+ * group (ct_fit_stats.ms); the batched form then runs its levels from the
+ * host.  The batched form otherwise runs its levels of at most
+ * graph_samples samples as one CUDA graph with a device-side loop condition
+ * (no host round trip between them); CT_FIT_HOST_LOOP asks for the
+ * host-driven loop throughout (one host round trip per level, as the
+ * reference's BFS, random_tree.py:428-431).  The trees are the same. */
+enum { CT_FIT_PROFILE = 1, CT_FIT_HOST_LOOP = 2 };
 
 /* Bytes of the ct_lists.mark buffer for n_slots tree slots. */
 int ct_mark_bytes(uint32_t n_rows, uint32_t n_slots, size_t* bytes);
@@ -197,8 +211,8 @@ int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint
 
 /* Per-kernel-group statistics of the last ct_fit on the calling thread.
  * Launch counts and algorithmic bytes are always recorded; ms[] is filled
- * when ct_fit_options.reserved[0] has bit 0 set (CUDA events recorded on
- * the fit's stream around each kernel group). */
+ * with CT_FIT_PROFILE (CUDA events recorded on the fit's stream around each
+ * kernel group). */
 enum {
   CT_K_SELECT = 0, CT_K_SCAN = 1, CT_K_REDUCE = 2, CT_K_MARK = 3,
   CT_K_PARTITION = 4, CT_K_CHILDREN = 5, CT_K_BOOTSTRAP = 6, CT_K_SUBTREE = 7,

@@ -286,3 +286,34 @@ def test_two_valued_features_match_oracle(cuda_device, n, c, piece, mode):
     ref = O.fit_forest(x, y, n_estimators=3, max_features=4, seed=29)
     _assert_same_trees(forest._trees, ref.trees)
     np.testing.assert_array_equal(forest.predict(x), O.predict(ref, x))
+
+
+@pytest.mark.parametrize("step_nodes", [0, 7])
+@pytest.mark.parametrize("cut", [32, 128])
+def test_graph_level_loop_matches_host_loop_and_oracle(cuda_device, step_nodes, cut):
+    """The batched form runs its levels of at most graph_samples samples as
+    one CUDA graph (a device-side loop condition over persistent launches)
+    and larger levels from the host.  Every level in the graph, a switch
+    after the first levels, and the host-driven loop throughout all grow the
+    oracle's trees; with 7 nodes per step a level takes many steps and the
+    warp-subtree list (two steps' worth) overflows into the level steps."""
+    x, y = _synthetic(5000, 10, 6, 41)
+    ref = O.fit_forest(x, y, n_estimators=5, seed=43)
+    for host, graph_samples in ((False, 0xFFFFFFFF), (False, 3000), (True, 0)):
+        f = RandomForestClassifier(n_estimators=5, seed=43, subtree_cutoff=cut)
+        f.host_level_loop = host
+        f.step_nodes = step_nodes
+        f.graph_samples = graph_samples
+        f.fit(x, y)
+        _assert_same_trees(f._trees, ref.trees)
+        st = f.last_fit_stats
+        assert st["steps"] >= 10 and st["total_launches"] > 0
+
+
+def test_graph_level_loop_reused_across_fits(cuda_device):
+    """Fits of the same shape reuse the instantiated loop graph; a fit of
+    another shape builds a new one; the trees stay the oracle's."""
+    for n, seed in ((3000, 1), (3000, 2), (4100, 3), (3000, 4)):
+        x, y = _synthetic(n, 8, 4, seed)
+        f = RandomForestClassifier(n_estimators=3, seed=seed).fit(x, y)
+        _assert_same_trees(f._trees, O.fit_forest(x, y, n_estimators=3, seed=seed).trees)
