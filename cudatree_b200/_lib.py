@@ -17,6 +17,7 @@ CT_FIT_PLAIN = 0
 CT_FIT_BATCHED = 1
 CT_FIT_PROFILE = 1     # ct_fit_options.flags
 CT_FIT_HOST_LOOP = 2
+CT_FIT_NO_VIRTUAL = 4
 MAX_CLASSES = 1024
 MAX_FEATURES = 65536
 

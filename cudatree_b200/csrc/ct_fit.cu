@@ -25,7 +25,7 @@ size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
                    const void* src, uint32_t row_mask, uint32_t* n_in_dev, void* ws, size_t wsb,
                    cudaStream_t st);
-int pack_presort(const ct_problem* p, void* out, uint32_t shift, cudaStream_t st);
+int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, cudaStream_t st);
 
 namespace {
 
@@ -100,7 +100,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
     if (threadIdx.x == 0) s_mask = 0;
     __syncthreads();
     const uint32_t f = threadIdx.x;
-    if (f > 0 && f < v.n_features && f < 64) {
+    if (f > 0 && f < v.n_features && f < 64 && !is_virtual(v, f)) {
       const IdxT* lf = list_ptr<IdxT>(v, 0, slot, f);
       const float* xf = v.x_fm + (size_t)f * v.n_rows;
       if (xf[entry_row(v, lf[0])] == xf[entry_row(v, lf[n - 1])]) atomicOr(&s_mask, 1ull << f);
@@ -122,7 +122,7 @@ void begin_level(Counters* c, cudaStream_t st) {
 void account_level(const ct_problem* p, const View& view, const Counters& h) {
   Prof* pf = current_prof();
   const double w = p->index_bytes, l = view.lab_shift ? 0.0 : p->label_bytes, v = sizeof(float);
-  pf->stats.bytes[CT_K_SCAN] += (double)h.scan_elems * (w + l + v);
+  pf->stats.bytes[CT_K_SCAN] += (double)h.scan_elems * (w + l + v) + (double)h.vrows * (w + 8.0);
   pf->stats.bytes[CT_K_MARK] += (double)h.split_total * (w + 1.0);
   pf->stats.bytes[CT_K_PARTITION] += (double)h.part_elems * (2.0 * w + 1.0);  // chains actually partitioned
   pf->stats.steps += 1;
@@ -139,6 +139,7 @@ struct LoopCtl {
   unsigned long long scan_elems;   // totals of the finished levels
   unsigned long long split_total;
   unsigned long long part_elems;
+  unsigned long long vrows;
 };
 
 struct FitLayout {
@@ -154,6 +155,9 @@ struct FitLayout {
   mutable uint64_t small_bound;  // upper bound of the entries in small
   uint32_t* n_in;
   uint32_t* fbin;        // two-valued feature bits (feature_flags)
+  bool virt;             // the fit may have virtual features (View::vmask)
+  uint64_t* vrow;        // [n_rows] their value bits
+  float2* vval;          // [n_features] (low, high) values
   ct_node* list[2];
   uint32_t* tot[2];
   uint64_t* mask[2];     // constant-feature masks of the lists (batched form, n_features <= 64), else NULL
@@ -186,6 +190,9 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->small_bound = 0;
   L->n_in = a.take<uint32_t>(slots);
   L->fbin = a.take<uint32_t>((p->n_features + 31) / 32);
+  L->virt = virtual_possible(p) && !(o->flags & CT_FIT_NO_VIRTUAL);
+  L->vrow = L->virt ? a.take<uint64_t>(p->n_rows) : nullptr;
+  L->vval = L->virt ? a.take<float2>(p->n_features) : nullptr;
   // the plain form moves nodes through the host, so only the batched form keeps masks
   const bool masks = o->mode == CT_FIT_BATCHED && p->n_features <= 64;
   for (int i = 0; i < 2; ++i) {
@@ -196,7 +203,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, slots);
   L->boot_ws = a.take<char>(L->boot_bytes);
   LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
-  carve_level_scratch(a, v, caps, &L->s);
+  carve_level_scratch(a, v, caps, &L->s, L->virt);
   L->ctl = a.take<LoopCtl>(1);
   L->bytes = a.used + 256;
   return base != nullptr && a.ok();
@@ -362,6 +369,7 @@ __global__ void k_loop_init(LoopCtl* ctl, Counters* c, uint32_t cap_list, cudaGr
   ctl->scan_elems = 0;
   ctl->split_total = 0;
   ctl->part_elems = 0;
+  ctl->vrows = 0;
   reset_level_counters(c);
   c->claim[ITEM_SUBTREE] = 0;
   c->claim[ITEM_SUBTREE_WIDE] = 0;
@@ -395,6 +403,7 @@ __global__ void k_loop_end(LoopCtl* ctl, Counters* c, uint32_t chunk, uint32_t c
   ctl->scan_elems += c->scan_elems;
   ctl->split_total += c->split_total;
   ctl->part_elems += c->part_elems;
+  ctl->vrows += c->vrows;
   ctl->levels += 1;
   const uint32_t n = min(c->n_next, cap_list);
   ctl->n_level = n;
@@ -573,6 +582,7 @@ int graph_level_loop(const ct_problem* p, const View& v, const FitLayout& L, con
   tot.scan_elems = ctl.scan_elems;
   tot.split_total = ctl.split_total;
   tot.part_elems = ctl.part_elems;
+  tot.vrows = ctl.vrows;
   const uint64_t steps = pf->stats.steps;
   account_level(p, v, tot);
   pf->stats.steps = steps + ctl.levels;
@@ -617,10 +627,30 @@ View fit_view(const ct_problem* p, const ct_lists* l, const FitLayout& L) {
   return v;
 }
 
+// Per-feature preparation of a fit call: the two-valued features and, when
+// the fit can have virtual features, which ones are (every two-valued
+// feature but feature 0, whose lists give the leaf labels) and their rows'
+// value bits.  One host read of the flags.
+int prepare_features(const ct_problem* p, const FitLayout& L, View* v, cudaStream_t st) {
+  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, L.virt ? L.vval : nullptr, st));
+  if (!L.virt) return CT_OK;
+  uint32_t fb[2] = {0, 0};
+  CT_CUDA_TRY(cudaMemcpyAsync(fb, L.fbin, ((p->n_features + 31) / 32) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaStreamSynchronize(st));
+  const uint64_t all = p->n_features >= 64 ? ~0ull : (1ull << p->n_features) - 1ull;
+  const uint64_t vm = (((uint64_t)fb[1] << 32) | fb[0]) & all & ~1ull;
+  if (!vm) return CT_OK;
+  v->vmask = vm;
+  v->vslot = (uint32_t)__builtin_ctzll(vm);
+  v->vrow = L.vrow;
+  v->vval = L.vval;
+  return virtual_rows(p->x_fm, p->n_rows, vm, L.vval, L.vrow, st);
+}
+
 int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const void** src, cudaStream_t st) {
   *src = p->presort;
   if (v.lab_shift) {
-    CT_TRY(pack_presort(p, l->si1, v.lab_shift, st));
+    CT_TRY(pack_presort(p, l->si1, v.lab_shift, v.vmask ? v.vslot : NONE, st));
     *src = l->si1;
   }
   return CT_OK;
@@ -630,7 +660,7 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
                 const FitLayout& L, const ct_tree_buffers* trees, cudaStream_t st) {
   View v = fit_view(p, l, L);
   TreeView tv = tree_view(trees, 0);
-  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, st));
+  CT_TRY(prepare_features(p, L, &v, st));
   CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
   CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
   current_prof()->begin(CT_K_BOOTSTRAP);
@@ -683,7 +713,7 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
   View v = fit_view(p, l, L);
   const uint32_t C = p->n_classes;
   const uint32_t thr = o->bfs_threshold ? o->bfs_threshold : default_bfs_threshold(p);
-  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, st));
+  CT_TRY(prepare_features(p, L, &v, st));
   struct Pending {
     ct_node nd;
     std::vector<uint32_t> tot;

@@ -98,13 +98,15 @@ struct Counters {
   uint32_t n_small_segs;  // partition segments of small splits
   uint32_t n_big_segs;
   uint32_t n_tiles;       // partition tiles of big splits
-  uint32_t pad[3];
+  uint32_t n_vpieces;     // row-list pieces (virtual features)
+  uint32_t pad[2];
   uint32_t claim[16];     // item counters of persistent launches (ITEM_* slots)
   unsigned long long next_total;
   unsigned long long small_total;
   unsigned long long split_total;  // samples in nodes partitioned this level
   unsigned long long scan_elems;   // (node, feature) elements scanned this level
   unsigned long long part_elems;   // (node, feature) elements partitioned this level
+  unsigned long long vrows;        // row-list rows read by the virtual-feature counts this level
 };
 
 // Counters of one step, zeroed at its start (n_nodes set); the level totals
@@ -114,10 +116,12 @@ struct Counters {
 // and its loop graph, not per step (subtrees run after the level loop).
 enum : uint32_t {
   ITEM_SELECT, ITEM_HIST, ITEM_CARRY, ITEM_SCAN, ITEM_TWO_VALUED, ITEM_REDUCE, ITEM_PLAN, ITEM_FILL,
-  ITEM_CHILDREN, ITEM_STEP_SLOTS, ITEM_SUBTREE = ITEM_STEP_SLOTS, ITEM_SUBTREE_WIDE
+  ITEM_CHILDREN, ITEM_VPIECES, ITEM_VCOUNT, ITEM_VCLASS, ITEM_STEP_SLOTS, ITEM_SUBTREE = ITEM_STEP_SLOTS,
+  ITEM_SUBTREE_WIDE
 };
 __device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_nodes) {
   for (uint32_t i = 0; i < ITEM_STEP_SLOTS; ++i) c->claim[i] = 0;
+  c->n_vpieces = 0;
   c->n_nodes = n_nodes;
   c->n_scan_pieces = 0;
   c->n_carry = 0;
@@ -136,6 +140,7 @@ __device__ __forceinline__ void reset_level_counters(Counters* c) {
   c->split_total = 0;
   c->scan_elems = 0;
   c->part_elems = 0;
+  c->vrows = 0;
 }
 
 // One stable-partition segment: a node range in every feature list.
@@ -201,9 +206,30 @@ struct View {
   // (feature_flags), so its split scan needs only the position of the node's
   // value boundary.  NULL: every feature takes the general scan.
   const uint32_t* fbin;
+  // Virtual features (a fit with label-carrying entries and at most 64
+  // features): two-valued features other than feature 0 whose index lists
+  // are never partitioned.  A node's sorted list of such a feature is the
+  // node's rows in row order, its low value's rows first (the stable order
+  // of the presort), so it is fully described by the node's row list and
+  // one bit per row: bit f of vrow[row] says x[f][row] is the feature's high
+  // value.  The list slot of feature vslot (the lowest virtual feature)
+  // holds the row list instead of that feature's list.  vval[f] = (low,
+  // high).  vmask == 0: no virtual features.
+  uint64_t vmask;
+  const uint64_t* vrow;
+  const float2* vval;
+  uint32_t vslot;
 };
 __device__ __forceinline__ bool two_valued(const View& v, uint32_t f) {
   return v.fbin && ((__ldg(v.fbin + (f >> 5)) >> (f & 31)) & 1u);
+}
+__host__ __device__ __forceinline__ bool is_virtual(const View& v, uint32_t f) {
+  return f < 64 && ((v.vmask >> f) & 1u);
+}
+// Features whose lists a split leaves as they are: the virtual ones except
+// the row-list slot.
+__host__ __device__ __forceinline__ uint64_t virtual_skip(const View& v) {
+  return v.vmask ? v.vmask & ~(1ull << v.vslot) : 0ull;
 }
 
 // Packed mark table: bit r of a slot's words is row r's left flag.  The
@@ -304,6 +330,11 @@ struct LevelScratch {
   // does not read them; k_children writes the next list's masks.  Feature 0
   // is never in a mask (leaf labels and subtrees read its lists).
   StepLists* step;
+  // Virtual features (View::vmask), else NULL / 0:
+  uint32_t* vcnt;         // [cap_nodes][64] rows of each node with the feature's high value
+  uint32_t* vcls;         // [cap_nodes][max_features][n_classes] those rows' classes, per selected slot
+  uint2* vpieces;         // [cap_vpieces] (node, piece) of the nodes' row lists
+  uint32_t cap_vpieces;
 };
 __device__ __forceinline__ bool masked(uint64_t m, uint32_t f) { return f < 64 && ((m >> f) & 1u); }
 
@@ -380,11 +411,14 @@ struct LevelBounds {
   uint64_t samples;
 };
 struct LevelCaps {
-  uint32_t nodes, scan, carry, part, status;
+  uint32_t nodes, scan, carry, part, status, vpieces;
 };
 LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b);
-bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s);
-size_t level_scratch_bytes(const View& v, const LevelCaps& c);
+constexpr uint32_t VPIECE = 2048;  // rows per row-list piece (virtual features)
+// Scratch of virtual features: carved when `virt` (the fit may have some).
+bool virtual_possible(const ct_problem* p);
+bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s, bool virt = false);
+size_t level_scratch_bytes(const View& v, const LevelCaps& c, bool virt = false);
 
 // Level-step launches (ct_level.cu).  The step's node count is in
 // s.ctr->n_nodes and its lists in *s.step (both on the device, set by the
@@ -463,7 +497,12 @@ int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_block
 // Bit f of bits ([ceil(n_features / 32)] words, zeroed here): feature f takes
 // at most two distinct values (-0.0 and +0.0 count as one, as in the scan's
 // comparisons).
-int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, cudaStream_t st);
+// vals (or NULL): each feature's (minimum, maximum).
+int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, float2* vals,
+                  cudaStream_t st);
+// Value bits of the virtual features vmask (View::vrow) into out[n_rows].
+int virtual_rows(const float* x_fm, uint32_t n_rows, uint64_t vmask, const float2* vval, uint64_t* out,
+                 cudaStream_t st);
 int transpose_rows(const float* x_rm, uint32_t n_rows, uint32_t n_cols, float* x_cm, cudaStream_t st,
                    uint32_t* nan_flag = nullptr);
 int check_problem(const ct_problem* p);

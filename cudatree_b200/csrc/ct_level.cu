@@ -82,6 +82,147 @@ __device__ __forceinline__ void warp_argmin2(double& score, uint32_t& pos, float
 }
 
 // ------------------------------------------------------------------------
+// Virtual features: per-node counts from the node's row list (list slot
+// vslot: its rows in row order) and the rows' value bits (vrow).
+//
+//   k_vpieces    cuts each node's row list into pieces of VPIECE rows and
+//                zeroes the node's counts
+//   k_vcount     per piece: the rows with each virtual feature's high value,
+//                added into vcnt[node][f]; k_select then takes a virtual
+//                feature as non-constant in a node when 0 < vcnt < n
+//   k_vclass     per piece of a node that selected virtual features: the
+//                classes of the rows with each selected one's high value,
+//                added into vcls[node][slot][c]; k_split_reduce scores the
+//                feature's one candidate (the last low-value row) from them
+__device__ __forceinline__ void vpieces_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                             uint32_t w) {
+  const uint32_t lane = lane_id();
+  const ct_node nd = lists.nodes[w];
+  const uint32_t mc = v.max_features * v.n_classes;
+  for (uint32_t f = lane; f < 64; f += 32) s.vcnt[(size_t)w * 64 + f] = 0;
+  for (uint32_t i = lane; i < mc; i += 32) s.vcls[(size_t)w * mc + i] = 0;
+  if (nd.n < 2) return;
+  const uint32_t np = ceil_div(nd.n, VPIECE);
+  uint32_t base = 0;
+  if (lane == 0) {
+    base = atomicAdd(&s.ctr->n_vpieces, np);
+    if (base + (uint64_t)np > s.cap_vpieces) {
+      atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+      base = NONE;
+    }
+  }
+  base = __shfl_sync(FULL, base, 0);
+  if (base == NONE) return;
+  for (uint32_t j = lane; j < np; j += 32) s.vpieces[base + j] = make_uint2(w, j);
+}
+
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vpieces(View v, LevelScratch s) {
+  const uint32_t count = min(s.ctr->n_nodes, s.cap_nodes);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_VPIECES], [&](uint32_t w) { vpieces_item(v, sl, s, w); });
+}
+
+template <typename IdxT>
+__device__ __forceinline__ void vcount_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                            uint32_t pi) {
+  const uint32_t lane = lane_id();
+  const uint2 pc = s.vpieces[pi];
+  const ct_node nd = lists.nodes[pc.x];
+  const IdxT* rl = list_ptr<IdxT>(v, nd.buf, nd.slot, v.vslot) + nd.start;
+  const uint32_t lo = pc.y * VPIECE;
+  const uint32_t hi = min(lo + VPIECE, nd.n);
+  // Bit-sliced counters: bit f of plane k is bit k of this lane's count of
+  // rows with feature f's high value (at most VPIECE / 32 = 64 rows a lane).
+  uint64_t pl[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = lo + lane; i < hi; i += 32) {
+    uint64_t c = __ldg(v.vrow + entry_row(v, (uint32_t)__ldcs(rl + i)));
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const uint64_t t = pl[k] & c;
+      pl[k] ^= c;
+      c = t;
+    }
+  }
+  if (lane == 0) atomicAdd(&s.ctr->vrows, (unsigned long long)(hi - lo));
+  for (uint64_t vm = v.vmask; vm; vm &= vm - 1) {
+    const uint32_t f = (uint32_t)__ffsll((long long)vm) - 1;
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) cnt |= (uint32_t)((pl[k] >> f) & 1ull) << k;
+    cnt = __reduce_add_sync(FULL, cnt);
+    if (lane == 0 && cnt) atomicAdd(&s.vcnt[(size_t)pc.x * 64 + f], cnt);
+  }
+}
+
+template <typename IdxT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vcount(View v, LevelScratch s) {
+  const uint32_t count = live_count(s, s.ctr->n_vpieces, s.cap_vpieces);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_VCOUNT], [&](uint32_t pi) { vcount_item<IdxT>(v, sl, s, pi); });
+}
+
+// Per-warp shared memory: [max_features][n_classes] class counts.
+template <typename IdxT, typename LabT>
+__device__ __forceinline__ void vclass_item(const View& v, const StepLists& lists, const LevelScratch& s,
+                                            uint32_t* cnt, uint32_t pi) {
+  const uint32_t lane = lane_id();
+  const uint32_t C = v.n_classes, m = v.max_features;
+  const uint2 pc = s.vpieces[pi];
+  const uint32_t w = pc.x;
+  const uint32_t nsel = s.nsel[w];
+  // selected slots holding virtual features (m <= 64)
+  uint64_t vs = 0;
+  for (uint32_t q0 = 0; q0 < nsel; q0 += 32) {
+    const uint32_t q = q0 + lane;
+    const bool vq = q < nsel && is_virtual(v, s.sel[(size_t)w * m + q]);
+    vs |= (uint64_t)__ballot_sync(FULL, vq) << q0;
+  }
+  if (!vs) return;
+  for (uint64_t b = vs; b; b &= b - 1) {
+    const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
+    for (uint32_t c = lane; c < C; c += 32) cnt[q * C + c] = 0;
+  }
+  __syncwarp();
+  const ct_node nd = lists.nodes[w];
+  const IdxT* rl = list_ptr<IdxT>(v, nd.buf, nd.slot, v.vslot) + nd.start;
+  const uint32_t lo = pc.y * VPIECE;
+  const uint32_t hi = min(lo + VPIECE, nd.n);
+  for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
+    const uint32_t i = i0 + lane;
+    uint32_t lab = NONE;
+    uint64_t bits = 0;
+    if (i < hi) {
+      const uint32_t e = (uint32_t)__ldcs(rl + i);
+      lab = entry_label<LabT>(v, e);
+      bits = __ldg(v.vrow + entry_row(v, e));
+    }
+    for (uint64_t b = vs; b; b &= b - 1) {
+      const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
+      const uint32_t f = s.sel[(size_t)w * m + q];
+      const uint32_t key = ((bits >> f) & 1ull) ? lab : NONE;
+      const unsigned grp = __match_any_sync(FULL, key);
+      if (key != NONE && (grp >> lane) == 1u) cnt[q * C + key] += __popc(grp);
+      __syncwarp();
+    }
+  }
+  if (lane == 0) atomicAdd(&s.ctr->vrows, (unsigned long long)(hi - lo));
+  for (uint64_t b = vs; b; b &= b - 1) {
+    const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
+    for (uint32_t c = lane; c < C; c += 32)
+      if (cnt[q * C + c]) atomicAdd(&s.vcls[((size_t)w * m + q) * C + c], cnt[q * C + c]);
+  }
+}
+
+template <typename IdxT, typename LabT>
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vclass(View v, LevelScratch s) {
+  extern __shared__ uint32_t smem[];
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.max_features * v.n_classes;
+  const uint32_t count = live_count(s, s.ctr->n_vpieces, s.cap_vpieces);
+  const StepLists sl = *s.step;
+  for_items(count, &s.ctr->claim[ITEM_VCLASS], [&](uint32_t pi) { vclass_item<IdxT, LabT>(v, sl, s, cnt, pi); });
+}
+
+// ------------------------------------------------------------------------
 template <typename IdxT>
 __device__ __forceinline__ void select_item(const View& v, const StepLists& lists, const LevelScratch& s,
                                             uint32_t scan_piece, uint32_t w) {
@@ -90,14 +231,19 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
   const uint32_t m = v.max_features;
   const uint64_t cmask = lists.node_mask ? lists.node_mask[w] : 0ull;  // constant features (lists not current)
   uint32_t taken = 0;
+  uint64_t vsel = 0;  // selected slots that hold virtual features (m <= 64 when there are any)
   if (nd.n >= 2) {
     for (uint32_t i0 = 0; i0 < v.n_features && taken < m; i0 += 32) {
       const uint32_t i = i0 + lane;
-      bool usable = false;
+      bool usable = false, virt = false;
       uint32_t f = 0;
       if (i < v.n_features) {
         f = feature_perm(i, v.n_features, nd.key, v.feistel_h);
-        if (!masked(cmask, f)) {
+        virt = is_virtual(v, f);
+        if (virt) {  // non-constant: some but not all rows take the high value
+          const uint32_t nb = s.vcnt[(size_t)w * 64 + f];
+          usable = nb > 0 && nb < nd.n;
+        } else if (!masked(cmask, f)) {
           const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
           const float* xf = v.x_fm + (size_t)f * v.n_rows;
           usable = xf[entry_row(v, lst[0])] != xf[entry_row(v, lst[nd.n - 1])];
@@ -105,15 +251,20 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
       }
       const unsigned mask = __ballot_sync(FULL, usable);
       const uint32_t rank = __popc(mask & lanemask_lt());
-      if (usable && taken + rank < m) s.sel[(size_t)w * m + taken + rank] = f;
+      const bool keep = usable && taken + rank < m;
+      if (keep) s.sel[(size_t)w * m + taken + rank] = f;
+      const uint64_t vb = (keep && virt) ? 1ull << (taken + rank) : 0ull;
+      vsel |= ((uint64_t)__reduce_or_sync(FULL, (uint32_t)(vb >> 32)) << 32) | __reduce_or_sync(FULL, (uint32_t)vb);
       taken += min((uint32_t)__popc(mask), m - taken);
     }
   }
+  // scan pieces for the materialized slots only (virtual ones are scored from counts)
+  const uint32_t tmat = taken - (uint32_t)__popcll(vsel);
   const uint32_t pps = ceil_div(nd.n, scan_piece);
-  uint32_t npieces = taken * pps;
+  uint32_t npieces = tmat * pps;
   uint32_t base = 0, cbase = 0;
   if (lane == 0) {
-    if (taken) atomicAdd(&s.ctr->scan_elems, (unsigned long long)taken * nd.n);
+    if (tmat) atomicAdd(&s.ctr->scan_elems, (unsigned long long)tmat * nd.n);
     if (npieces) base = atomicAdd(&s.ctr->n_scan_pieces, npieces);
     if (npieces && pps > 1) cbase = atomicAdd(&s.ctr->n_carry, npieces);
     const bool overflow = (base + (uint64_t)npieces > s.cap_scan) ||
@@ -132,8 +283,15 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
   for (uint32_t q = lane; q < npieces; q += 32) {
     ScanPiece pc;
     pc.node = w;
-    pc.slot = q / pps;
-    pc.j = q - pc.slot * pps;
+    const uint32_t k = q / pps;  // k-th materialized slot
+    pc.slot = k;
+    if (vsel) {
+      uint32_t slot = 0;
+      for (uint32_t left = k;; ++slot)
+        if (!((vsel >> slot) & 1ull) && left-- == 0) break;
+      pc.slot = slot;
+    }
+    pc.j = q - k * pps;
     pc.npieces = pps;
     pc.carry = cbase + q;
     pc.pad[0] = pc.pad[1] = pc.pad[2] = 0;
@@ -524,19 +682,60 @@ __device__ __forceinline__ void split_reduce_item(const View& v, const StepLists
     }
   }
   warp_argmin3(best, bf, bp, il, ir);
+  if (v.vmask) {
+    // virtual features: one candidate each, the last low-value row, with the
+    // class counts of the high-value rows from k_vclass (the same exact
+    // arithmetic as the scan; the same (score, feature, position) order)
+    const uint32_t nsel = s.nsel[w];
+    const ct_node nd = lists.nodes[w];
+    const uint32_t C = v.n_classes;
+    const double nn = (double)nd.n;
+    for (uint32_t q = 0; q < nsel; ++q) {
+      const uint32_t f = s.sel[(size_t)w * m + q];
+      if (!is_virtual(v, f)) continue;
+      const float2 lh = v.vval[f];
+      if (!is_candidate_sorted(lh.x, lh.y)) continue;
+      const uint32_t pos = nd.n - s.vcnt[(size_t)w * 64 + f] - 1;
+      int64_t sl = 0, sr = 0;
+      for (uint32_t c = lane; c < C; c += 32) {
+        const int64_t r = s.vcls[((size_t)w * m + q) * C + c];
+        const int64_t l = (int64_t)lists.tot[(size_t)w * C + c] - r;
+        sl += l * l;
+        sr += r * r;
+      }
+      sl = warp_sum_i64(sl);
+      sr = warp_sum_i64(sr);
+      const double nl = (double)(pos + 1);
+      const double gl = gini_part(sl, nl, nn);
+      const double gr = gini_part(sr, __dsub_rn(nn, nl), nn);
+      const double sc = __dadd_rn(gl, gr);
+      if (sc < best || (sc == best && (f < bf || (f == bf && pos < bp)))) {
+        best = sc;
+        bf = f;
+        bp = pos;
+        il = __double2float_rn(gl);
+        ir = __double2float_rn(gr);
+      }
+    }
+  }
   if (lane == 0) {
     ct_split_result r;
     r.n_selected = s.nsel[w];
     if (best < dinf()) {
-      const ct_node nd = lists.nodes[w];
-      const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, bf) + nd.start;
-      const float* xf = v.x_fm + (size_t)bf * v.n_rows;
       r.score = best;
       r.feature = bf;
       r.pos = bp;
       r.imp_left = il;
       r.imp_right = ir;
-      r.threshold = midpoint(xf[entry_row(v, lst[bp])], xf[entry_row(v, lst[bp + 1])]);
+      if (is_virtual(v, bf)) {
+        const float2 lh = v.vval[bf];
+        r.threshold = midpoint(lh.x, lh.y);
+      } else {
+        const ct_node nd = lists.nodes[w];
+        const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, bf) + nd.start;
+        const float* xf = v.x_fm + (size_t)bf * v.n_rows;
+        r.threshold = midpoint(xf[entry_row(v, lst[bp])], xf[entry_row(v, lst[bp + 1])]);
+      }
     } else {
       r.score = dinf();
       r.feature = NONE;
@@ -600,7 +799,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
     atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
-    const uint64_t skip = lists.node_mask ? lists.node_mask[w] : 0ull;
+    const uint64_t skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
     atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * (v.n_features - (uint32_t)__popcll(skip)));
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
     if (big) {
@@ -629,7 +828,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
       sg.n = nd.n;
       sg.nl = r.pos + 1;
       sg.status = tbase;
-      sg.skip = lists.node_mask ? lists.node_mask[w] : 0ull;
+      sg.skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
       (big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
@@ -674,7 +873,10 @@ __device__ __forceinline__ void fill_mark_item(const View& v, const StepLists& l
   const PartPiece pp = s.part[pi];
   const SplitRec sr = s.splits[pp.split];
   const ct_node nd = lists.nodes[sr.node];
-  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, sr.feature) + nd.start;
+  // a virtual split feature: its left rows are the node's rows with its low
+  // value, read from the row list (row order) and the rows' value bits
+  const bool virt = is_virtual(v, sr.feature);
+  const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, virt ? v.vslot : sr.feature) + nd.start;
   uint32_t* bw = v.bits + (size_t)nd.slot * v.bit_words;
   for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
   __syncwarp();
@@ -694,8 +896,8 @@ __device__ __forceinline__ void fill_mark_item(const View& v, const StepLists& l
     const uint32_t p = lo + r * 32 + lane;
     cls[r] = NONE;
     if (p < hi) {
-      const bool left = p <= sr.pos;
       const uint32_t row = entry_row(v, rows[r]);
+      const bool left = virt ? !((__ldg(v.vrow + row) >> sr.feature) & 1ull) : p <= sr.pos;
       if (left) atomicOr(bw + (row >> 5), 1u << (row & 31));
       else atomicAnd(bw + (row >> 5), ~(1u << (row & 31)));
       if (left) cls[r] = entry_label<LabT>(v, rows[r]);
@@ -797,7 +999,7 @@ __device__ __forceinline__ void children_item(const View& v, const StepLists& li
       for (uint32_t f0 = 0; f0 < v.n_features; f0 += 32) {
         const uint32_t f = f0 + lane;
         bool cst = false;
-        if (f > 0 && f < v.n_features && !masked(pm, f)) {
+        if (f > 0 && f < v.n_features && !masked(pm, f) && !is_virtual(v, f)) {
           const IdxT* lst = list_ptr<IdxT>(v, ch.buf, ch.slot, f) + ch.start;
           const float* xf = v.x_fm + (size_t)f * v.n_rows;
           cst = xf[entry_row(v, lst[0])] == xf[entry_row(v, lst[ch.n - 1])];
@@ -1360,6 +1562,13 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
                 cudaStream_t st) {
   Prof* pf = current_prof();
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
+  if (v.vmask) {  // counts of the virtual features, before the selection reads them
+    pf->begin(CT_K_SCAN);
+    k_vpieces<<<grid_for(k_vpieces, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
+    k_vcount<IdxT><<<grid_for(k_vcount<IdxT>, caps.vpieces, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
+    pf->end();
+    pf->launched(CT_K_SCAN, 2);
+  }
   pf->begin(CT_K_SELECT);
   k_select<IdxT><<<grid_for(k_select<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s, scan_piece);
   pf->end();
@@ -1373,8 +1582,13 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
   if (v.fbin)
     k_scan_two_valued<IdxT, LabT><<<grid_for(k_scan_two_valued<IdxT, LabT>, caps.scan, sm1, persistent),
                                     THREADS_PER_BLOCK, sm1, st>>>(v, s, scan_piece);
+  if (v.vmask) {
+    const size_t smv = (size_t)WARPS_PER_BLOCK * v.max_features * v.n_classes * sizeof(uint32_t);
+    k_vclass<IdxT, LabT><<<grid_for(k_vclass<IdxT, LabT>, caps.vpieces, smv, persistent), THREADS_PER_BLOCK, smv,
+                           st>>>(v, s);
+  }
   pf->end();
-  pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
+  pf->launched(CT_K_SCAN, (v.fbin ? 4 : 3) + (v.vmask ? 1 : 0));
   pf->begin(CT_K_REDUCE);
   k_split_reduce<IdxT><<<grid_for(k_split_reduce<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
   pf->end();
@@ -1425,10 +1639,11 @@ LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b) {
   c.carry = clamp32(m * (2 * b.samples / scan_piece) + 1);
   c.part = clamp32(b.samples / PART_PIECE + b.nodes + 1);
   c.status = clamp32(b.samples / TILE_ELEMS + b.samples / (SMALL_SEG + 1) + 1);  // tiles of big splits
+  c.vpieces = clamp32(b.samples / VPIECE + b.nodes + 1);
   return c;
 }
 
-static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s) {
+static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s, bool virt) {
   const size_t C = v.n_classes;
   LevelScratch t;
   t.cap_nodes = c.nodes;
@@ -1453,18 +1668,27 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   t.step = a.take<StepLists>(1);
+  t.vcnt = virt ? a.take<uint32_t>((size_t)c.nodes * 64) : nullptr;
+  t.vcls = virt ? a.take<uint32_t>((size_t)c.nodes * v.max_features * C) : nullptr;
+  t.vpieces = virt ? a.take<uint2>(c.vpieces) : nullptr;
+  t.cap_vpieces = virt ? c.vpieces : 0u;
   if (s) *s = t;
   return a.used;
 }
 
-size_t level_scratch_bytes(const View& v, const LevelCaps& c) {
+size_t level_scratch_bytes(const View& v, const LevelCaps& c, bool virt) {
   Arena a{nullptr, 0, 0};
-  return carve_or_size(a, v, c, nullptr) + 256;
+  return carve_or_size(a, v, c, nullptr, virt) + 256;
 }
 
-bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s) {
-  carve_or_size(a, v, c, s);
+bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScratch* s, bool virt) {
+  carve_or_size(a, v, c, s, virt);
   return a.ok();
+}
+
+bool virtual_possible(const ct_problem* p) {
+  return p->n_features >= 2 && p->n_features <= 64 && fit_label_shift(p) != 0 &&
+         (uint64_t)p->max_features * p->n_classes <= 2048;
 }
 
 #define CT_DISPATCH(IB, LB, CALL)                                   \
@@ -1572,7 +1796,7 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
 namespace {
 // One block per feature: the row's minimum and maximum, then whether every
 // value equals one of them (float equality: -0.0 == +0.0).
-__global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows, uint32_t* bits) {
+__global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows, uint32_t* bits, float2* vals) {
   __shared__ float s_mn[32], s_mx[32];
   const uint32_t f = blockIdx.x;
   const float* xr = x_fm + (size_t)f * n_rows;
@@ -1598,6 +1822,7 @@ __global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows,
     mn = fminf(mn, s_mn[w]);
     mx = fmaxf(mx, s_mx[w]);
   }
+  if (vals && threadIdx.x == 0) vals[f] = make_float2(mn, mx);
   bool ok = true;
   for (uint32_t i = threadIdx.x; i < n_rows && ok; i += blockDim.x) {
     const float x = xr[i];
@@ -1608,9 +1833,33 @@ __global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows,
 }
 }  // namespace
 
-int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, cudaStream_t st) {
+int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, float2* vals,
+                  cudaStream_t st) {
   CT_CUDA_TRY(cudaMemsetAsync(bits, 0, ((n_features + 31) / 32) * sizeof(uint32_t), st));
-  k_feature_flags<<<n_features, 256, 0, st>>>(x_fm, n_rows, bits);
+  k_feature_flags<<<n_features, 256, 0, st>>>(x_fm, n_rows, bits, vals);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
+namespace {
+// Value bits of the virtual features: bit f of out[row] when x[f][row] is the
+// feature's high value.
+__global__ void k_vrow(const float* __restrict__ x_fm, uint32_t n_rows, uint64_t vmask, const float2* __restrict__ vval,
+                       uint64_t* __restrict__ out) {
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += gridDim.x * blockDim.x) {
+    uint64_t b = 0;
+    for (uint64_t vm = vmask; vm; vm &= vm - 1) {
+      const uint32_t f = (uint32_t)__ffsll((long long)vm) - 1;
+      if (x_fm[(size_t)f * n_rows + r] == vval[f].y) b |= 1ull << f;
+    }
+    out[r] = b;
+  }
+}
+}  // namespace
+
+int virtual_rows(const float* x_fm, uint32_t n_rows, uint64_t vmask, const float2* vval, uint64_t* out,
+                 cudaStream_t st) {
+  k_vrow<<<std::min<uint32_t>(ceil_div(n_rows, 256), 148 * 8), 256, 0, st>>>(x_fm, n_rows, vmask, vval, out);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
@@ -1640,6 +1889,10 @@ View make_view(const ct_problem* p, const ct_lists* l) {
   v.row_mask = 0xffffffffu;
   v.lab_shift = 0;
   v.fbin = nullptr;
+  v.vmask = 0;
+  v.vrow = nullptr;
+  v.vval = nullptr;
+  v.vslot = 0;
   return v;
 }
 

@@ -195,6 +195,9 @@ class RandomForestClassifier:
         self.host_level_loop = False
         # nodes per level step (0: 2^20); a wider level takes several steps
         self.step_nodes = 0
+        # keep no index lists for two-valued features (one row-order list per
+        # node and a value bit per row stand for them); False keeps them all
+        self.virtual_features = True
         # batched form: levels of at most this many samples run in the loop
         # graph (0: 2^22; 0xffffffff: all of them)
         self.graph_samples = 0
@@ -369,7 +372,7 @@ class RandomForestClassifier:
         tb = _lib.TreeBuffers(_ptr(raw["left"]), _ptr(raw["right"]), _ptr(raw["feature"]),
                               _ptr(raw["threshold"]), _ptr(raw["value"]), _ptr(n_nodes), cap)
         opts = self._fit_options(mode_id, bfs_threshold)
-        opts.flags = (_lib.CT_FIT_PROFILE if self.profile else 0) | (_lib.CT_FIT_HOST_LOOP if self.host_level_loop else 0)
+        opts.flags |= (_lib.CT_FIT_PROFILE if self.profile else 0) | (_lib.CT_FIT_HOST_LOOP if self.host_level_loop else 0)
         ws = C.c_size_t()
         _lib.call("ct_fit_workspace_size", C.byref(prob), per_call, C.byref(opts), C.byref(ws))
         work = _dev_bytes(ws.value, dev)
@@ -447,6 +450,8 @@ class RandomForestClassifier:
         t = self._tuned or {}
         o = _lib.FitOptions(mode_id, int(bfs_threshold), int(t.get("subtree_cutoff", self.subtree_cutoff)),
                             int(t.get("scan_piece", 0)))
+        if not self.virtual_features:
+            o.flags |= _lib.CT_FIT_NO_VIRTUAL
         o.step_nodes = int(self.step_nodes)
         o.graph_samples = int(self.graph_samples)
         return o

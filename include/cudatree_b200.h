@@ -135,7 +135,13 @@ typedef struct ct_fit_options {
  * (no host round trip between them); CT_FIT_HOST_LOOP asks for the
  * host-driven loop throughout (one host round trip per level, as the
  * reference's BFS, random_tree.py:428-431).  The trees are the same. */
-enum { CT_FIT_PROFILE = 1, CT_FIT_HOST_LOOP = 2 };
+enum { CT_FIT_PROFILE = 1, CT_FIT_HOST_LOOP = 2, CT_FIT_NO_VIRTUAL = 4 };
+/* CT_FIT_NO_VIRTUAL: keep an index list for every feature.  By default, a
+ * fit with label-carrying entries and at most 64 features keeps none for
+ * its two-valued features other than feature 0: a node's sorted list of
+ * such a feature is its rows in row order with the low value first, so one
+ * row-order list per node and a value bit per row stand for them, and a
+ * split moves that one list instead of theirs.  The trees are the same. */
 
 /* Bytes of the ct_lists.mark buffer for n_slots tree slots. */
 int ct_mark_bytes(uint32_t n_rows, uint32_t n_slots, size_t* bytes);

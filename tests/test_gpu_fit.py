@@ -317,3 +317,24 @@ def test_graph_level_loop_reused_across_fits(cuda_device):
         x, y = _synthetic(n, 8, 4, seed)
         f = RandomForestClassifier(n_estimators=3, seed=seed).fit(x, y)
         _assert_same_trees(f._trees, O.fit_forest(x, y, n_estimators=3, seed=seed).trees)
+
+
+@pytest.mark.parametrize("mode", ["plain", "batched"])
+@pytest.mark.parametrize("n,seed", [(3000, 71), (40000, 72), (70000, 73)])
+def test_virtual_two_valued_features_match_oracle(cuda_device, n, seed, mode):
+    """Covtype-shaped data (44 of 54 features one-hot): with label-carrying
+    entries every two-valued feature but feature 0 keeps no index lists (a
+    row-order list per node and a value bit per row stand for them).  Those
+    fits, the fits that keep every list, and the oracle grow the same trees.
+    3,000 rows (16-bit entries) and 70,000 rows (32-bit) carry labels in
+    their entries; at 40,000 rows a 16-bit entry holds the row id alone, so
+    that fit keeps every list either way."""
+    from cudatree_b200 import synthetic
+    x, y = synthetic.covtype_like(n=n, seed=seed)
+    ref = O.fit_forest(x, y, n_estimators=3, max_features=7, seed=seed)
+    for virt in (True, False):
+        f = RandomForestClassifier(n_estimators=3, max_features=7, seed=seed, fit_mode=mode)
+        f.virtual_features = virt
+        f.fit(x, y)
+        _assert_same_trees(f._trees, ref.trees)
+    np.testing.assert_array_equal(f.predict(x[:3000]), O.predict(ref, x[:3000]))
