@@ -155,6 +155,7 @@ struct FitLayout {
   mutable uint64_t small_bound;  // upper bound of the entries in small
   uint32_t* n_in;
   uint32_t* fbin;        // two-valued feature bits (feature_flags)
+  void* ffwork;          // feature_flags scratch
   bool virt;             // the fit may have virtual features (View::vmask)
   uint64_t* vrow;        // [n_rows] their value bits
   float2* vval;          // [n_features] (low, high) values
@@ -177,6 +178,11 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->n_slots = slots;
   L->cap_list = (uint32_t)std::min<uint64_t>(cap_list64, 0xffffffffull);
   L->chunk = std::min<uint32_t>(L->cap_list, o->step_nodes ? o->step_nodes : CHUNK_NODES_MAX);
+  if (virtual_possible(p) && !(o->flags & CT_FIT_NO_VIRTUAL)) {
+    // the per-node class counts of the virtual features stay within 1 GiB
+    const uint64_t per_node = (uint64_t)p->n_features * p->n_classes * sizeof(uint32_t);
+    L->chunk = std::min<uint32_t>(L->chunk, (uint32_t)std::max<uint64_t>(4096, (1ull << 30) / per_node));
+  }
   L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
   // the warp subtree packs a row id into 27 bits of its sort key
   L->subtree_cut = p->n_rows < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 128u) : 0u;
@@ -190,6 +196,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->small_bound = 0;
   L->n_in = a.take<uint32_t>(slots);
   L->fbin = a.take<uint32_t>((p->n_features + 31) / 32);
+  L->ffwork = a.take<char>(feature_flags_work_bytes(p->n_features));
   L->virt = virtual_possible(p) && !(o->flags & CT_FIT_NO_VIRTUAL);
   L->vrow = L->virt ? a.take<uint64_t>(p->n_rows) : nullptr;
   L->vval = L->virt ? a.take<float2>(p->n_features) : nullptr;
@@ -632,7 +639,7 @@ View fit_view(const ct_problem* p, const ct_lists* l, const FitLayout& L) {
 // feature but feature 0, whose lists give the leaf labels) and their rows'
 // value bits.  One host read of the flags.
 int prepare_features(const ct_problem* p, const FitLayout& L, View* v, cudaStream_t st) {
-  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, L.virt ? L.vval : nullptr, st));
+  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, L.virt ? L.vval : nullptr, L.ffwork, st));
   if (!L.virt) return CT_OK;
   uint32_t fb[2] = {0, 0};
   CT_CUDA_TRY(cudaMemcpyAsync(fb, L.fbin, ((p->n_features + 31) / 32) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));

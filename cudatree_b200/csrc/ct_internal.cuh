@@ -116,7 +116,7 @@ struct Counters {
 // and its loop graph, not per step (subtrees run after the level loop).
 enum : uint32_t {
   ITEM_SELECT, ITEM_HIST, ITEM_CARRY, ITEM_SCAN, ITEM_TWO_VALUED, ITEM_REDUCE, ITEM_PLAN, ITEM_FILL,
-  ITEM_CHILDREN, ITEM_VPIECES, ITEM_VCOUNT, ITEM_VCLASS, ITEM_STEP_SLOTS, ITEM_SUBTREE = ITEM_STEP_SLOTS,
+  ITEM_CHILDREN, ITEM_VPIECES, ITEM_VCOUNT, ITEM_STEP_SLOTS, ITEM_SUBTREE = ITEM_STEP_SLOTS,
   ITEM_SUBTREE_WIDE
 };
 __device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_nodes) {
@@ -332,7 +332,7 @@ struct LevelScratch {
   StepLists* step;
   // Virtual features (View::vmask), else NULL / 0:
   uint32_t* vcnt;         // [cap_nodes][64] rows of each node with the feature's high value
-  uint32_t* vcls;         // [cap_nodes][max_features][n_classes] those rows' classes, per selected slot
+  uint32_t* vcls;         // [cap_nodes][n_features][n_classes] those rows by class
   uint2* vpieces;         // [cap_vpieces] (node, piece) of the nodes' row lists
   uint32_t cap_vpieces;
 };
@@ -497,9 +497,11 @@ int predict_batch(const BatchReq* reqs_dev, uint32_t n_req, uint32_t total_block
 // Bit f of bits ([ceil(n_features / 32)] words, zeroed here): feature f takes
 // at most two distinct values (-0.0 and +0.0 count as one, as in the scan's
 // comparisons).
-// vals (or NULL): each feature's (minimum, maximum).
-int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, float2* vals,
+// vals (or NULL): each feature's (minimum, maximum); work: device scratch
+// of feature_flags_work_bytes(n_features).
+int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, float2* vals, void* work,
                   cudaStream_t st);
+size_t feature_flags_work_bytes(uint32_t n_features);
 // Value bits of the virtual features vmask (View::vrow) into out[n_rows].
 int virtual_rows(const float* x_fm, uint32_t n_rows, uint64_t vmask, const float2* vval, uint64_t* out,
                  cudaStream_t st);

@@ -87,20 +87,20 @@ __device__ __forceinline__ void warp_argmin2(double& score, uint32_t& pos, float
 //
 //   k_vpieces    cuts each node's row list into pieces of VPIECE rows and
 //                zeroes the node's counts
-//   k_vcount     per piece: the rows with each virtual feature's high value,
-//                added into vcnt[node][f]; k_select then takes a virtual
-//                feature as non-constant in a node when 0 < vcnt < n
-//   k_vclass     per piece of a node that selected virtual features: the
-//                classes of the rows with each selected one's high value,
-//                added into vcls[node][slot][c]; k_split_reduce scores the
-//                feature's one candidate (the last low-value row) from them
+//   k_vcount     per piece: for every virtual feature f and class c, the rows
+//                with f's high value and class c (one shared-memory add per
+//                set value bit: one-hot rows have one per group), added into
+//                vcls[node][f][c], and their sum into vcnt[node][f].
+//                k_select takes a virtual feature as non-constant in a node
+//                when 0 < vcnt < n; k_split_reduce scores its one candidate
+//                (the last low-value row) from vcls.
 __device__ __forceinline__ void vpieces_item(const View& v, const StepLists& lists, const LevelScratch& s,
                                              uint32_t w) {
   const uint32_t lane = lane_id();
   const ct_node nd = lists.nodes[w];
-  const uint32_t mc = v.max_features * v.n_classes;
+  const uint32_t fc = v.n_features * v.n_classes;
   for (uint32_t f = lane; f < 64; f += 32) s.vcnt[(size_t)w * 64 + f] = 0;
-  for (uint32_t i = lane; i < mc; i += 32) s.vcls[(size_t)w * mc + i] = 0;
+  for (uint32_t i = lane; i < fc; i += 32) s.vcls[(size_t)w * fc + i] = 0;
   if (nd.n < 2) return;
   const uint32_t np = ceil_div(nd.n, VPIECE);
   uint32_t base = 0;
@@ -122,104 +122,45 @@ __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vpieces(View v, LevelScra
   for_items(count, &s.ctr->claim[ITEM_VPIECES], [&](uint32_t w) { vpieces_item(v, sl, s, w); });
 }
 
-template <typename IdxT>
+// Per-warp shared memory: [n_features][n_classes] counts.
+template <typename IdxT, typename LabT>
 __device__ __forceinline__ void vcount_item(const View& v, const StepLists& lists, const LevelScratch& s,
-                                            uint32_t pi) {
+                                            uint32_t* cnt, uint32_t pi) {
   const uint32_t lane = lane_id();
+  const uint32_t C = v.n_classes, fc = v.n_features * C;
   const uint2 pc = s.vpieces[pi];
   const ct_node nd = lists.nodes[pc.x];
   const IdxT* rl = list_ptr<IdxT>(v, nd.buf, nd.slot, v.vslot) + nd.start;
   const uint32_t lo = pc.y * VPIECE;
   const uint32_t hi = min(lo + VPIECE, nd.n);
-  // Bit-sliced counters: bit f of plane k is bit k of this lane's count of
-  // rows with feature f's high value (at most VPIECE / 32 = 64 rows a lane).
-  uint64_t pl[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = lane; i < fc; i += 32) cnt[i] = 0;
+  __syncwarp();
   for (uint32_t i = lo + lane; i < hi; i += 32) {
-    uint64_t c = __ldg(v.vrow + entry_row(v, (uint32_t)__ldcs(rl + i)));
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const uint64_t t = pl[k] & c;
-      pl[k] ^= c;
-      c = t;
-    }
-  }
-  if (lane == 0) atomicAdd(&s.ctr->vrows, (unsigned long long)(hi - lo));
-  for (uint64_t vm = v.vmask; vm; vm &= vm - 1) {
-    const uint32_t f = (uint32_t)__ffsll((long long)vm) - 1;
-    uint32_t cnt = 0;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) cnt |= (uint32_t)((pl[k] >> f) & 1ull) << k;
-    cnt = __reduce_add_sync(FULL, cnt);
-    if (lane == 0 && cnt) atomicAdd(&s.vcnt[(size_t)pc.x * 64 + f], cnt);
-  }
-}
-
-template <typename IdxT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vcount(View v, LevelScratch s) {
-  const uint32_t count = live_count(s, s.ctr->n_vpieces, s.cap_vpieces);
-  const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_VCOUNT], [&](uint32_t pi) { vcount_item<IdxT>(v, sl, s, pi); });
-}
-
-// Per-warp shared memory: [max_features][n_classes] class counts.
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void vclass_item(const View& v, const StepLists& lists, const LevelScratch& s,
-                                            uint32_t* cnt, uint32_t pi) {
-  const uint32_t lane = lane_id();
-  const uint32_t C = v.n_classes, m = v.max_features;
-  const uint2 pc = s.vpieces[pi];
-  const uint32_t w = pc.x;
-  const uint32_t nsel = s.nsel[w];
-  // selected slots holding virtual features (m <= 64)
-  uint64_t vs = 0;
-  for (uint32_t q0 = 0; q0 < nsel; q0 += 32) {
-    const uint32_t q = q0 + lane;
-    const bool vq = q < nsel && is_virtual(v, s.sel[(size_t)w * m + q]);
-    vs |= (uint64_t)__ballot_sync(FULL, vq) << q0;
-  }
-  if (!vs) return;
-  for (uint64_t b = vs; b; b &= b - 1) {
-    const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
-    for (uint32_t c = lane; c < C; c += 32) cnt[q * C + c] = 0;
+    const uint32_t e = (uint32_t)__ldcs(rl + i);
+    const uint32_t lab = entry_label<LabT>(v, e);
+    for (uint64_t b = __ldg(v.vrow + entry_row(v, e)); b; b &= b - 1)
+      atomicAdd(&cnt[((uint32_t)__ffsll((long long)b) - 1) * C + lab], 1u);
   }
   __syncwarp();
-  const ct_node nd = lists.nodes[w];
-  const IdxT* rl = list_ptr<IdxT>(v, nd.buf, nd.slot, v.vslot) + nd.start;
-  const uint32_t lo = pc.y * VPIECE;
-  const uint32_t hi = min(lo + VPIECE, nd.n);
-  for (uint32_t i0 = lo; i0 < hi; i0 += 32) {
-    const uint32_t i = i0 + lane;
-    uint32_t lab = NONE;
-    uint64_t bits = 0;
-    if (i < hi) {
-      const uint32_t e = (uint32_t)__ldcs(rl + i);
-      lab = entry_label<LabT>(v, e);
-      bits = __ldg(v.vrow + entry_row(v, e));
-    }
-    for (uint64_t b = vs; b; b &= b - 1) {
-      const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
-      const uint32_t f = s.sel[(size_t)w * m + q];
-      const uint32_t key = ((bits >> f) & 1ull) ? lab : NONE;
-      const unsigned grp = __match_any_sync(FULL, key);
-      if (key != NONE && (grp >> lane) == 1u) cnt[q * C + key] += __popc(grp);
-      __syncwarp();
-    }
-  }
   if (lane == 0) atomicAdd(&s.ctr->vrows, (unsigned long long)(hi - lo));
-  for (uint64_t b = vs; b; b &= b - 1) {
-    const uint32_t q = (uint32_t)__ffsll((long long)b) - 1;
-    for (uint32_t c = lane; c < C; c += 32)
-      if (cnt[q * C + c]) atomicAdd(&s.vcls[((size_t)w * m + q) * C + c], cnt[q * C + c]);
+  uint32_t* out = s.vcls + (size_t)pc.x * fc;
+  for (uint32_t i = lane; i < fc; i += 32)
+    if (cnt[i]) atomicAdd(&out[i], cnt[i]);
+  for (uint32_t f = lane; f < v.n_features; f += 32) {
+    if (!is_virtual(v, f)) continue;
+    uint32_t t = 0;
+    for (uint32_t c = 0; c < C; ++c) t += cnt[f * C + c];
+    if (t) atomicAdd(&s.vcnt[(size_t)pc.x * 64 + f], t);
   }
 }
 
 template <typename IdxT, typename LabT>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vclass(View v, LevelScratch s) {
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vcount(View v, LevelScratch s) {
   extern __shared__ uint32_t smem[];
-  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.max_features * v.n_classes;
+  uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_features * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_vpieces, s.cap_vpieces);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_VCLASS], [&](uint32_t pi) { vclass_item<IdxT, LabT>(v, sl, s, cnt, pi); });
+  for_items(count, &s.ctr->claim[ITEM_VCOUNT], [&](uint32_t pi) { vcount_item<IdxT, LabT>(v, sl, s, cnt, pi); });
 }
 
 // ------------------------------------------------------------------------
@@ -684,7 +625,7 @@ __device__ __forceinline__ void split_reduce_item(const View& v, const StepLists
   warp_argmin3(best, bf, bp, il, ir);
   if (v.vmask) {
     // virtual features: one candidate each, the last low-value row, with the
-    // class counts of the high-value rows from k_vclass (the same exact
+    // class counts of the high-value rows from k_vcount (the same exact
     // arithmetic as the scan; the same (score, feature, position) order)
     const uint32_t nsel = s.nsel[w];
     const ct_node nd = lists.nodes[w];
@@ -698,7 +639,7 @@ __device__ __forceinline__ void split_reduce_item(const View& v, const StepLists
       const uint32_t pos = nd.n - s.vcnt[(size_t)w * 64 + f] - 1;
       int64_t sl = 0, sr = 0;
       for (uint32_t c = lane; c < C; c += 32) {
-        const int64_t r = s.vcls[((size_t)w * m + q) * C + c];
+        const int64_t r = s.vcls[((size_t)w * v.n_features + f) * C + c];
         const int64_t l = (int64_t)lists.tot[(size_t)w * C + c] - r;
         sl += l * l;
         sr += r * r;
@@ -1564,8 +1505,10 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
   if (v.vmask) {  // counts of the virtual features, before the selection reads them
     pf->begin(CT_K_SCAN);
+    const size_t smv = (size_t)WARPS_PER_BLOCK * v.n_features * v.n_classes * sizeof(uint32_t);
     k_vpieces<<<grid_for(k_vpieces, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
-    k_vcount<IdxT><<<grid_for(k_vcount<IdxT>, caps.vpieces, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
+    k_vcount<IdxT, LabT><<<grid_for(k_vcount<IdxT, LabT>, caps.vpieces, smv, persistent), THREADS_PER_BLOCK, smv,
+                           st>>>(v, s);
     pf->end();
     pf->launched(CT_K_SCAN, 2);
   }
@@ -1582,13 +1525,8 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
   if (v.fbin)
     k_scan_two_valued<IdxT, LabT><<<grid_for(k_scan_two_valued<IdxT, LabT>, caps.scan, sm1, persistent),
                                     THREADS_PER_BLOCK, sm1, st>>>(v, s, scan_piece);
-  if (v.vmask) {
-    const size_t smv = (size_t)WARPS_PER_BLOCK * v.max_features * v.n_classes * sizeof(uint32_t);
-    k_vclass<IdxT, LabT><<<grid_for(k_vclass<IdxT, LabT>, caps.vpieces, smv, persistent), THREADS_PER_BLOCK, smv,
-                           st>>>(v, s);
-  }
   pf->end();
-  pf->launched(CT_K_SCAN, (v.fbin ? 4 : 3) + (v.vmask ? 1 : 0));
+  pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
   pf->begin(CT_K_REDUCE);
   k_split_reduce<IdxT><<<grid_for(k_split_reduce<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
   pf->end();
@@ -1669,7 +1607,7 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   t.step = a.take<StepLists>(1);
   t.vcnt = virt ? a.take<uint32_t>((size_t)c.nodes * 64) : nullptr;
-  t.vcls = virt ? a.take<uint32_t>((size_t)c.nodes * v.max_features * C) : nullptr;
+  t.vcls = virt ? a.take<uint32_t>((size_t)c.nodes * v.n_features * C) : nullptr;
   t.vpieces = virt ? a.take<uint2>(c.vpieces) : nullptr;
   t.cap_vpieces = virt ? c.vpieces : 0u;
   if (s) *s = t;
@@ -1688,7 +1626,7 @@ bool carve_level_scratch(Arena& a, const View& v, const LevelCaps& c, LevelScrat
 
 bool virtual_possible(const ct_problem* p) {
   return p->n_features >= 2 && p->n_features <= 64 && fit_label_shift(p) != 0 &&
-         (uint64_t)p->max_features * p->n_classes <= 2048;
+         (uint64_t)p->n_features * p->n_classes <= 2048;
 }
 
 #define CT_DISPATCH(IB, LB, CALL)                                   \
@@ -1794,51 +1732,73 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
 }
 
 namespace {
-// One block per feature: the row's minimum and maximum, then whether every
-// value equals one of them (float equality: -0.0 == +0.0).
-__global__ void k_feature_flags(const float* __restrict__ x_fm, uint32_t n_rows, uint32_t* bits, float2* vals) {
-  __shared__ float s_mn[32], s_mx[32];
-  const uint32_t f = blockIdx.x;
+// Feature flags over a (row chunk, feature) grid: the minimum and maximum of
+// each feature (as order-preserving bits, -0.0 folded onto +0.0), then
+// whether some row holds a third value.
+constexpr uint32_t FLAG_ROWS = 8192;  // rows per block
+
+__global__ void k_ff_minmax(const float* __restrict__ x_fm, uint32_t n_rows, uint2* __restrict__ mm) {
+  const uint32_t f = blockIdx.y;
   const float* xr = x_fm + (size_t)f * n_rows;
-  float mn = xr[0], mx = xr[0];
-  for (uint32_t i = threadIdx.x; i < n_rows; i += blockDim.x) {
-    const float x = xr[i];
-    mn = fminf(mn, x);
-    mx = fmaxf(mx, x);
+  const uint32_t lo = blockIdx.x * FLAG_ROWS, hi = min(lo + FLAG_ROWS, n_rows);
+  uint32_t mn = 0xffffffffu, mx = 0u;
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t o = f32_order(xr[i]);
+    mn = min(mn, o);
+    mx = max(mx, o);
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    mn = fminf(mn, __shfl_xor_sync(FULL, mn, o));
-    mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, o));
-  }
+  mn = __reduce_min_sync(FULL, mn);
+  mx = __reduce_max_sync(FULL, mx);
   if (lane_id() == 0) {
-    s_mn[threadIdx.x >> 5] = mn;
-    s_mx[threadIdx.x >> 5] = mx;
+    atomicMin(&mm[f].x, mn);
+    atomicMax(&mm[f].y, mx);
   }
-  __syncthreads();
-  mn = s_mn[0];
-  mx = s_mx[0];
-  for (uint32_t w = 1; w < blockDim.x / 32; ++w) {
-    mn = fminf(mn, s_mn[w]);
-    mx = fmaxf(mx, s_mx[w]);
+}
+
+__global__ void k_ff_third(const float* __restrict__ x_fm, uint32_t n_rows, const uint2* __restrict__ mm,
+                           uint32_t* __restrict__ third) {
+  const uint32_t f = blockIdx.y;
+  const float* xr = x_fm + (size_t)f * n_rows;
+  const uint32_t lo = blockIdx.x * FLAG_ROWS, hi = min(lo + FLAG_ROWS, n_rows);
+  const uint2 b = mm[f];
+  bool other = false;
+  for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const uint32_t o = f32_order(xr[i]);
+    other |= o != b.x && o != b.y;
   }
-  if (vals && threadIdx.x == 0) vals[f] = make_float2(mn, mx);
-  bool ok = true;
-  for (uint32_t i = threadIdx.x; i < n_rows && ok; i += blockDim.x) {
-    const float x = xr[i];
-    ok = (x == mn) || (x == mx);
+  if (__any_sync(FULL, other) && lane_id() == 0) atomicOr(third + (f >> 5), 1u << (f & 31));
+}
+
+__global__ void k_ff_final(const uint2* __restrict__ mm, const uint32_t* __restrict__ third, uint32_t n_features,
+                           uint32_t* __restrict__ bits, float2* vals) {
+  for (uint32_t f = threadIdx.x; f < n_features; f += blockDim.x) {
+    if (vals) vals[f] = make_float2(f32_unorder(mm[f].x), f32_unorder(mm[f].y));
+    if (!((third[f >> 5] >> (f & 31)) & 1u)) atomicOr(bits + (f >> 5), 1u << (f & 31));
   }
-  if (!__syncthreads_and(ok)) return;
-  if (threadIdx.x == 0) atomicOr(bits + (f >> 5), 1u << (f & 31));
 }
 }  // namespace
 
+// work: feature_flags_work_bytes(n_features) of device scratch (the
+// per-feature minimum/maximum bits and the third-value words).
 int feature_flags(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t* bits, float2* vals,
-                  cudaStream_t st) {
-  CT_CUDA_TRY(cudaMemsetAsync(bits, 0, ((n_features + 31) / 32) * sizeof(uint32_t), st));
-  k_feature_flags<<<n_features, 256, 0, st>>>(x_fm, n_rows, bits, vals);
+                  void* work, cudaStream_t st) {
+  const uint32_t words = (n_features + 31) / 32;
+  uint2* mm = reinterpret_cast<uint2*>(work);
+  uint32_t* third = reinterpret_cast<uint32_t*>(mm + n_features);
+  CT_CUDA_TRY(cudaMemsetAsync(bits, 0, words * sizeof(uint32_t), st));
+  CT_CUDA_TRY(cudaMemsetAsync(third, 0, words * sizeof(uint32_t), st));
+  CT_CUDA_TRY(cudaMemsetAsync(mm, 0xff, n_features * sizeof(uint2), st));  // min: all ones
+  CT_CUDA_TRY(cudaMemset2DAsync(reinterpret_cast<char*>(mm) + 4, sizeof(uint2), 0, 4, n_features, st));  // max: 0
+  const dim3 grid(ceil_div(n_rows, FLAG_ROWS), n_features);
+  k_ff_minmax<<<grid, 256, 0, st>>>(x_fm, n_rows, mm);
+  k_ff_third<<<grid, 256, 0, st>>>(x_fm, n_rows, mm, third);
+  k_ff_final<<<1, 256, 0, st>>>(mm, third, n_features, bits, vals);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
+}
+
+size_t feature_flags_work_bytes(uint32_t n_features) {
+  return n_features * sizeof(uint2) + ((n_features + 31) / 32) * sizeof(uint32_t);
 }
 
 namespace {
