@@ -99,7 +99,10 @@ struct Counters {
   uint32_t n_big_segs;
   uint32_t n_tiles;       // partition tiles of big splits
   uint32_t n_vpieces;     // row-list pieces (virtual features)
-  uint32_t pad[2];
+  uint32_t n_huge_segs;   // partition segments of k_part_seg
+  uint32_t n_hchains;     // their chains (quads)
+  uint32_t ticket_huge;   // k_part_seg's unit counter
+  uint32_t pad;
   uint32_t claim[16];     // item counters of persistent launches (ITEM_* slots)
   unsigned long long next_total;
   unsigned long long small_total;
@@ -122,6 +125,9 @@ enum : uint32_t {
 __device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_nodes) {
   for (uint32_t i = 0; i < ITEM_STEP_SLOTS; ++i) c->claim[i] = 0;
   c->n_vpieces = 0;
+  c->n_huge_segs = 0;
+  c->n_hchains = 0;
+  c->ticket_huge = 0;
   c->n_nodes = n_nodes;
   c->n_scan_pieces = 0;
   c->n_carry = 0;
@@ -168,6 +174,12 @@ struct PartWork {
   PartSeg* big;
   uint32_t* n_big;
   uint32_t cap_big;
+  PartSeg* huge;          // segments of k_part_seg (NULL: none)
+  const uint2* hchains;   // their active chains (segment, feature or NONE), quads
+  uint32_t* n_hchains;
+  uint32_t cap_hchains;
+  uint32_t* ticket_huge;
+  uint32_t bit_words;     // mark-bit words of one tree
   PartTile* tiles;
   uint32_t* n_tiles;
   uint32_t cap_tiles;
@@ -321,6 +333,10 @@ struct LevelScratch {
   PartPiece* part;        // [cap_part] mark-table pieces
   PartSeg* small_segs;    // [cap_nodes]
   PartSeg* big_segs;      // [cap_nodes]
+  PartSeg* huge_segs;     // [cap_huge] segments of at least HUGE_SEG rows (k_part_seg)
+  uint2* hchains;         // [cap_hchains] their active chains in quads
+  uint32_t cap_huge;
+  uint32_t cap_hchains;
   PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
@@ -401,6 +417,13 @@ constexpr uint32_t DEFAULT_SCAN_PIECE = 2048;   // elements per split-scan work 
 constexpr uint32_t PART_ROUNDS = 16;            // rounds of 32 held in registers
 constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
 constexpr uint32_t TILE_ELEMS = 4096;           // partition tile of big segments
+// Segments of at least HUGE_SEG rows are partitioned with the tree's mark
+// bits staged in shared memory (k_part_seg) when those bits fit the budget.
+constexpr uint32_t HUGE_SEG = 16384;
+constexpr uint32_t HUGE_BITS_MAX = 150u * 1024u;
+__host__ __device__ __forceinline__ bool huge_partition_ok(uint32_t bit_words) {
+  return (uint64_t)bit_words * 4u <= HUGE_BITS_MAX;
+}
 constexpr uint32_t SMALL_SEG = 32 * PART_ROUNDS; // segments up to this size: one warp
 constexpr int WARPS_PER_BLOCK = 4;
 constexpr int THREADS_PER_BLOCK = 32 * WARPS_PER_BLOCK;
@@ -411,7 +434,7 @@ struct LevelBounds {
   uint64_t samples;
 };
 struct LevelCaps {
-  uint32_t nodes, scan, carry, part, status, vpieces;
+  uint32_t nodes, scan, carry, part, status, vpieces, huge, hchains;
 };
 LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b);
 constexpr uint32_t VPIECE = 2048;  // rows per row-list piece (virtual features)

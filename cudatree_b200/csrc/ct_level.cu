@@ -735,21 +735,22 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   if (!split) return;
   const uint32_t npp = ceil_div(nd.n, PART_PIECE);
   const bool big = nd.n > SMALL_SEG;
+  const bool huge = big && nd.n >= HUGE_SEG && s.huge_segs && huge_partition_ok(v.bit_words);
   const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
+  const uint64_t skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
   uint32_t sidx = 0, pbase = 0, tbase = 0, gidx = 0, ok = 1;
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
     atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
-    const uint64_t skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
     atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * (v.n_features - (uint32_t)__popcll(skip)));
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
     if (big) {
-      gidx = atomicAdd(&s.ctr->n_big_segs, 1u);
+      gidx = atomicAdd(huge ? &s.ctr->n_huge_segs : &s.ctr->n_big_segs, 1u);
       tbase = atomicAdd(&s.ctr->n_tiles, ntiles);
     } else {
       gidx = atomicAdd(&s.ctr->n_small_segs, 1u);
     }
-    if (sidx >= s.cap_nodes || gidx >= s.cap_nodes || pbase + (uint64_t)npp > s.cap_part ||
+    if (sidx >= s.cap_nodes || gidx >= (huge ? s.cap_huge : s.cap_nodes) || pbase + (uint64_t)npp > s.cap_part ||
         (big && tbase + (uint64_t)ntiles > s.cap_status)) {
       atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
       ok = 0;
@@ -769,8 +770,8 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
       sg.n = nd.n;
       sg.nl = r.pos + 1;
       sg.status = tbase;
-      sg.skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
-      (big ? s.big_segs : s.small_segs)[gidx] = sg;
+      sg.skip = skip;
+      (huge ? s.huge_segs : big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
   ok = __shfl_sync(FULL, ok, 0);
@@ -795,6 +796,32 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
     tl.ntiles = ntiles;
     tl.pad = 0;
     s.tiles[tbase + j] = tl;
+  }
+  if (huge) {
+    // the segment's active chains (features whose lists move), padded to a
+    // multiple of four so that k_part_seg's quads never span two segments
+    const uint32_t F = v.n_features;
+    const uint32_t nact = F - (uint32_t)__popcll(skip);
+    const uint32_t nq4 = (nact + 3u) & ~3u;
+    uint32_t hb = 0;
+    if (lane == 0) {
+      hb = atomicAdd(&s.ctr->n_hchains, nq4);
+      if (hb + (uint64_t)nq4 > s.cap_hchains) {
+        atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
+        hb = NONE;
+      }
+    }
+    hb = __shfl_sync(FULL, hb, 0);
+    if (hb == NONE) return;
+    uint32_t done = 0;
+    for (uint32_t f0 = 0; f0 < F; f0 += 32) {
+      const uint32_t f = f0 + lane;
+      const bool act = f < F && !masked(skip, f);
+      const unsigned am = __ballot_sync(FULL, act);
+      if (act) s.hchains[hb + done + __popc(am & lanemask_lt())] = make_uint2(gidx, f);
+      done += __popc(am);
+    }
+    for (uint32_t i = nact + lane; i < nq4; i += 32) s.hchains[hb + i] = make_uint2(gidx, NONE);
   }
 }
 
@@ -1578,6 +1605,8 @@ LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b) {
   c.part = clamp32(b.samples / PART_PIECE + b.nodes + 1);
   c.status = clamp32(b.samples / TILE_ELEMS + b.samples / (SMALL_SEG + 1) + 1);  // tiles of big splits
   c.vpieces = clamp32(b.samples / VPIECE + b.nodes + 1);
+  c.huge = clamp32(b.samples / HUGE_SEG + 1);
+  c.hchains = clamp32((uint64_t)c.huge * (v.n_features + 3));
   return c;
 }
 
@@ -1603,6 +1632,11 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.part = a.take<PartPiece>(c.part);
   t.small_segs = a.take<PartSeg>(c.nodes);
   t.big_segs = a.take<PartSeg>(c.nodes);
+  const bool huge = huge_partition_ok(v.bit_words);
+  t.huge_segs = huge ? a.take<PartSeg>(c.huge) : nullptr;
+  t.hchains = huge ? a.take<uint2>(c.hchains) : nullptr;
+  t.cap_huge = huge ? c.huge : 0u;
+  t.cap_hchains = huge ? c.hchains : 0u;
   t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   t.step = a.take<StepLists>(1);
@@ -1719,6 +1753,12 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   w.big = s.big_segs;
   w.n_big = &s.ctr->n_big_segs;
   w.cap_big = s.cap_nodes;
+  w.huge = s.huge_segs;
+  w.hchains = s.hchains;
+  w.n_hchains = &s.ctr->n_hchains;
+  w.cap_hchains = s.cap_hchains;
+  w.ticket_huge = &s.ctr->ticket_huge;
+  w.bit_words = v.bit_words;
   w.tiles = s.tiles;
   w.n_tiles = &s.ctr->n_tiles;
   w.cap_tiles = s.cap_status;

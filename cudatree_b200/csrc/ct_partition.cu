@@ -193,14 +193,48 @@ constexpr uint32_t ring_buf_bytes() {
   return BIG_WARPS * 32 * ROUNDS * sizeof(IdxT) + 128;
 }
 
-// One tile of a chain: the left flags of the CTA's BIG_WARPS * 32 * ROUNDS
-// positions, the CTA's prefix of left counts, and the stable stores; returns
-// the tile's left count.  WHOLE: the tile is full, so positions need no range check.
-template <typename IdxT, uint32_t ROUNDS, bool WHOLE>
-__device__ __forceinline__ uint32_t part_tile(const IdxT* rows, uint32_t cnt, uint32_t lo, const PartSeg& sg,
-                                              uint32_t row_mask, IdxT* out, uint32_t n, uint32_t carry,
-                                              uint32_t* s_wcnt) {
-  const uint32_t lane = lane_id(), warp = threadIdx.x >> 5;
+// Where a chain's partition runs.  CtaEnv: a k_part_big CTA of BIG_WARPS
+// warps, mark bits read from global memory (L1).  GroupEnv: one group of
+// BIG_WARPS warps of a k_part_seg CTA, mark bits staged in shared memory.
+struct CtaEnv {
+  const uint32_t* bits;
+  __device__ uint32_t warp() const { return threadIdx.x >> 5; }
+  __device__ bool leader() const { return threadIdx.x == 0; }
+  __device__ void sync() const { __syncthreads(); }
+  __device__ bool all(bool ok) const { return __syncthreads_and(ok); }
+  __device__ bool left(uint32_t row) const { return left_bit(bits, row); }
+};
+
+constexpr uint32_t SEG_GROUPS = 4;  // k_part_seg: groups of BIG_WARPS warps per CTA
+constexpr uint32_t SEG_THREADS = SEG_GROUPS * BIG_THREADS;
+
+struct GroupEnv {
+  const uint32_t* sbits;
+  uint32_t g;
+  __device__ uint32_t warp() const { return (threadIdx.x >> 5) - g * BIG_WARPS; }
+  __device__ bool leader() const { return threadIdx.x == g * BIG_THREADS; }
+  __device__ void sync() const { asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(BIG_THREADS) : "memory"); }
+  __device__ bool all(bool ok) const {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.and.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}"
+        : "=r"(r)
+        : "r"((uint32_t)ok), "r"(g + 1), "r"(BIG_THREADS)
+        : "memory");
+    return r != 0;
+  }
+  __device__ bool left(uint32_t row) const { return (sbits[row >> 5] >> (row & 31)) & 1u; }
+};
+
+// One tile of a chain: the left flags of the group's BIG_WARPS * 32 * ROUNDS
+// positions, the group's prefix of left counts, and the stable stores;
+// returns the tile's left count.  WHOLE: the tile is full, so positions need
+// no range check.
+template <typename IdxT, uint32_t ROUNDS, bool WHOLE, typename Env>
+__device__ __forceinline__ uint32_t part_tile(const Env& env, const IdxT* rows, uint32_t cnt, uint32_t lo,
+                                              const PartSeg& sg, uint32_t row_mask, IdxT* out, uint32_t n,
+                                              uint32_t carry, uint32_t* s_wcnt) {
+  const uint32_t lane = lane_id(), warp = env.warp();
   const unsigned lt = lanemask_lt();
   const uint32_t wlo = warp * (32 * ROUNDS);
   unsigned lmask[ROUNDS];
@@ -211,12 +245,12 @@ __device__ __forceinline__ uint32_t part_tile(const IdxT* rows, uint32_t cnt, ui
     const uint32_t q = wlo + r * 32 + lane;
     const bool in = WHOLE || q < cnt;
     e[r] = rows[in ? q : 0];
-    const bool left = in && left_bit(sg.bits, (uint32_t)e[r] & row_mask);
+    const bool left = in && env.left((uint32_t)e[r] & row_mask);
     lmask[r] = __ballot_sync(FULL, left);
     wc += __popc(lmask[r]);
   }
   if (lane == 0) s_wcnt[warp] = wc;
-  __syncthreads();
+  env.sync();
   // the warps' left counts: lane k of every warp holds warp k's, scanned over 8 lanes
   static_assert(BIG_WARPS == 8, "the count prefix scans 8 lanes");
   uint32_t v = s_wcnt[lane & 7u];
@@ -242,12 +276,69 @@ __device__ __forceinline__ uint32_t part_tile(const IdxT* rows, uint32_t cnt, ui
   return total;
 }
 
-template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
-__global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
+// One (segment, feature) chain through a ring of RING tile buffers: tiles
+// arrive by bulk copies RING-1 ahead of the one being partitioned; the left
+// count carried between tiles is a register.  g counts the tiles this ring
+// has consumed, uses[b] the completed phases of buffer b.  Returns false
+// (error word set, the ring drained, bounded) when a copy did not arrive.
+template <typename IdxT, uint32_t ROUNDS, uint32_t RING, typename Env>
+__device__ __forceinline__ bool run_chain(const Env& env, const PartWork& w, const PartSeg& sg, uint32_t f,
+                                          unsigned char* ring, uint64_t* bars, uint32_t* s_off, uint32_t* s_wcnt,
+                                          uint32_t (&uses)[RING], uint32_t& g, uint64_t stream_pol) {
   constexpr uint32_t TILE = BIG_WARPS * 32 * ROUNDS;
   constexpr uint32_t BUF = ring_buf_bytes<IdxT, ROUNDS>();
+  unsigned char(*sbuf)[BUF] = reinterpret_cast<unsigned char(*)[BUF]>(ring);
+  const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
+  IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
+  const uint32_t n = sg.n;
+  const uint32_t ntiles = ceil_div(n, TILE);
+  if (env.leader())
+    for (uint32_t j = 0; j < RING - 1 && j < ntiles; ++j)
+      issue_tile<IdxT, TILE>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING],
+                             stream_pol);
+  uint32_t carry = 0;
+  for (uint32_t j = 0; j < ntiles; ++j, ++g) {
+    const uint32_t b = g % RING;
+    if (env.leader() && j + RING - 1 < ntiles) {  // refill the buffer freed by tile j-1
+      const uint32_t bn = (g + RING - 1) % RING;
+      issue_tile<IdxT, TILE>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn], stream_pol);
+    }
+    bool ok = true;
+    {
+      uint32_t spins = 0;
+      while (!mbar_try_wait(&bars[b], uses[b] & 1u)) {
+        if (++spins > (SPIN_LIMIT << 2)) {
+          ok = false;
+          break;
+        }
+      }
+    }
+    if (!env.all(ok)) {
+      // never read a tile that did not arrive: flag, drain the ring (bounded), leave
+      if (env.leader()) atomicOr(w.error, DEV_ERR_TIMEOUT);
+      for (uint32_t k = 0; k < RING && j + k < ntiles; ++k) {  // tiles j .. j+RING-1 may be in flight
+        const uint32_t bb = (g + k) % RING;
+        uint32_t spins = 0;
+        while (!mbar_try_wait(&bars[bb], uses[bb] & 1u) && ++spins < (SPIN_LIMIT << 4)) {
+        }
+        uses[bb] += 1;
+      }
+      return false;
+    }
+    uses[b] += 1;
+    const uint32_t lo = j * TILE;
+    const uint32_t cnt = min(TILE, n - lo);
+    const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
+    carry += cnt == TILE ? part_tile<IdxT, ROUNDS, true>(env, rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt)
+                         : part_tile<IdxT, ROUNDS, false>(env, rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt);
+    env.sync();  // tile buffer and s_wcnt free for reuse
+  }
+  return true;
+}
+
+template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
+__global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   extern __shared__ __align__(128) unsigned char ring_smem[];
-  unsigned char(*sbuf)[BUF] = reinterpret_cast<unsigned char(*)[BUF]>(ring_smem);
   __shared__ alignas(8) uint64_t bars[RING];
   __shared__ uint32_t s_off[RING];
   __shared__ uint32_t s_chain;
@@ -262,7 +353,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   uint32_t uses[RING];  // completed phases per ring buffer (uniform)
 #pragma unroll
   for (uint32_t i = 0; i < RING; ++i) uses[i] = 0;
-  uint32_t g = 0;                      // tiles consumed by this CTA (ring position)
+  uint32_t g = 0;  // tiles consumed by this CTA (ring position)
   while (true) {
     __syncthreads();
     if (threadIdx.x == 0) s_chain = atomicAdd(w.ticket, 1u);
@@ -275,50 +366,85 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
     const uint32_t f = c - si * w.n_features;
     const PartSeg sg = w.big[si];
     if (masked(sg.skip, f)) continue;  // constant in the node: its lists are never read again
-    const IdxT* in = reinterpret_cast<const IdxT*>(sg.in) + (size_t)f * sg.in_fstride;
-    IdxT* out = reinterpret_cast<IdxT*>(sg.out) + (size_t)f * sg.out_fstride;
-    const uint32_t n = sg.n;
-    const uint32_t ntiles = ceil_div(n, TILE);
-    if (threadIdx.x == 0)
-      for (uint32_t j = 0; j < RING - 1 && j < ntiles; ++j)
-        issue_tile<IdxT, TILE>(in, n, j, sbuf[(g + j) % RING], &bars[(g + j) % RING], &s_off[(g + j) % RING],
-                               stream_pol);
-    uint32_t carry = 0;
-    for (uint32_t j = 0; j < ntiles; ++j, ++g) {
-      const uint32_t b = g % RING;
-      if (threadIdx.x == 0 && j + RING - 1 < ntiles) {  // refill the buffer freed by tile j-1
-        const uint32_t bn = (g + RING - 1) % RING;
-        issue_tile<IdxT, TILE>(in, n, j + RING - 1, sbuf[bn], &bars[bn], &s_off[bn], stream_pol);
+    const CtaEnv env{sg.bits};
+    if (!run_chain<IdxT, ROUNDS, RING>(env, w, sg, f, ring_smem, bars, s_off, s_wcnt, uses, g, stream_pol)) return;
+  }
+}
+
+// Segments of at least HUGE_SEG rows, when the tree's mark bits fit shared
+// memory (huge_partition_ok): one CTA of SEG_GROUPS groups per SM.  A work
+// unit is a quad of the segment's active chains (k_plan lists them, padded
+// to quads, so a quad never spans two segments); the CTA stages the
+// segment's tree's mark bits in shared memory by one bulk copy (kept while
+// consecutive units share the tree) and each group partitions one chain of
+// the quad with a bit lookup in shared memory: a divergent load of 32 rows
+// there costs a few bank cycles, against up to 32 L1 wavefronts.
+template <typename IdxT, uint32_t ROUNDS, uint32_t RING>
+__global__ void __launch_bounds__(SEG_THREADS, 1) k_part_seg(PartWork w) {
+  constexpr uint32_t BUF = ring_buf_bytes<IdxT, ROUNDS>();
+  extern __shared__ __align__(128) unsigned char seg_smem[];
+  __shared__ alignas(8) uint64_t bars[SEG_GROUPS][RING];
+  __shared__ alignas(8) uint64_t bits_bar;
+  __shared__ uint32_t s_off[SEG_GROUPS][RING];
+  __shared__ uint32_t s_wcnt[SEG_GROUPS][BIG_WARPS];
+  __shared__ uint32_t s_unit;
+  __shared__ uint32_t s_fail;
+  const uint32_t bit_bytes = w.bit_words * 4u;
+  uint32_t* sbits = reinterpret_cast<uint32_t*>(seg_smem);
+  const uint32_t g = threadIdx.x / BIG_THREADS;
+  unsigned char* ring = seg_smem + ((bit_bytes + 127u) & ~127u) + (size_t)g * RING * BUF;
+  const uint32_t nq = live(w, w.n_hchains, w.cap_hchains) / SEG_GROUPS;
+  const uint64_t stream_pol = l2_evict_first();
+  const uint64_t keep_pol = l2_evict_last();  // mark bits are staged again by later units
+  if (threadIdx.x == 0) {
+    for (uint32_t k = 0; k < SEG_GROUPS; ++k)
+      for (uint32_t i = 0; i < RING; ++i) mbar_init(&bars[k][i], 1);
+    mbar_init(&bits_bar, 1);
+    mbar_fence_init();
+    s_fail = 0;
+  }
+  uint32_t uses[RING];
+#pragma unroll
+  for (uint32_t i = 0; i < RING; ++i) uses[i] = 0;
+  uint32_t gpos = 0, bits_uses = 0;
+  const uint32_t* staged = nullptr;
+  while (true) {
+    __syncthreads();  // every group is done with the previous unit (its bits, its chain)
+    if (threadIdx.x == 0) s_unit = atomicAdd(w.ticket_huge, 1u);
+    __syncthreads();
+    const uint32_t u = s_unit;
+    if (u >= nq || s_fail) break;
+    const uint2 ch = w.hchains[u * SEG_GROUPS + g];
+    const uint2 first = w.hchains[u * SEG_GROUPS];
+    const PartSeg sg = w.huge[first.x];
+    if (sg.bits != staged) {
+      if (threadIdx.x == 0) {
+        mbar_expect_tx(&bits_bar, bit_bytes);
+        bulk_g2s(sbits, sg.bits, bit_bytes, &bits_bar, keep_pol);
       }
+      uint32_t spins = 0;
       bool ok = true;
-      {
-        uint32_t spins = 0;
-        while (!mbar_try_wait(&bars[b], uses[b] & 1u)) {
-          if (++spins > (SPIN_LIMIT << 2)) {
-            ok = false;
-            break;
-          }
+      while (!mbar_try_wait(&bits_bar, bits_uses & 1u)) {
+        if (++spins > (SPIN_LIMIT << 2)) {
+          ok = false;
+          break;
         }
       }
-      if (!__syncthreads_and(ok)) {
-        // never read a tile that did not arrive: flag, drain the ring (bounded), leave
+      if (!__syncthreads_and(ok)) {  // drain the copy (bounded) and leave
         if (threadIdx.x == 0) atomicOr(w.error, DEV_ERR_TIMEOUT);
-        for (uint32_t k = 0; k < RING && j + k < ntiles; ++k) {  // tiles j .. j+RING-1 may be in flight
-          const uint32_t bb = (g + k) % RING;
-          uint32_t spins = 0;
-          while (!mbar_try_wait(&bars[bb], uses[bb] & 1u) && ++spins < (SPIN_LIMIT << 4)) {
-          }
-          uses[bb] += 1;
+        spins = 0;
+        while (!mbar_try_wait(&bits_bar, bits_uses & 1u) && ++spins < (SPIN_LIMIT << 4)) {
         }
         return;
       }
-      uses[b] += 1;
-      const uint32_t lo = j * TILE;
-      const uint32_t cnt = min(TILE, n - lo);
-      const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
-      carry += cnt == TILE ? part_tile<IdxT, ROUNDS, true>(rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt)
-                           : part_tile<IdxT, ROUNDS, false>(rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt);
-      __syncthreads();  // tile buffer and s_wcnt free for reuse
+      bits_uses += 1;
+      staged = sg.bits;
+    }
+    if (ch.y != NONE) {
+      const GroupEnv env{sbits, g};
+      if (!run_chain<IdxT, ROUNDS, RING>(env, w, w.huge[ch.x], ch.y, ring, bars[g], s_off[g], s_wcnt[g], uses, gpos,
+                                         stream_pol))
+        s_fail = 1;
     }
   }
 }
@@ -363,8 +489,32 @@ int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
 
 }  // namespace
 
+template <typename IdxT>
+int launch_seg(const PartWork& w, cudaStream_t st) {
+  constexpr uint32_t ROUNDS = 8, RING = 2;
+  const size_t smem = (((size_t)w.bit_words * 4 + 127) & ~size_t(127)) +
+                      (size_t)SEG_GROUPS * RING * ring_buf_bytes<IdxT, ROUNDS>();
+  static bool configured = false;  // per instantiation: the largest staging it can take
+  if (!configured) {
+    const size_t most = (size_t)HUGE_BITS_MAX + 128 + (size_t)SEG_GROUPS * RING * ring_buf_bytes<IdxT, ROUNDS>();
+    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_seg<IdxT, ROUNDS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)most));
+    configured = true;
+  }
+  int dev = 0, sms = 0;
+  CT_CUDA_TRY(cudaGetDevice(&dev));
+  CT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  k_part_seg<IdxT, ROUNDS, RING><<<(uint32_t)std::max(1, sms), SEG_THREADS, smem, st>>>(w);
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
+
 int launch_seg_partition(uint32_t index_bytes, const PartWork& w, uint64_t bound_small, uint64_t bound_tiles,
                          cudaStream_t st) {
+  if (bound_tiles > 0 && w.huge && huge_partition_ok(w.bit_words)) {
+    if (index_bytes == 2) CT_TRY(launch_seg<uint16_t>(w, st));
+    else CT_TRY(launch_seg<uint32_t>(w, st));
+  }
   if (bound_small > 0) {
     const uint64_t items = bound_small * ceil_div(w.n_features, FEAT_BLOCK);
     const uint64_t want = (items + (SMALL_THREADS / 32) - 1) / (SMALL_THREADS / 32);

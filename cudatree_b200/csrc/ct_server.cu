@@ -269,6 +269,7 @@ class Server {
     ct_fit_options o{};
     o.mode = CT_FIT_BATCHED;
     o.subtree_cutoff = 32;
+    o.flags = CT_FIT_HOST_LOOP;  // as the job fit below
     const size_t ib = p.index_bytes, nf = (size_t)n * f;
     size_t mb = 0;
     mb = (((size_t)t * n + 255) & ~size_t(255)) + (size_t)t * mark_bit_words(n) * 4 + 64;
@@ -727,6 +728,9 @@ class Server {
     ct_fit_options o{};
     o.mode = CT_FIT_BATCHED;
     o.subtree_cutoff = 32;
+    // each job has its own shape and arena, so a loop graph would be built
+    // for one fit and dropped: host-driven levels cost less here
+    o.flags = CT_FIT_HOST_LOOP;
     const size_t wsb = fit_workspace_bytes(&p, T, &o);
     char* ws = a.take<char>(wsb);
     if (!ws || !a.ok()) {

@@ -112,7 +112,15 @@ def test_split_nodes_match_oracle(cuda_device, case):
         assert np.float32(res[i]["threshold"]) == thr
 
 
-@pytest.mark.parametrize("case", CASES[:4])
+HUGE_CASES = [
+    # nodes of at least 16,384 rows take k_part_seg (mark bits staged in shared
+    # memory, four chains per CTA); 3,616 and 10,000 rows take k_part_big
+    (50000, 6, 5, 3, [30000, 16384, 3616], 6, False, (2,)),
+    (80000, 5, 3, 2, [70000, 10000], 7, True, ()),
+]
+
+
+@pytest.mark.parametrize("case", CASES[:4] + HUGE_CASES)
 def test_partition_matches_oracle(cuda_device, case):
     n, f, c, m, sizes, seed, integer, consts = case
     gp, gl, groups, nodes, totals, keys, lists = _grouped_case(n, f, c, m, sizes, seed, integer, consts)
