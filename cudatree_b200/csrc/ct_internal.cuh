@@ -102,7 +102,7 @@ struct Counters {
   uint32_t n_huge_segs;   // partition segments of k_part_seg
   uint32_t n_hchains;     // their chains (quads)
   uint32_t ticket_huge;   // k_part_seg's unit counter
-  uint32_t pad;
+  uint32_t n_bchains;     // active chains of k_part_big's segments
   uint32_t claim[16];     // item counters of persistent launches (ITEM_* slots)
   unsigned long long next_total;
   unsigned long long small_total;
@@ -128,6 +128,7 @@ __device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_node
   c->n_huge_segs = 0;
   c->n_hchains = 0;
   c->ticket_huge = 0;
+  c->n_bchains = 0;
   c->n_nodes = n_nodes;
   c->n_scan_pieces = 0;
   c->n_carry = 0;
@@ -174,6 +175,9 @@ struct PartWork {
   PartSeg* big;
   uint32_t* n_big;
   uint32_t cap_big;
+  const uint2* bchains;   // active chains (segment, feature) of the big segments
+  uint32_t* n_bchains;
+  uint32_t cap_bchains;
   PartSeg* huge;          // segments of k_part_seg (NULL: none)
   const uint2* hchains;   // their active chains (segment, feature or NONE), quads
   uint32_t* n_hchains;
@@ -337,6 +341,8 @@ struct LevelScratch {
   uint2* hchains;         // [cap_hchains] their active chains in quads
   uint32_t cap_huge;
   uint32_t cap_hchains;
+  uint2* bchains;         // [cap_bchains] active chains of the big segments
+  uint32_t cap_bchains;
   PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
@@ -419,7 +425,7 @@ constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
 constexpr uint32_t TILE_ELEMS = 4096;           // partition tile of big segments
 // Segments of at least HUGE_SEG rows are partitioned with the tree's mark
 // bits staged in shared memory (k_part_seg) when those bits fit the budget.
-constexpr uint32_t HUGE_SEG = 16384;
+constexpr uint32_t HUGE_SEG = 4096;
 constexpr uint32_t HUGE_BITS_MAX = 150u * 1024u;
 __host__ __device__ __forceinline__ bool huge_partition_ok(uint32_t bit_words) {
   return (uint64_t)bit_words * 4u <= HUGE_BITS_MAX;
@@ -434,7 +440,7 @@ struct LevelBounds {
   uint64_t samples;
 };
 struct LevelCaps {
-  uint32_t nodes, scan, carry, part, status, vpieces, huge, hchains;
+  uint32_t nodes, scan, carry, part, status, vpieces, huge, hchains, bchains;
 };
 LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b);
 constexpr uint32_t VPIECE = 2048;  // rows per row-list piece (virtual features)

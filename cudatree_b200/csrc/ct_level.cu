@@ -797,16 +797,21 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
     tl.pad = 0;
     s.tiles[tbase + j] = tl;
   }
-  if (huge) {
-    // the segment's active chains (features whose lists move), padded to a
-    // multiple of four so that k_part_seg's quads never span two segments
+  if (big) {
+    // the segment's active chains (features whose lists move): k_part_big and
+    // k_part_seg claim these instead of every (segment, feature); a huge
+    // segment's are padded to a multiple of four so that k_part_seg's quads
+    // never span two segments
     const uint32_t F = v.n_features;
     const uint32_t nact = F - (uint32_t)__popcll(skip);
-    const uint32_t nq4 = (nact + 3u) & ~3u;
+    const uint32_t nlist = huge ? (nact + 3u) & ~3u : nact;
+    uint32_t* count = huge ? &s.ctr->n_hchains : &s.ctr->n_bchains;
+    uint2* list = huge ? s.hchains : s.bchains;
+    const uint32_t cap = huge ? s.cap_hchains : s.cap_bchains;
     uint32_t hb = 0;
     if (lane == 0) {
-      hb = atomicAdd(&s.ctr->n_hchains, nq4);
-      if (hb + (uint64_t)nq4 > s.cap_hchains) {
+      hb = atomicAdd(count, nlist);
+      if (hb + (uint64_t)nlist > cap) {
         atomicOr(&s.ctr->error, DEV_ERR_CAPACITY);
         hb = NONE;
       }
@@ -818,10 +823,10 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
       const uint32_t f = f0 + lane;
       const bool act = f < F && !masked(skip, f);
       const unsigned am = __ballot_sync(FULL, act);
-      if (act) s.hchains[hb + done + __popc(am & lanemask_lt())] = make_uint2(gidx, f);
+      if (act) list[hb + done + __popc(am & lanemask_lt())] = make_uint2(gidx, f);
       done += __popc(am);
     }
-    for (uint32_t i = nact + lane; i < nq4; i += 32) s.hchains[hb + i] = make_uint2(gidx, NONE);
+    for (uint32_t i = nact + lane; i < nlist; i += 32) list[hb + i] = make_uint2(gidx, NONE);
   }
 }
 
@@ -1607,6 +1612,7 @@ LevelCaps level_caps(const View& v, uint32_t scan_piece, LevelBounds b) {
   c.vpieces = clamp32(b.samples / VPIECE + b.nodes + 1);
   c.huge = clamp32(b.samples / HUGE_SEG + 1);
   c.hchains = clamp32((uint64_t)c.huge * (v.n_features + 3));
+  c.bchains = clamp32((b.samples / (SMALL_SEG + 1) + 1) * (uint64_t)v.n_features);
   return c;
 }
 
@@ -1637,6 +1643,8 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.hchains = huge ? a.take<uint2>(c.hchains) : nullptr;
   t.cap_huge = huge ? c.huge : 0u;
   t.cap_hchains = huge ? c.hchains : 0u;
+  t.bchains = a.take<uint2>(c.bchains);
+  t.cap_bchains = c.bchains;
   t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   t.step = a.take<StepLists>(1);
@@ -1753,6 +1761,9 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   w.big = s.big_segs;
   w.n_big = &s.ctr->n_big_segs;
   w.cap_big = s.cap_nodes;
+  w.bchains = s.bchains;
+  w.n_bchains = &s.ctr->n_bchains;
+  w.cap_bchains = s.cap_bchains;
   w.huge = s.huge_segs;
   w.hchains = s.hchains;
   w.n_hchains = &s.ctr->n_hchains;

@@ -167,8 +167,8 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       : "memory");
 }
 
-// Persistent CTAs; each claims a whole (segment, feature) chain from a
-// ticket counter and streams its tiles in order, so the running count of
+// Persistent CTAs; each claims a whole (segment, feature) chain (k_plan lists
+// the active ones) from a ticket counter and streams its tiles in order, so the running count of
 // left rows (the chain's carry) stays in a register and no CTA ever waits
 // for another.  Index tiles arrive by TMA bulk copies into a ring of
 // RING buffers, RING-1 tiles ahead of the one being partitioned.  Copies
@@ -343,8 +343,7 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
   __shared__ uint32_t s_off[RING];
   __shared__ uint32_t s_chain;
   __shared__ uint32_t s_wcnt[BIG_WARPS];
-  const uint32_t nbig = live(w, w.n_big, w.cap_big);
-  const uint64_t chains = (uint64_t)nbig * w.n_features;
+  const uint32_t chains = live(w, w.n_bchains, w.cap_bchains);
   const uint64_t stream_pol = l2_evict_first();  // list tiles are read once
   if (threadIdx.x == 0) {
     for (uint32_t i = 0; i < RING; ++i) mbar_init(&bars[i], 1);
@@ -359,13 +358,12 @@ __global__ void __launch_bounds__(BIG_THREADS, MINB) k_part_big(PartWork w) {
     if (threadIdx.x == 0) s_chain = atomicAdd(w.ticket, 1u);
     __syncthreads();
     const uint32_t c = s_chain;
-    if ((uint64_t)c >= chains) break;
-    // feature-fastest: the chains in flight share few segments (trees), so the
-    // mark bytes they gather stay hot in L2
-    const uint32_t si = c / w.n_features;
-    const uint32_t f = c - si * w.n_features;
-    const PartSeg sg = w.big[si];
-    if (masked(sg.skip, f)) continue;  // constant in the node: its lists are never read again
+    if (c >= chains) break;
+    // a segment's chains are listed together: the chains in flight share few
+    // segments (trees), so the mark bits they gather stay hot in L2
+    const uint2 ch = w.bchains[c];
+    const uint32_t f = ch.y;
+    const PartSeg sg = w.big[ch.x];
     const CtaEnv env{sg.bits};
     if (!run_chain<IdxT, ROUNDS, RING>(env, w, sg, f, ring_smem, bars, s_off, s_wcnt, uses, g, stream_pol)) return;
   }
