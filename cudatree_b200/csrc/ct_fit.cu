@@ -57,7 +57,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
                        TreeView tv, const uint32_t* hist_in, ct_node* out, uint32_t* out_tot, uint32_t cap,
                        Counters* ctr, uint64_t* out_mask) {
   __shared__ uint32_t s_idx;
-  __shared__ unsigned long long s_mask;
+  extern __shared__ unsigned long long s_mask[];  // [mask_words(n_features)] with out_mask
   const uint32_t slot = slot_lo + blockIdx.x;
   const uint32_t C = v.n_classes;
   const uint32_t n = n_in[slot];
@@ -97,16 +97,17 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
     for (uint32_t c = threadIdx.x; c < C; c += blockDim.x)
       out_tot[(size_t)s_idx * C + c] = hist_in[(size_t)blockIdx.x * C + c];
   if (out_mask && s_idx != NONE) {  // features constant over the tree's in-bag rows (feature 0 excepted)
-    if (threadIdx.x == 0) s_mask = 0;
+    const uint32_t mw = mask_words(v.n_features);
+    for (uint32_t k = threadIdx.x; k < mw; k += blockDim.x) s_mask[k] = 0;
     __syncthreads();
-    const uint32_t f = threadIdx.x;
-    if (f > 0 && f < v.n_features && f < 64 && !is_virtual(v, f)) {
+    for (uint32_t f = threadIdx.x; f < v.n_features; f += blockDim.x) {
+      if (f == 0 || is_virtual(v, f)) continue;
       const IdxT* lf = list_ptr<IdxT>(v, 0, slot, f);
       const float* xf = v.x_fm + (size_t)f * v.n_rows;
-      if (xf[entry_row(v, lf[0])] == xf[entry_row(v, lf[n - 1])]) atomicOr(&s_mask, 1ull << f);
+      if (xf[entry_row(v, lf[0])] == xf[entry_row(v, lf[n - 1])]) atomicOr(&s_mask[f >> 6], 1ull << (f & 63));
     }
     __syncthreads();
-    if (threadIdx.x == 0) out_mask[s_idx] = s_mask;
+    for (uint32_t k = threadIdx.x; k < mw; k += blockDim.x) out_mask[(size_t)s_idx * mw + k] = s_mask[k];
   }
 }
 
@@ -161,7 +162,8 @@ struct FitLayout {
   float2* vval;          // [n_features] (low, high) values
   ct_node* list[2];
   uint32_t* tot[2];
-  uint64_t* mask[2];     // constant-feature masks of the lists (batched form, n_features <= 64), else NULL
+  uint64_t* mask[2];     // constant-feature masks of the lists (batched form), else NULL
+  uint32_t mask_words;   // words of one node's mask
   LevelScratch s;
   struct LoopCtl* ctl;   // state of the graph-driven level loop
   void* boot_ws;
@@ -201,11 +203,12 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->vrow = L->virt ? a.take<uint64_t>(p->n_rows) : nullptr;
   L->vval = L->virt ? a.take<float2>(p->n_features) : nullptr;
   // the plain form moves nodes through the host, so only the batched form keeps masks
-  const bool masks = o->mode == CT_FIT_BATCHED && p->n_features <= 64;
+  const bool masks = o->mode == CT_FIT_BATCHED;
+  L->mask_words = mask_words(p->n_features);
   for (int i = 0; i < 2; ++i) {
     L->list[i] = a.take<ct_node>(L->cap_list);
     L->tot[i] = a.take<uint32_t>((size_t)L->cap_list * p->n_classes);
-    L->mask[i] = masks ? a.take<uint64_t>(L->cap_list) : nullptr;
+    L->mask[i] = masks ? a.take<uint64_t>((size_t)L->cap_list * mask_words(p->n_features)) : nullptr;
   }
   L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, slots);
   L->boot_ws = a.take<char>(L->boot_bytes);
@@ -266,8 +269,9 @@ int launch_root(const View& v, const FitLayout& L, uint32_t slot_lo, uint32_t n_
   CT_CUDA_TRY(cudaMemsetAsync(hist, 0, n_slots * C * sizeof(uint32_t), st));
   const uint32_t blocks = std::min<uint32_t>(ceil_div(v.n_rows, 256 * 8), 256);
   k_root_hist<IdxT, LabT><<<dim3(blocks, n_slots), 256, C * sizeof(uint32_t), st>>>(v, L.n_in, slot_lo, hist);
-  k_root<IdxT, LabT><<<n_slots, 128, 0, st>>>(v, L.n_in, slot_lo, seed, tree_lo, tv, hist, L.list[cur],
-                                                L.tot[cur], L.cap_list, L.s.ctr, L.mask[cur]);
+  const size_t smask = L.mask[cur] ? (size_t)L.mask_words * sizeof(uint64_t) : 0;
+  k_root<IdxT, LabT><<<n_slots, 128, smask, st>>>(v, L.n_in, slot_lo, seed, tree_lo, tv, hist, L.list[cur],
+                                                  L.tot[cur], L.cap_list, L.s.ctr, L.mask[cur]);
   current_prof()->launched(CT_K_CHILDREN, 2);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
@@ -303,7 +307,7 @@ StepLists step_lists(const FitLayout& L, int cur, uint32_t lo, uint32_t C) {
   StepLists sl;
   sl.nodes = L.list[cur] + lo;
   sl.tot = L.tot[cur] + (size_t)lo * C;
-  sl.node_mask = L.mask[cur] ? L.mask[cur] + lo : nullptr;
+  sl.node_mask = L.mask[cur] ? L.mask[cur] + (size_t)lo * L.mask_words : nullptr;
   sl.next = L.list[1 - cur];
   sl.next_tot = L.tot[1 - cur];
   sl.next_mask = L.mask[1 - cur];
@@ -362,6 +366,7 @@ struct LoopLists {
   ct_node* list[2];
   uint32_t* tot[2];
   uint64_t* mask[2];
+  uint32_t mask_words;
 };
 
 // The level the loop starts with is the last step's children (the roots, or
@@ -389,7 +394,7 @@ __global__ void k_loop_step(LoopCtl* ctl, Counters* c, StepLists* step, LoopList
   StepLists sl;
   sl.nodes = ll.list[cur] + lo;
   sl.tot = ll.tot[cur] + (size_t)lo * C;
-  sl.node_mask = ll.mask[cur] ? ll.mask[cur] + lo : nullptr;
+  sl.node_mask = ll.mask[cur] ? ll.mask[cur] + (size_t)lo * ll.mask_words : nullptr;
   sl.next = ll.list[cur ^ 1u];
   sl.next_tot = ll.tot[cur ^ 1u];
   sl.next_mask = ll.mask[cur ^ 1u];
@@ -485,7 +490,7 @@ int build_loop_graph(const ct_problem* p, const View& v, const FitLayout& L, con
                      LoopGraph& lg) {
   const uint32_t ib = p->index_bytes, lb = p->label_bytes, C = p->n_classes;
   const LevelBounds b{L.chunk, (uint64_t)L.n_slots * p->n_rows};
-  const LoopLists ll{{L.list[0], L.list[1]}, {L.tot[0], L.tot[1]}, {L.mask[0], L.mask[1]}};
+  const LoopLists ll{{L.list[0], L.list[1]}, {L.tot[0], L.tot[1]}, {L.mask[0], L.mask[1]}, L.mask_words};
   Prof* pf = current_prof();
   CT_CUDA_TRY(cudaGraphCreate(&lg.graph, 0));
   cudaGraphConditionalHandle h;
@@ -638,20 +643,36 @@ View fit_view(const ct_problem* p, const ct_lists* l, const FitLayout& L) {
 // the fit can have virtual features, which ones are (every two-valued
 // feature but feature 0, whose lists give the leaf labels) and their rows'
 // value bits.  One host read of the flags.
-int prepare_features(const ct_problem* p, const FitLayout& L, View* v, cudaStream_t st) {
-  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L.fbin, L.virt ? L.vval : nullptr, L.ffwork, st));
-  if (!L.virt) return CT_OK;
+// Feature flags, virtual features, and whether a batched fit of more than 64
+// features keeps constant-feature masks: with few-valued features, lists go
+// constant in big nodes and the masks save their partition; with continuous
+// features they rarely do, and k_children would only pay for the checks.
+// Two-valued features stand for the few-valued ones: masks are kept when at
+// least one feature in eight is two-valued.
+int prepare_features(const ct_problem* p, FitLayout* L, View* v, cudaStream_t st) {
+  CT_TRY(feature_flags(p->x_fm, p->n_rows, p->n_features, L->fbin, L->virt ? L->vval : nullptr, L->ffwork, st));
+  if (L->mask[0] && p->n_features > 64) {
+    std::vector<uint32_t> fb((p->n_features + 31) / 32);
+    CT_CUDA_TRY(cudaMemcpyAsync(fb.data(), L->fbin, fb.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CT_CUDA_TRY(cudaStreamSynchronize(st));
+    uint64_t two = 0;
+    for (uint32_t w : fb) two += (uint64_t)__builtin_popcount(w);
+    if (two * 8 < p->n_features) L->mask[0] = L->mask[1] = nullptr;
+  }
+  if (!L->virt) return CT_OK;
+  const FitLayout& Lc = *L;
   uint32_t fb[2] = {0, 0};
-  CT_CUDA_TRY(cudaMemcpyAsync(fb, L.fbin, ((p->n_features + 31) / 32) * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  CT_CUDA_TRY(cudaMemcpyAsync(fb, Lc.fbin, ((p->n_features + 31) / 32) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              st));
   CT_CUDA_TRY(cudaStreamSynchronize(st));
   const uint64_t all = p->n_features >= 64 ? ~0ull : (1ull << p->n_features) - 1ull;
   const uint64_t vm = (((uint64_t)fb[1] << 32) | fb[0]) & all & ~1ull;
   if (!vm) return CT_OK;
   v->vmask = vm;
   v->vslot = (uint32_t)__builtin_ctzll(vm);
-  v->vrow = L.vrow;
-  v->vval = L.vval;
-  return virtual_rows(p->x_fm, p->n_rows, vm, L.vval, L.vrow, st);
+  v->vrow = Lc.vrow;
+  v->vval = Lc.vval;
+  return virtual_rows(p->x_fm, p->n_rows, vm, Lc.vval, Lc.vrow, st);
 }
 
 int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const void** src, cudaStream_t st) {
@@ -664,10 +685,11 @@ int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const voi
 }
 
 int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
-                const FitLayout& L, const ct_tree_buffers* trees, cudaStream_t st) {
+                const FitLayout& L0, const ct_tree_buffers* trees, cudaStream_t st) {
+  FitLayout L = L0;
   View v = fit_view(p, l, L);
   TreeView tv = tree_view(trees, 0);
-  CT_TRY(prepare_features(p, L, &v, st));
+  CT_TRY(prepare_features(p, &L, &v, st));
   CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
   CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
   current_prof()->begin(CT_K_BOOTSTRAP);
@@ -715,12 +737,13 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
 }
 
 int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
-              const ct_fit_options* o, const FitLayout& L, const ct_tree_buffers* trees,
+              const ct_fit_options* o, const FitLayout& L0, const ct_tree_buffers* trees,
               cudaStream_t st) {
+  FitLayout L = L0;
   View v = fit_view(p, l, L);
   const uint32_t C = p->n_classes;
   const uint32_t thr = o->bfs_threshold ? o->bfs_threshold : default_bfs_threshold(p);
-  CT_TRY(prepare_features(p, L, &v, st));
+  CT_TRY(prepare_features(p, &L, &v, st));
   struct Pending {
     ct_node nd;
     std::vector<uint32_t> tot;

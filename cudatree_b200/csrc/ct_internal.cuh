@@ -160,7 +160,8 @@ struct PartSeg {
   uint32_t n;
   uint32_t nl;            // number of left rows
   uint32_t status;        // first status slot (tiled segments)
-  uint64_t skip;          // features whose lists are left as they are (constant in the node)
+  uint64_t skip;          // features < 64 whose lists are left as they are (constant in the node)
+  const uint64_t* skip_hi;  // the node's mask words of features 64.. (n_features > 64), else NULL
 };
 struct PartTile {
   uint32_t seg;
@@ -346,9 +347,10 @@ struct LevelScratch {
   PartTile* tiles;        // [cap_status]
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
-  // The step's lists.  Constant-feature masks exist in a batched fit with
-  // n_features <= 64: bit f of node_mask[i] says that feature f is constant
-  // in node i of the step, so its lists are not partitioned and k_select
+  // The step's lists.  Constant-feature masks exist in a batched fit: node
+  // i of the step owns mask_words(n_features) words from node_mask +
+  // i * mask_words, and bit f % 64 of word f / 64 says that feature f is
+  // constant in the node, so its lists are not partitioned and k_select
   // does not read them; k_children writes the next list's masks.  Feature 0
   // is never in a mask (leaf labels and subtrees read its lists).
   StepLists* step;
@@ -359,6 +361,14 @@ struct LevelScratch {
   uint32_t cap_vpieces;
 };
 __device__ __forceinline__ bool masked(uint64_t m, uint32_t f) { return f < 64 && ((m >> f) & 1u); }
+// words of one node's constant-feature mask
+__host__ __device__ __forceinline__ uint32_t mask_words(uint32_t n_features) { return (n_features + 63) / 64; }
+// bit f of a node's multi-word mask (NULL: no feature masked)
+__device__ __forceinline__ bool mask_bit(const uint64_t* m, uint32_t f) { return m && ((m[f >> 6] >> (f & 63)) & 1u); }
+// feature f's lists are left as they are in segment sg
+__device__ __forceinline__ bool seg_skips(const PartSeg& sg, uint32_t f) {
+  return f < 64 ? ((sg.skip >> f) & 1u) : mask_bit(sg.skip_hi, f - 64);
+}
 
 // Per-kernel-group launch counts and CUDA-event timing of one fit.
 struct Prof {

@@ -170,7 +170,8 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
   const uint32_t lane = lane_id();
   const ct_node nd = lists.nodes[w];
   const uint32_t m = v.max_features;
-  const uint64_t cmask = lists.node_mask ? lists.node_mask[w] : 0ull;  // constant features (lists not current)
+  // constant features (lists not current)
+  const uint64_t* cmask = lists.node_mask ? lists.node_mask + (size_t)w * mask_words(v.n_features) : nullptr;
   uint32_t taken = 0;
   uint64_t vsel = 0;  // selected slots that hold virtual features (m <= 64 when there are any)
   if (nd.n >= 2) {
@@ -184,7 +185,7 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
         if (virt) {  // non-constant: some but not all rows take the high value
           const uint32_t nb = s.vcnt[(size_t)w * 64 + f];
           usable = nb > 0 && nb < nd.n;
-        } else if (!masked(cmask, f)) {
+        } else if (!mask_bit(cmask, f)) {
           const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
           const float* xf = v.x_fm + (size_t)f * v.n_rows;
           usable = xf[entry_row(v, lst[0])] != xf[entry_row(v, lst[nd.n - 1])];
@@ -737,12 +738,19 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   const bool big = nd.n > SMALL_SEG;
   const bool huge = big && nd.n >= HUGE_SEG && s.huge_segs && huge_partition_ok(v.bit_words);
   const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
-  const uint64_t skip = (lists.node_mask ? lists.node_mask[w] : 0ull) | virtual_skip(v);
+  const uint64_t* nmask = lists.node_mask ? lists.node_mask + (size_t)w * mask_words(v.n_features) : nullptr;
+  const uint64_t skip = (nmask ? nmask[0] : 0ull) | virtual_skip(v);
+  const uint64_t* skip_hi = nmask && v.n_features > 64 ? nmask + 1 : nullptr;
+  // features whose lists move
+  uint32_t nskip = (uint32_t)__popcll(skip);
+  if (skip_hi)
+    for (uint32_t k = 0; k + 1 < mask_words(v.n_features); ++k) nskip += (uint32_t)__popcll(skip_hi[k]);
+  const uint32_t nact = v.n_features - nskip;
   uint32_t sidx = 0, pbase = 0, tbase = 0, gidx = 0, ok = 1;
   if (lane == 0) {
     sidx = atomicAdd(&s.ctr->n_splits, 1u);
     atomicAdd(&s.ctr->split_total, (unsigned long long)nd.n);
-    atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * (v.n_features - (uint32_t)__popcll(skip)));
+    atomicAdd(&s.ctr->part_elems, (unsigned long long)nd.n * nact);
     pbase = atomicAdd(&s.ctr->n_part_pieces, npp);
     if (big) {
       gidx = atomicAdd(huge ? &s.ctr->n_huge_segs : &s.ctr->n_big_segs, 1u);
@@ -771,6 +779,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
       sg.nl = r.pos + 1;
       sg.status = tbase;
       sg.skip = skip;
+      sg.skip_hi = skip_hi;
       (huge ? s.huge_segs : big ? s.big_segs : s.small_segs)[gidx] = sg;
     }
   }
@@ -803,7 +812,6 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
     // segment's are padded to a multiple of four so that k_part_seg's quads
     // never span two segments
     const uint32_t F = v.n_features;
-    const uint32_t nact = F - (uint32_t)__popcll(skip);
     const uint32_t nlist = huge ? (nact + 3u) & ~3u : nact;
     uint32_t* count = huge ? &s.ctr->n_hchains : &s.ctr->n_bchains;
     uint2* list = huge ? s.hchains : s.bchains;
@@ -821,7 +829,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
     uint32_t done = 0;
     for (uint32_t f0 = 0; f0 < F; f0 += 32) {
       const uint32_t f = f0 + lane;
-      const bool act = f < F && !masked(skip, f);
+      const bool act = f < F && !(f < 64 ? masked(skip, f) : mask_bit(skip_hi, f - 64));
       const unsigned am = __ballot_sync(FULL, act);
       if (act) list[hb + done + __popc(am & lanemask_lt())] = make_uint2(gidx, f);
       done += __popc(am);
@@ -966,20 +974,26 @@ __device__ __forceinline__ void children_item(const View& v, const StepLists& li
     if (lists.next_mask) {
       // the child's constant features: the parent's, and those whose values
       // agree at the child's first and last positions (the child's lists of
-      // the others were just partitioned)
-      const uint64_t pm = lists.node_mask[sr.node];
-      uint64_t cm = pm;
-      for (uint32_t f0 = 0; f0 < v.n_features; f0 += 32) {
-        const uint32_t f = f0 + lane;
-        bool cst = false;
-        if (f > 0 && f < v.n_features && !masked(pm, f) && !is_virtual(v, f)) {
-          const IdxT* lst = list_ptr<IdxT>(v, ch.buf, ch.slot, f) + ch.start;
-          const float* xf = v.x_fm + (size_t)f * v.n_rows;
-          cst = xf[entry_row(v, lst[0])] == xf[entry_row(v, lst[ch.n - 1])];
+      // the others were just partitioned); one mask word per 64 features
+      const uint32_t mw = mask_words(v.n_features);
+      const uint64_t* pm = lists.node_mask + (size_t)sr.node * mw;
+      uint64_t* cmw = lists.next_mask + (size_t)idx * mw;
+      for (uint32_t k = 0; k < mw; ++k) {
+        const uint64_t pw = pm[k];
+        uint64_t cw = pw;
+#pragma unroll
+        for (uint32_t h = 0; h < 2; ++h) {
+          const uint32_t f = k * 64 + h * 32 + lane;
+          bool cst = false;
+          if (f > 0 && f < v.n_features && !((pw >> (f & 63)) & 1u) && !is_virtual(v, f)) {
+            const IdxT* lst = list_ptr<IdxT>(v, ch.buf, ch.slot, f) + ch.start;
+            const float* xf = v.x_fm + (size_t)f * v.n_rows;
+            cst = xf[entry_row(v, lst[0])] == xf[entry_row(v, lst[ch.n - 1])];
+          }
+          cw |= (uint64_t)__ballot_sync(FULL, cst) << (h * 32);
         }
-        cm |= (uint64_t)__ballot_sync(FULL, cst) << f0;
+        if (lane == 0) cmw[k] = cw;
       }
-      if (lane == 0) lists.next_mask[idx] = cm;
     }
   }
 }

@@ -71,7 +71,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
 #pragma unroll
       for (uint32_t r = 0; r < R; ++r) {
         const uint32_t f = f_lo + r * per + sub;
-        valid[r] = f < f_hi && p < n && !masked(sg.skip, f);
+        valid[r] = f < f_hi && p < n && !seg_skips(sg, f);
         rows[r] = valid[r] ? (uint32_t)__ldcs(in + (size_t)f * sg.in_fstride + p) : 0u;
       }
 #pragma unroll
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < FEAT_BLOCK; ++r) {
         const uint32_t f = f_lo + r;
         if (f >= f_hi) break;
-        if (masked(sg.skip, f)) continue;
+        if (seg_skips(sg, f)) continue;
         const bool valid = lane < n;
         const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
         const unsigned lm = __ballot_sync(FULL, left);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
     } else {
       const uint32_t rounds = ceil_div(n, 32);
       for (uint32_t f = f_lo; f < f_hi; ++f) {
-        if (masked(sg.skip, f)) continue;
+        if (seg_skips(sg, f)) continue;
         const IdxT* fin = in + (size_t)f * sg.in_fstride;
         IdxT* fout = out + (size_t)f * sg.out_fstride;
         uint32_t rows[PART_ROUNDS];

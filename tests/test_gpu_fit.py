@@ -338,3 +338,24 @@ def test_virtual_two_valued_features_match_oracle(cuda_device, n, seed, mode):
         f.fit(x, y)
         _assert_same_trees(f._trees, ref.trees)
     np.testing.assert_array_equal(f.predict(x[:3000]), O.predict(ref, x[:3000]))
+
+
+@pytest.mark.parametrize("f", [65, 130, 300])
+def test_constant_feature_masks_beyond_64_features_match_oracle(cuda_device, f):
+    """The batched fit keeps one constant-feature mask word per 64 features
+    for every node when at least one feature in eight is two-valued:
+    features that are constant from the start (some above index 64) and
+    few-valued features that turn constant deeper in the tree are skipped by
+    the partition and the selection, and the trees are the oracle's."""
+    rng = np.random.default_rng(f)
+    n = 2500
+    y = rng.integers(0, 4, size=n)
+    x = (rng.normal(size=(n, f)) + 0.8 * y[:, None] * (np.arange(f) % 5 == 0)).astype(np.float32)
+    x[:, 1::4] = rng.integers(0, 2, size=(n, len(range(1, f, 4))))  # two values: constant in many nodes
+    x[:, 3::8] = rng.integers(0, 3, size=(n, len(range(3, f, 8))))  # three values
+    for j in (2, 64, f - 1):
+        x[:, j] = 7.0
+    ref = O.fit_forest(x, y, n_estimators=3, max_features=9, seed=f)
+    forest = RandomForestClassifier(n_estimators=3, max_features=9, seed=f, fit_mode="batched").fit(x, y)
+    _assert_same_trees(forest._trees, ref.trees)
+    np.testing.assert_array_equal(forest.predict(x[:500]), O.predict(ref, x[:500]))
