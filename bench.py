@@ -436,7 +436,13 @@ def run_ours(args, world, rank, local):
     x, y = synthetic.covtype_like()
     seed = replica_seed(rank)
     n_trees = args.trees
-    forest = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
+    tune = not args.no_autotune
+    forest = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed, autotune=tune)
+    tune_s = None
+    if tune:  # the library's autotuner on the whole forest, before anything is timed
+        t0 = time.perf_counter()
+        forest.autotune(x, y, sample_trees=n_trees)
+        tune_s = time.perf_counter() - t0
     forest.fit_init(x, y)
     thr = forest.bfs_threshold
     stream = torch.cuda.current_stream()
@@ -489,7 +495,7 @@ def run_ours(args, world, rank, local):
     e2e_times = []
     f2 = forest
     for i in range(1 + args.e2e_steps if args.e2e_steps > 0 else 0):
-        f2 = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed)
+        f2 = RandomForestClassifier(n_trees, max_features=MAX_FEATURES, bootstrap=True, seed=seed, autotune=tune)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         f2.fit(xp, yp)
@@ -541,6 +547,8 @@ def run_ours(args, world, rank, local):
         "plain_fit_s": plain_s, "batched_speedup_vs_plain": (plain_s / step_s) if plain_s else None,
         "plain_trees_identical": same if plain_s else None,
         "nodes_per_forest": n_nodes, "level_steps": stats["steps"],
+        "fit_options": ({k: v for k, v in forest._tuned.items() if k != "sample_ms"} if forest._tuned else "defaults"),
+        "autotune_s": tune_s,
         "kernels": kernels,
         "roofline": {"bound": "hbm", "kernel": "k_partition", "achieved": round(p_gbs, 1) if p_gbs else None,
                      "peak": peak, "unit": "GB/s", "frac": round(p_gbs / peak, 4) if p_gbs else None,
@@ -572,6 +580,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2, help="0 skips the end-to-end measurement")
     ap.add_argument("--trees", type=int, default=N_TREES, help="trees per forest (profiling runs use fewer)")
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="fit with the default options (no autotuner)")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-serving", action="store_true")
     ap.add_argument("--predict-only", action="store_true", help="time plain predict only (profiling runs)")

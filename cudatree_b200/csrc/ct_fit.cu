@@ -214,6 +214,8 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   L->boot_ws = a.take<char>(L->boot_bytes);
   LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
   carve_level_scratch(a, v, caps, &L->s, L->virt);
+  L->s.huge_rows = o->huge_rows ? o->huge_rows : HUGE_SEG;
+  L->s.part_shape = o->part_shape;
   L->ctl = a.take<LoopCtl>(1);
   L->bytes = a.used + 256;
   return base != nullptr && a.ok();
@@ -835,13 +837,17 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
 }  // namespace
 
 // Autotuner candidates.  Every option here grows the same trees, so they are
-// chosen by timing: the scan piece length and the warp-subtree cutoff for the
-// batched form, the depth-first/breadth-first switch for the plain form (the
-// quantity the reference fits offline, estimate_threshold.py, and predicts
-// with random_forest.py:278-289).
-std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode) {
+// chosen by timing.  The batched form is tuned in two stages: the scan piece
+// length x the warp-subtree cutoff with the default partition, then the
+// partition shape of big segments (tile, ring buffers, CTAs per SM) x the
+// size from which a node partitions with its tree's mark bits in shared
+// memory, around the first stage's choice.  The plain form tunes the
+// depth-first/breadth-first switch (the quantity the reference fits offline,
+// estimate_threshold.py, and predicts with random_forest.py:278-289).
+std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode, int stage,
+                                            const ct_fit_options& base) {
   std::vector<ct_fit_options> c;
-  if (mode == CT_FIT_BATCHED) {
+  if (mode == CT_FIT_BATCHED && stage == 0) {
     for (uint32_t sp : {1024u, 2048u, 4096u})
       for (uint32_t cut : {0u, 32u, 128u}) {
         ct_fit_options o{};
@@ -850,7 +856,15 @@ std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode) 
         o.scan_piece = sp;
         c.push_back(o);
       }
-  } else {
+  } else if (mode == CT_FIT_BATCHED) {
+    for (uint32_t shape = 0; shape < CT_PART_SHAPES; ++shape)
+      for (uint32_t huge : {0u, 16384u, 0xffffffffu}) {
+        ct_fit_options o = base;
+        o.part_shape = shape;
+        o.huge_rows = huge;
+        c.push_back(o);
+      }
+  } else if (stage == 0) {
     std::vector<uint32_t> thr = {default_bfs_threshold(p), 2000u, 8000u, 32000u, std::max(2u, p->n_rows)};
     std::sort(thr.begin(), thr.end());
     thr.erase(std::unique(thr.begin(), thr.end()), thr.end());
@@ -869,9 +883,11 @@ size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_o
 int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
         const ct_fit_options* o, const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
 
+// The second stage changes no capacity, so the first stage's candidates bound the workspace.
 size_t autotune_workspace_bytes(const ct_problem* p, uint32_t n_trees, uint32_t mode) {
   size_t most = 0;
-  for (const ct_fit_options& o : tune_candidates(p, mode)) most = std::max(most, fit_workspace_bytes(p, n_trees, &o));
+  for (const ct_fit_options& o : tune_candidates(p, mode, 0, ct_fit_options{}))
+    most = std::max(most, fit_workspace_bytes(p, n_trees, &o));
   return most;
 }
 
@@ -884,22 +900,26 @@ int autotune(const ct_problem* p, const ct_lists* l, uint32_t n_trees, uint32_t 
   float top = 3.0e38f;
   int rc = CT_OK;
   bool any = false;
-  for (const ct_fit_options& o : tune_candidates(p, mode)) {
-    if (fit_workspace_bytes(p, n_trees, &o) > wsb) continue;
-    float t = 3.0e38f;
-    for (int rep = 0; rep < 2 && rc == CT_OK; ++rep) {
-      cudaEventRecord(e0, st);
-      rc = fit(p, l, 0, n_trees, &o, trees, ws, wsb, st);
-      cudaEventRecord(e1, st);
-      if (cudaEventSynchronize(e1) != cudaSuccess) rc = CT_ERR_CUDA;
-      float ms = 0.f;
-      if (rc == CT_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) t = std::min(t, ms);
-    }
-    if (rc != CT_OK) break;
-    if (t < top) {
-      top = t;
-      *best = o;
-      any = true;
+  for (int stage = 0; stage < 2 && rc == CT_OK; ++stage) {
+    if (stage == 1 && !any) break;
+    const ct_fit_options base = *best;
+    for (const ct_fit_options& o : tune_candidates(p, mode, stage, base)) {
+      if (fit_workspace_bytes(p, n_trees, &o) > wsb) continue;
+      float t = 3.0e38f;
+      for (int rep = 0; rep < 2 && rc == CT_OK; ++rep) {
+        cudaEventRecord(e0, st);
+        rc = fit(p, l, 0, n_trees, &o, trees, ws, wsb, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = CT_ERR_CUDA;
+        float ms = 0.f;
+        if (rc == CT_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) t = std::min(t, ms);
+      }
+      if (rc != CT_OK) break;
+      if (t < top) {
+        top = t;
+        *best = o;
+        any = true;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -927,6 +947,8 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
                    trees->n_nodes,
                "tree buffers are NULL");
   CT_ARG_CHECK(o && (o->mode == CT_FIT_PLAIN || o->mode == CT_FIT_BATCHED), "bad fit mode");
+  CT_ARG_CHECK(o->part_shape < CT_PART_SHAPES, "part_shape out of range");
+  CT_ARG_CHECK(o->huge_rows == 0 || o->huge_rows >= CT_HUGE_ROWS_MIN, "huge_rows must be 0 or >= 4096");
   CT_ARG_CHECK(n_trees >= 1, "n_trees must be >= 1");
   CT_ARG_CHECK(trees->capacity >= 2u * p->n_rows, "tree capacity must be >= 2 * n_rows");
   CT_ARG_CHECK(l->stride >= p->n_rows, "list stride must be >= n_rows");

@@ -185,6 +185,7 @@ struct PartWork {
   uint32_t cap_hchains;
   uint32_t* ticket_huge;
   uint32_t bit_words;     // mark-bit words of one tree
+  uint32_t shape;         // CT_PART_* of k_part_big
   PartTile* tiles;
   uint32_t* n_tiles;
   uint32_t cap_tiles;
@@ -354,6 +355,8 @@ struct LevelScratch {
   // does not read them; k_children writes the next list's masks.  Feature 0
   // is never in a mask (leaf labels and subtrees read its lists).
   StepLists* step;
+  uint32_t huge_rows;     // segments of at least this many rows take k_part_seg (>= HUGE_SEG)
+  uint32_t part_shape;    // CT_PART_* of k_part_big
   // Virtual features (View::vmask), else NULL / 0:
   uint32_t* vcnt;         // [cap_nodes][64] rows of each node with the feature's high value
   uint32_t* vcls;         // [cap_nodes][n_features][n_classes] those rows by class
@@ -435,7 +438,7 @@ constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
 constexpr uint32_t TILE_ELEMS = 4096;           // partition tile of big segments
 // Segments of at least HUGE_SEG rows are partitioned with the tree's mark
 // bits staged in shared memory (k_part_seg) when those bits fit the budget.
-constexpr uint32_t HUGE_SEG = 4096;
+constexpr uint32_t HUGE_SEG = CT_HUGE_ROWS_MIN;  // default and smallest ct_fit_options.huge_rows (capacities)
 constexpr uint32_t HUGE_BITS_MAX = 150u * 1024u;
 __host__ __device__ __forceinline__ bool huge_partition_ok(uint32_t bit_words) {
   return (uint64_t)bit_words * 4u <= HUGE_BITS_MAX;

@@ -736,7 +736,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   if (!split) return;
   const uint32_t npp = ceil_div(nd.n, PART_PIECE);
   const bool big = nd.n > SMALL_SEG;
-  const bool huge = big && nd.n >= HUGE_SEG && s.huge_segs && huge_partition_ok(v.bit_words);
+  const bool huge = big && nd.n >= s.huge_rows && s.huge_segs && huge_partition_ok(v.bit_words);
   const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
   const uint64_t* nmask = lists.node_mask ? lists.node_mask + (size_t)w * mask_words(v.n_features) : nullptr;
   const uint64_t skip = (nmask ? nmask[0] : 0ull) | virtual_skip(v);
@@ -1662,6 +1662,8 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.tiles = a.take<PartTile>(c.status);
   t.status = a.take<uint64_t>((size_t)c.status * v.n_features);
   t.step = a.take<StepLists>(1);
+  t.huge_rows = HUGE_SEG;
+  t.part_shape = 0;
   t.vcnt = virt ? a.take<uint32_t>((size_t)c.nodes * 64) : nullptr;
   t.vcls = virt ? a.take<uint32_t>((size_t)c.nodes * v.n_features * C) : nullptr;
   t.vpieces = virt ? a.take<uint2>(c.vpieces) : nullptr;
@@ -1784,6 +1786,7 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   w.cap_hchains = s.cap_hchains;
   w.ticket_huge = &s.ctr->ticket_huge;
   w.bit_words = v.bit_words;
+  w.shape = s.part_shape;
   w.tiles = s.tiles;
   w.n_tiles = &s.ctr->n_tiles;
   w.cap_tiles = s.cap_status;

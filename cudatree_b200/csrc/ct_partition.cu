@@ -476,13 +476,19 @@ int launch_big_v(const PartWork& w, uint64_t want, cudaStream_t st) {
   return CT_OK;
 }
 
-// Tiles of 2,048 elements (8 warps x 8 rounds of 32), two ring buffers, six
-// CTAs per SM (at most 40 registers): 16 KB of ring per CTA leaves most of
-// the SM's L1 to the mark bits the chains gather, which measured faster than
-// 4,096-element tiles with three or four buffers.
+// The shapes of CT_PART_*: tile (8 warps x ROUNDS rounds of 32), ring
+// buffers, CTAs per SM.  The default, 2,048-element tiles in two buffers at
+// six CTAs per SM (at most 40 registers), leaves most of the SM's L1 to the
+// mark bits the chains gather; the others trade tile length, copies in
+// flight and occupancy, for the autotuner to time.
 template <typename IdxT>
 int launch_big(const PartWork& w, uint64_t want, cudaStream_t st) {
-  return launch_big_v<IdxT, 8, 2, 6>(w, want, st);
+  switch (w.shape) {
+    case CT_PART_1024_R3_B8: return launch_big_v<IdxT, 4, 3, 8>(w, want, st);
+    case CT_PART_4096_R2_B4: return launch_big_v<IdxT, 16, 2, 4>(w, want, st);
+    case CT_PART_2048_R3_B4: return launch_big_v<IdxT, 8, 3, 4>(w, want, st);
+    default: return launch_big_v<IdxT, 8, 2, 6>(w, want, st);
+  }
 }
 
 }  // namespace

@@ -24,7 +24,7 @@ import time
 import numpy as np
 import torch
 
-from . import _lib, forest_format
+from . import _lib, forest_format, tune_cache
 from .forest_format import PACKED_DTYPE
 from .random_tree import RandomClassifierTree
 
@@ -101,7 +101,6 @@ def pack_trees(trees):
     return packed, offsets
 
 
-_TUNED = {}  # tuned fit options per (mode, rows, features, classes, max_features, ...)
 
 
 def compact_labels(y):
@@ -428,7 +427,7 @@ class RandomForestClassifier:
         if bfs_threshold is not None:
             self.bfs_threshold = int(bfs_threshold)
         if self.autotune_fit and self._tuned is None:
-            self._tuned = _TUNED.get(self._shape_key(self.fit_mode))
+            self._tuned = tune_cache.get(self._tune_key(self.fit_mode))
             if self._tuned is None:
                 self._run_autotune(self.fit_mode, min(8, self.n_estimators))
             if bfs_threshold is None and self.fit_mode == "plain":
@@ -454,11 +453,16 @@ class RandomForestClassifier:
             o.flags |= _lib.CT_FIT_NO_VIRTUAL
         o.step_nodes = int(self.step_nodes)
         o.graph_samples = int(self.graph_samples)
+        o.part_shape = int(t.get("part_shape", 0))
+        o.huge_rows = int(t.get("huge_rows", 0))
         return o
 
     def _shape_key(self, mode):
         return (mode, self.n_samples, self.n_features, self.n_labels, self._m, self.index_bytes,
                 bool(self.bootstrap), self.min_samples_split)
+
+    def _tune_key(self, mode):
+        return tune_cache.key(torch.cuda.get_device_name(_device()), self._shape_key(mode))
 
     def _run_autotune(self, mode, sample_trees):
         dev = _device()
@@ -483,15 +487,17 @@ class RandomForestClassifier:
                   wsb.value, C.byref(best), C.byref(ms), _stream())
         self._tuned = {"scan_piece": int(best.scan_piece), "subtree_cutoff": int(best.subtree_cutoff),
                        "bfs_threshold": int(best.bfs_threshold) or self.bfs_threshold,
+                       "part_shape": int(best.part_shape), "huge_rows": int(best.huge_rows),
                        "sample_trees": sample_trees, "sample_ms": float(ms.value)}
-        _TUNED[self._shape_key(mode)] = self._tuned
+        tune_cache.put(self._tune_key(mode), self._tuned)
         return self._tuned
 
     def autotune(self, samples, target, sample_trees=8):
         """Choose fit options for this data shape by timing candidate fits of
         sample_trees trees (the reference's offline threshold estimate,
         estimate_threshold.py, done on the device at hand); later fits of the
-        same shape with autotune=True reuse the choice.  Returns it."""
+        same shape with autotune=True reuse the choice, in this process and,
+        through tune_cache's file, in later ones.  Returns it."""
         self.fit_init(samples, target)
         try:
             return dict(self._run_autotune(self.fit_mode, max(1, min(int(sample_trees), self.n_estimators))))

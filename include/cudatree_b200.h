@@ -126,8 +126,22 @@ typedef struct ct_fit_options {
   uint32_t graph_samples;   /* batched: levels of at most this many samples run in
                                the loop graph, larger ones from the host (0 = 2^22,
                                0xffffffff = every level in the graph)               */
-  uint32_t reserved;
+  uint32_t part_shape;      /* partition of big segments: CT_PART_* (0 = default)   */
+  uint32_t huge_rows;       /* nodes of at least this many rows partition with the
+                               tree's mark bits in shared memory (0 = 4096, at
+                               least 4096; 0xffffffff = never)                      */
+  uint32_t reserved;        /* 0                                                    */
 } ct_fit_options;
+/* ct_fit_options.part_shape: tile of a big segment's chain x ring buffers x
+ * CTAs per SM of its partition.  Every shape partitions the same way. */
+enum {
+  CT_PART_2048_R2_B6 = 0, /* 2,048-element tiles, 2 buffers, 6 CTAs per SM (default) */
+  CT_PART_1024_R3_B8 = 1, /* 1,024-element tiles, 3 buffers, 8 CTAs per SM           */
+  CT_PART_4096_R2_B4 = 2, /* 4,096-element tiles, 2 buffers, 4 CTAs per SM           */
+  CT_PART_2048_R3_B4 = 3, /* 2,048-element tiles, 3 buffers, 4 CTAs per SM           */
+  CT_PART_SHAPES = 4
+};
+#define CT_HUGE_ROWS_MIN 4096u
 /* ct_fit_options.flags.  CT_FIT_PROFILE: CUDA events around each kernel
  * group (ct_fit_stats.ms); the batched form then runs its levels from the
  * host.  The batched form otherwise runs its levels of at most
@@ -243,8 +257,9 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
 /* Autotuner: fits n_trees sample trees (first tree 0) with each candidate
  * option set of the given mode and returns the fastest in *best (its time in
  * *best_ms).  Every candidate grows the same trees, so the choice changes
- * speed only.  Batched: scan piece length (1024, 2048, 4096) x warp-subtree
- * cutoff (0, 32, 128); plain: the
+ * speed only.  Batched, in two stages: scan piece length (1024, 2048, 4096)
+ * x warp-subtree cutoff (0, 32, 128); then, around that choice, the
+ * partition shape (CT_PART_*) x huge_rows (4096, 16384, never).  Plain: the
  * depth-first/breadth-first switch, which the reference sets with an offline
  * regression (estimate_threshold.py, random_forest.py:278-289).  The
  * workspace must hold ct_autotune_workspace_size bytes; lists and trees as

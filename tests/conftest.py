@@ -13,6 +13,15 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200) and the built library")
 
 
+@pytest.fixture(autouse=True, scope="session")
+def _tune_cache_in_tmp(tmp_path_factory):
+    """Autotuner choices made by the tests go to a file of the test session,
+    not to the user's cache."""
+    import os
+    os.environ["CUDATREE_B200_TUNE_CACHE"] = str(tmp_path_factory.mktemp("tune") / "autotune.json")
+    yield
+
+
 @pytest.fixture(scope="session")
 def cuda_device():
     import torch

@@ -204,3 +204,20 @@ def test_malformed_forests_are_rejected_before_any_walk(case):
     else:
         assert st == 1, case
         assert "malformed forest" in _lib.last_error()
+
+
+def test_fit_rejects_bad_partition_options_before_any_launch():
+    """part_shape beyond CT_PART_SHAPES and huge_rows below 4,096 are refused
+    with CT_ERR_ARG before the fit touches the device (the pointers here are
+    never dereferenced)."""
+    lib = _lib.load()
+    fake = 256
+    prob = _lib.Problem(fake, fake, fake, 1000, 8, 3, 4, 1, 3, 1, 1, 0)
+    lists = _lib.Lists(fake, fake, fake, 1000, 4)
+    trees = _lib.TreeBuffers(fake, fake, fake, fake, fake, fake, 2000)
+    for shape, huge, text in ((4, 0, "part_shape"), (0, 100, "huge_rows")):
+        opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, 0, 0)
+        opts.part_shape, opts.huge_rows = shape, huge
+        st = lib.ct_fit(C.byref(prob), C.byref(lists), 0, 4, C.byref(opts), C.byref(trees), C.c_void_p(fake), 0,
+                        None)
+        assert st == 1 and text in _lib.last_error()
