@@ -256,9 +256,9 @@ def run_configs(args):
         "sklearn_fit_s": sk, "sklearn_cores": cores}
     n_jobs = args.queue_jobs
     jobs = [synthetic.blob_job(j) for j in range(n_jobs)]
-    fit_forests(jobs[:4], n_estimators=10, seeds=range(4), workers=4)  # warm-up
+    fit_forests(jobs[:4], n_estimators=10, seeds=range(4))  # warm-up
     t0 = time.perf_counter()
-    forests = fit_forests(jobs, n_estimators=10, seeds=range(n_jobs), workers=args.queue_workers)
+    forests = fit_forests(jobs, n_estimators=10, seeds=range(n_jobs))
     q_s = time.perf_counter() - t0
     checked = list(range(0, n_jobs, max(1, n_jobs // 8)))
     same = True
@@ -271,7 +271,9 @@ def run_configs(args):
     sk = sum(_sk_fit_s(jobs[j][0], jobs[j][1], 10, int(np.ceil(np.sqrt(jobs[j][0].shape[1]))), True, cores)[0]
              for j in range(sample))
     out[f"queue_{n_jobs}_jobs_10trees"] = {
-        "total_s": q_s, "jobs_per_s": n_jobs / q_s, "workers": args.queue_workers,
+        "total_s": q_s, "jobs_per_s": n_jobs / q_s,
+        "form": "ct_fit_queue: jobs grouped by index/label width, each group one shared level loop",
+        "level_launches": forests[0].last_fit_stats["total_launches"] if forests[0].last_fit_stats else None,
         "trees_identical_to_solo_fits": bool(same), "checked_jobs": len(checked),
         "sklearn_sample_s": sk, "sklearn_sample": f"jobs 0-{sample - 1} one after another",
         "sklearn_sequential_s_estimate": sk * n_jobs / sample, "sklearn_cores": cores}
@@ -592,7 +594,6 @@ def main():
     ap.add_argument("--skip-configs", action="store_true", help="skip the digits, wide and queue configurations")
     ap.add_argument("--configs-only", action="store_true", help="run only the digits, wide and queue configurations")
     ap.add_argument("--queue-jobs", type=int, default=256)
-    ap.add_argument("--queue-workers", type=int, default=8)
     args = ap.parse_args()
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))

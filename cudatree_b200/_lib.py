@@ -73,6 +73,11 @@ class FitOptions(C.Structure):
                 ("reserved", C.c_uint32)]
 
 
+class FitJob(C.Structure):
+    """ct_fit_job: one forest of a queue fit (ct_fit_queue)."""
+    _fields_ = [("problem", Problem), ("lists", Lists), ("n_trees", C.c_uint32), ("first_tree", C.c_uint32)]
+
+
 class PackedNode(C.Structure):
     _fields_ = [("threshold", C.c_float), ("feature", C.c_uint32), ("left", C.c_uint32),
                 ("value", C.c_uint32)]
@@ -123,6 +128,10 @@ PROTOTYPES = {
                                         C.POINTER(C.c_size_t)]),
     "ct_fit": (C.c_int, [C.POINTER(Problem), C.POINTER(Lists), C.c_uint32, C.c_uint32,
                          C.POINTER(FitOptions), C.POINTER(TreeBuffers), P, C.c_size_t, P]),
+    "ct_fit_queue_workspace_size": (C.c_int, [C.POINTER(FitJob), C.c_uint32, C.POINTER(FitOptions),
+                                              C.POINTER(C.c_size_t)]),
+    "ct_fit_queue": (C.c_int, [C.POINTER(FitJob), C.c_uint32, C.POINTER(FitOptions), C.POINTER(TreeBuffers), P,
+                               C.c_size_t, P]),
     "ct_fit_stats": (C.c_int, [C.c_void_p]),
     "ct_tree_canonicalize": (C.c_int, [P, P, P, P, P, C.c_uint32, P, P, P, P, P]),
     "ct_predict": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P, P]),

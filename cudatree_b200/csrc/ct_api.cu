@@ -17,6 +17,9 @@ size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_
 int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree,
                       uint32_t* n_in_dev, void* ws, size_t wsb, cudaStream_t st);
 size_t fit_workspace_bytes(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o);
+size_t fit_queue_workspace_bytes(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o);
+int fit_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o, const ct_tree_buffers* trees,
+              void* ws, size_t wsb, cudaStream_t st);
 int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_trees,
         const ct_fit_options* o, const ct_tree_buffers* trees, void* ws, size_t wsb, cudaStream_t st);
 int canonicalize(const uint32_t* left, const uint32_t* right, const uint32_t* feature, const float* threshold,
@@ -215,6 +218,17 @@ int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint
            void* stream) {
   CT_GUARD(return fit(p, lists, first_tree, n_trees, opt, trees, workspace, workspace_bytes,
                       (cudaStream_t)stream);)
+}
+
+int ct_fit_queue_workspace_size(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* opt,
+                                size_t* bytes) {
+  CT_ARG_CHECK(jobs && n_jobs >= 1 && opt && bytes, "NULL argument");
+  CT_GUARD(*bytes = fit_queue_workspace_bytes(jobs, n_jobs, opt); return CT_OK;)
+}
+
+int ct_fit_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* opt, const ct_tree_buffers* trees,
+                 void* workspace, size_t workspace_bytes, void* stream) {
+  CT_GUARD(return fit_queue(jobs, n_jobs, opt, trees, workspace, workspace_bytes, (cudaStream_t)stream);)
 }
 
 int ct_fit_stats(ct_kernel_stats* out) {

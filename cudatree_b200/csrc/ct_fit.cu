@@ -107,7 +107,7 @@ __global__ void k_root(View v, const uint32_t* n_in, uint32_t slot_lo, uint64_t 
       if (xf[entry_row(v, lf[0])] == xf[entry_row(v, lf[n - 1])]) atomicOr(&s_mask[f >> 6], 1ull << (f & 63));
     }
     __syncthreads();
-    for (uint32_t k = threadIdx.x; k < mw; k += blockDim.x) out_mask[(size_t)s_idx * mw + k] = s_mask[k];
+    for (uint32_t k = threadIdx.x; k < mw; k += blockDim.x) out_mask[(size_t)s_idx * v.mask_stride + k] = s_mask[k];
   }
 }
 
@@ -641,14 +641,13 @@ View fit_view(const ct_problem* p, const ct_lists* l, const FitLayout& L) {
   return v;
 }
 
-// Per-feature preparation of a fit call: the two-valued features and, when
-// the fit can have virtual features, which ones are (every two-valued
-// feature but feature 0, whose lists give the leaf labels) and their rows'
-// value bits.  One host read of the flags.
-// Feature flags, virtual features, and whether a batched fit of more than 64
-// features keeps constant-feature masks: with few-valued features, lists go
-// constant in big nodes and the masks save their partition; with continuous
-// features they rarely do, and k_children would only pay for the checks.
+// Per-feature preparation of a fit call: the two-valued features; when the
+// fit can have virtual features, which ones are (every two-valued feature
+// but feature 0, whose lists give the leaf labels) and their rows' value
+// bits; and whether a batched fit of more than 64 features keeps
+// constant-feature masks.  With few-valued features, lists go constant in
+// big nodes and the masks save their partition; with continuous features
+// they rarely do, and k_children would only pay for the checks.
 // Two-valued features stand for the few-valued ones: masks are kept when at
 // least one feature in eight is two-valued.
 int prepare_features(const ct_problem* p, FitLayout* L, View* v, cudaStream_t st) {
@@ -1116,6 +1115,242 @@ int fetch_trees(const ct_tree_buffers* tb, uint32_t n_trees, const uint32_t* cou
       return status[w];
     }
   return CT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Forest queue: the batched fit of several independent jobs (each its own
+// samples, labels, presort, index lists, F, C, m and seed) through shared
+// level steps.  Each job is prepared on its own (feature flags, packed
+// presort, bootstrap, roots); from then on one node list holds every job's
+// nodes and every level kernel serves all of them, each work item reading
+// its job's view (View::jobs).  The tree slots are numbered across the jobs
+// in order; a job's trees are the ones its solo fit grows (the same seed,
+// tree keys and canonical rule).  The reference runs such a queue as one
+// process per job over its GPU (hybridforest/builder.py:79-141).
+namespace {
+
+struct QueueShape {
+  uint32_t slots = 0;      // trees of all jobs
+  uint64_t samples = 0;    // sum over trees of their job's rows
+  uint32_t n_max = 0, f_max = 0, c_max = 0, m_max = 0;
+  uint32_t fbin_words = 0; // sum over jobs of their flag words
+  size_t ff_bytes = 0, boot_bytes = 0;
+};
+
+QueueShape queue_shape(const ct_fit_job* jobs, uint32_t n_jobs) {
+  QueueShape q;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const ct_problem& p = jobs[j].problem;
+    q.slots += jobs[j].n_trees;
+    q.samples += (uint64_t)jobs[j].n_trees * p.n_rows;
+    q.n_max = std::max(q.n_max, p.n_rows);
+    q.f_max = std::max(q.f_max, p.n_features);
+    q.c_max = std::max(q.c_max, p.n_classes);
+    q.m_max = std::max(q.m_max, p.max_features);
+    q.fbin_words += (p.n_features + 31) / 32;
+    q.ff_bytes = std::max(q.ff_bytes, feature_flags_work_bytes(p.n_features));
+    q.boot_bytes = std::max(q.boot_bytes, bootstrap_scratch_bytes(p.n_rows, p.n_features, jobs[j].n_trees));
+  }
+  return q;
+}
+
+// The batch's problem: the first job's widths, the largest F, C and m of any
+// job (the scratch strides), and the largest row count.
+ct_problem batch_problem(const ct_fit_job* jobs, const QueueShape& q) {
+  ct_problem pb = jobs[0].problem;
+  pb.n_rows = q.n_max;
+  pb.n_features = q.f_max;
+  pb.n_classes = q.c_max;
+  pb.max_features = q.m_max;
+  return pb;
+}
+
+bool layout_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o, char* base, size_t size,
+                  FitLayout* L, View** views_dev, uint32_t** slot_job_dev) {
+  const QueueShape q = queue_shape(jobs, n_jobs);
+  const ct_problem pb = batch_problem(jobs, q);
+  View v = make_view(&pb, nullptr);
+  L->n_slots = q.slots;
+  L->cap_list = (uint32_t)std::min<uint64_t>(q.samples / 2 + q.slots + 2, 0xffffffffull);
+  L->chunk = std::min<uint32_t>(L->cap_list, o->step_nodes ? o->step_nodes : CHUNK_NODES_MAX);
+  L->scan_piece = o->scan_piece ? o->scan_piece : DEFAULT_SCAN_PIECE;
+  L->subtree_cut = q.n_max < (1u << 27) ? std::min<uint32_t>(o->subtree_cutoff, 128u) : 0u;
+  L->cap_small = L->subtree_cut ? 2 * L->chunk : 0u;
+  L->host_loop = (o->flags & CT_FIT_HOST_LOOP) != 0;
+  L->graph_samples = o->graph_samples == 0xffffffffu ? UINT64_MAX
+                     : o->graph_samples               ? o->graph_samples
+                                                      : DEFAULT_GRAPH_SAMPLES;
+  Arena a{base, size, 0};
+  L->small = L->cap_small ? a.take<ct_node>(L->cap_small) : nullptr;
+  L->small_bound = 0;
+  L->n_in = a.take<uint32_t>(q.slots);
+  L->fbin = a.take<uint32_t>(q.fbin_words);
+  L->ffwork = a.take<char>(q.ff_bytes);
+  L->virt = false;
+  L->vrow = nullptr;
+  L->vval = nullptr;
+  // constant-feature masks while every job has at most 64 features
+  const bool masks = q.f_max <= 64;
+  L->mask_words = mask_words(q.f_max);
+  for (int i = 0; i < 2; ++i) {
+    L->list[i] = a.take<ct_node>(L->cap_list);
+    L->tot[i] = a.take<uint32_t>((size_t)L->cap_list * q.c_max);
+    L->mask[i] = masks ? a.take<uint64_t>((size_t)L->cap_list * L->mask_words) : nullptr;
+  }
+  L->boot_bytes = q.boot_bytes;
+  L->boot_ws = a.take<char>(L->boot_bytes);
+  LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, q.samples});
+  carve_level_scratch(a, v, caps, &L->s, false);
+  // jobs of different row counts have mark bits of different sizes: no shared-memory staging
+  L->s.huge_segs = nullptr;
+  L->s.cap_huge = 0;
+  L->s.huge_rows = 0xffffffffu;
+  L->s.part_shape = o->part_shape;
+  L->ctl = a.take<LoopCtl>(1);
+  *views_dev = a.take<View>(n_jobs);
+  *slot_job_dev = a.take<uint32_t>(q.slots);
+  L->bytes = a.used + 256;
+  return base != nullptr && a.ok();
+}
+
+}  // namespace
+
+size_t fit_queue_workspace_bytes(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o) {
+  FitLayout L;
+  View* vd = nullptr;
+  uint32_t* sj = nullptr;
+  layout_queue(jobs, n_jobs, o, nullptr, 0, &L, &vd, &sj);
+  return L.bytes;
+}
+
+int check_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o, const ct_tree_buffers* trees) {
+  CT_ARG_CHECK(jobs && n_jobs >= 1, "no jobs");
+  CT_ARG_CHECK(o && o->mode == CT_FIT_BATCHED, "a forest queue takes the batched form");
+  CT_ARG_CHECK(o->part_shape < CT_PART_SHAPES, "part_shape out of range");
+  CT_ARG_CHECK(trees && trees->left && trees->right && trees->feature && trees->threshold && trees->value &&
+                   trees->n_nodes,
+               "tree buffers are NULL");
+  uint64_t slots = 0;
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    const ct_fit_job& jb = jobs[j];
+    CT_TRY(check_problem(&jb.problem));
+    CT_ARG_CHECK(jb.problem.index_bytes == jobs[0].problem.index_bytes &&
+                     jb.problem.label_bytes == jobs[0].problem.label_bytes,
+                 "the jobs of one queue fit share index_bytes and label_bytes");
+    CT_ARG_CHECK(jb.n_trees >= 1, "a job has no trees");
+    CT_ARG_CHECK(jb.lists.si0 && jb.lists.si1 && jb.lists.mark, "a job's lists are NULL");
+    CT_ARG_CHECK(jb.lists.stride >= jb.problem.n_rows, "a job's list stride is below its n_rows");
+    CT_ARG_CHECK(jb.lists.n_slots >= jb.n_trees, "a job's lists hold too few tree slots");
+    CT_ARG_CHECK(trees->capacity >= 2u * jb.problem.n_rows, "tree capacity must be >= 2 * every job's n_rows");
+    slots += jb.n_trees;
+  }
+  CT_ARG_CHECK(slots < (1ull << 31), "too many trees in one queue fit");
+  return CT_OK;
+}
+
+int fit_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o, const ct_tree_buffers* trees,
+              void* ws, size_t wsb, cudaStream_t st) {
+  CT_TRY(check_queue(jobs, n_jobs, o, trees));
+  FitLayout L;
+  View* views_dev = nullptr;
+  uint32_t* slot_job_dev = nullptr;
+  if (!layout_queue(jobs, n_jobs, o, reinterpret_cast<char*>(ws), wsb, &L, &views_dev, &slot_job_dev)) {
+    set_last_error("queue fit workspace too small");
+    return CT_ERR_OOM;
+  }
+  const QueueShape q = queue_shape(jobs, n_jobs);
+  const ct_problem pb = batch_problem(jobs, q);
+  Prof* pf = current_prof();
+  pf->finish();
+  pf->stats = ct_kernel_stats{};
+  pf->timing = (o->flags & CT_FIT_PROFILE) != 0;
+  pf->st = st;
+  auto run = [&]() -> int {
+    // the jobs' views, with the batch's strides
+    std::vector<View> views(n_jobs);
+    std::vector<uint32_t> slot_job(q.slots);
+    std::vector<uint32_t> first_slot(n_jobs);
+    uint32_t slot = 0, fw = 0;
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+      const ct_fit_job& jb = jobs[j];
+      View vj = fit_view(&jb.problem, &jb.lists, L);
+      vj.fbin = L.fbin + fw;
+      vj.n_classes = q.c_max;
+      vj.slot_base = slot;
+      vj.sel_stride = q.m_max;
+      vj.mask_stride = L.mask_words;
+      views[j] = vj;
+      first_slot[j] = slot;
+      for (uint32_t t = 0; t < jb.n_trees; ++t) slot_job[slot + t] = j;
+      CT_TRY(feature_flags(jb.problem.x_fm, jb.problem.n_rows, jb.problem.n_features, L.fbin + fw, nullptr,
+                           L.ffwork, st));
+      slot += jb.n_trees;
+      fw += (jb.problem.n_features + 31) / 32;
+    }
+    CT_CUDA_TRY(cudaMemcpyAsync(views_dev, views.data(), n_jobs * sizeof(View), cudaMemcpyHostToDevice, st));
+    CT_CUDA_TRY(cudaMemcpyAsync(slot_job_dev, slot_job.data(), q.slots * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                st));
+    // the batch view carries the strides; lists and marks are read through
+    // the jobs' views (its own point at the first job's, never dereferenced)
+    View vb = make_view(&pb, &jobs[0].lists);
+    vb.jobs = views_dev;
+    vb.slot_job = slot_job_dev;
+    vb.sel_stride = q.m_max;
+    vb.mask_stride = L.mask_words;
+    vb.bit_words = 0;  // per job (the shared-memory staging of marks is off)
+    vb.lab_shift = views[0].lab_shift;
+    vb.row_mask = views[0].row_mask;
+    TreeView tv = tree_view(trees, 0);
+    CT_CUDA_TRY(cudaMemsetAsync(L.s.ctr, 0, sizeof(Counters), st));
+    CT_CUDA_TRY(cudaMemsetAsync(L.boot_ws, 0, 16, st));
+    current_prof()->begin(CT_K_BOOTSTRAP);
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+      const ct_fit_job& jb = jobs[j];
+      const void* src = nullptr;
+      CT_TRY(seed_source(&jb.problem, &jb.lists, views[j], &src, st));
+      CT_TRY(bootstrap_many(&jb.problem, &jb.lists, 0, jb.n_trees, jb.first_tree, src, views[j].row_mask,
+                            L.n_in + first_slot[j], L.boot_ws, L.boot_bytes, st));
+      for (uint32_t t = 0; t < jb.n_trees; ++t) account_bootstrap(&jb.problem);
+    }
+    current_prof()->end();
+    CT_TRY(check_boot_error(L, st));
+    begin_level(L.s.ctr, st);
+    for (uint32_t j = 0; j < n_jobs; ++j)
+      CT_TRY(root(&jobs[j].problem, views[j], L, first_slot[j], jobs[j].n_trees, jobs[j].first_tree, tv, 0, st));
+    Counters h;
+    if (!current_prof()->timing && !L.host_loop) {
+      uint32_t n = 0;
+      uint64_t total = 0;
+      if (L.graph_samples != UINT64_MAX) {
+        CT_TRY(read_counters(L, &h, st));
+        n = h.n_next;
+        total = h.next_total;
+      }
+      int cur = 0;
+      while (n > 0 && total > L.graph_samples) {
+        begin_level(L.s.ctr, st);
+        CT_TRY(step(&pb, vb, L, tv, cur, n, total, st));
+        CT_TRY(read_counters(L, &h, st));
+        account_level(&pb, vb, h);
+        if (L.subtree_cut) L.small_bound = h.n_small;
+        n = h.n_next;
+        total = h.next_total;
+        cur = 1 - cur;
+      }
+      return graph_level_loop(&pb, vb, L, tv, cur, st);
+    }
+    CT_TRY(read_counters(L, &h, st));
+    CT_TRY(level_loop(&pb, vb, L, tv, 0, h.n_next, h.next_total, st));
+    if (L.small_bound) {
+      CT_TRY(flush_subtrees(&pb, vb, L, tv, st));
+      CT_TRY(read_counters(L, &h, st));
+    }
+    return CT_OK;
+  };
+  const int rc = run();
+  pf->finish();
+  pf->timing = false;
+  return rc;
 }
 
 }  // namespace ct

@@ -162,6 +162,8 @@ struct PartSeg {
   uint32_t status;        // first status slot (tiled segments)
   uint64_t skip;          // features < 64 whose lists are left as they are (constant in the node)
   const uint64_t* skip_hi;  // the node's mask words of features 64.. (n_features > 64), else NULL
+  uint32_t n_features;    // of the segment's job
+  uint32_t row_mask;      // list entry -> row id of its mark bit (the job's View::row_mask)
 };
 struct PartTile {
   uint32_t seg;
@@ -193,8 +195,7 @@ struct PartWork {
   uint32_t cap_status;
   uint32_t* ticket;
   uint32_t* error;
-  uint32_t n_features;
-  uint32_t row_mask;      // list entry -> row id of its mark bit (see View::row_mask)
+  uint32_t n_features;    // the most of any segment's job (k_part_small's feature blocks)
 };
 
 // View of the problem + lists passed by value to kernels.
@@ -237,7 +238,29 @@ struct View {
   const uint64_t* vrow;
   const float2* vval;
   uint32_t vslot;
+  // A queue fit of several jobs (ct_fit_queue) passes the level kernels a
+  // batch view whose jobs table holds one view per job; a work item reads
+  // the view of its node's job (job_view).  Tree slots are numbered across
+  // the jobs, and a job's lists and mark bits are indexed by slot -
+  // slot_base.  The scratch strides are the batch's: sel_stride selected
+  // feature slots and mask_stride constant-mask words per node (a job's
+  // max_features and n_features are its own).  One job: jobs NULL,
+  // slot_base 0, sel_stride = max_features, mask_stride =
+  // mask_words(n_features).
+  const View* jobs;
+  const uint32_t* slot_job;
+  uint32_t slot_base;
+  uint32_t sel_stride;
+  uint32_t mask_stride;
 };
+// `const View& V`: the view of the job that owns tree slot SLOT.  In a
+// kernel instantiated for a queue (template flag Q) it is that job's entry
+// of the batch view VB's table; otherwise V is VB itself, so a fit of one
+// job compiles as if the lookup were not there.
+#define CT_JOB_VIEW(V, VB, SLOT)                              \
+  View V##_job;                                               \
+  if constexpr (Q) V##_job = (VB).jobs[(VB).slot_job[SLOT]];  \
+  const View& V = Q ? V##_job : (VB)
 __device__ __forceinline__ bool two_valued(const View& v, uint32_t f) {
   return v.fbin && ((__ldg(v.fbin + (f >> 5)) >> (f & 31)) & 1u);
 }
@@ -285,7 +308,11 @@ __device__ __forceinline__ float ld_keep(const float* p, uint64_t pol) {
 template <typename IdxT>
 __device__ __forceinline__ IdxT* list_ptr(const View& v, uint32_t buf, uint32_t slot, uint32_t f) {
   IdxT* base = reinterpret_cast<IdxT*>(buf ? v.si1 : v.si0);
-  return base + ((size_t)slot * v.n_features + f) * v.stride;
+  return base + ((size_t)(slot - v.slot_base) * v.n_features + f) * v.stride;
+}
+// mark bits of the tree in slot `slot`
+__device__ __forceinline__ uint32_t* slot_bits(const View& v, uint32_t slot) {
+  return v.bits + (size_t)(slot - v.slot_base) * v.bit_words;
 }
 __device__ __forceinline__ uint32_t entry_row(const View& v, uint32_t e) { return e & v.row_mask; }
 template <typename LabT>
@@ -349,8 +376,8 @@ struct LevelScratch {
   uint64_t* status;       // [n_features][cap_status]
   Counters* ctr;
   // The step's lists.  Constant-feature masks exist in a batched fit: node
-  // i of the step owns mask_words(n_features) words from node_mask +
-  // i * mask_words, and bit f % 64 of word f / 64 says that feature f is
+  // i of the step owns View::mask_stride words from node_mask +
+  // i * mask_stride, and bit f % 64 of word f / 64 says that feature f is
   // constant in the node, so its lists are not partitioned and k_select
   // does not read them; k_children writes the next list's masks.  Feature 0
   // is never in a mask (leaf labels and subtrees read its lists).

@@ -164,14 +164,15 @@ __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_vcount(View v, LevelScrat
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT>
-__device__ __forceinline__ void select_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, bool Q>
+__device__ __forceinline__ void select_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                             uint32_t scan_piece, uint32_t w) {
   const uint32_t lane = lane_id();
   const ct_node nd = lists.nodes[w];
+  CT_JOB_VIEW(v, vb, nd.slot);
   const uint32_t m = v.max_features;
   // constant features (lists not current)
-  const uint64_t* cmask = lists.node_mask ? lists.node_mask + (size_t)w * mask_words(v.n_features) : nullptr;
+  const uint64_t* cmask = lists.node_mask ? lists.node_mask + (size_t)w * v.mask_stride : nullptr;
   uint32_t taken = 0;
   uint64_t vsel = 0;  // selected slots that hold virtual features (m <= 64 when there are any)
   if (nd.n >= 2) {
@@ -194,7 +195,7 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
       const unsigned mask = __ballot_sync(FULL, usable);
       const uint32_t rank = __popc(mask & lanemask_lt());
       const bool keep = usable && taken + rank < m;
-      if (keep) s.sel[(size_t)w * m + taken + rank] = f;
+      if (keep) s.sel[(size_t)w * v.sel_stride + taken + rank] = f;
       const uint64_t vb = (keep && virt) ? 1ull << (taken + rank) : 0ull;
       vsel |= ((uint64_t)__reduce_or_sync(FULL, (uint32_t)(vb >> 32)) << 32) | __reduce_or_sync(FULL, (uint32_t)vb);
       taken += min((uint32_t)__popc(mask), m - taken);
@@ -241,23 +242,24 @@ __device__ __forceinline__ void select_item(const View& v, const StepLists& list
   }
 }
 
-template <typename IdxT>
+template <typename IdxT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_select(View v, LevelScratch s, uint32_t scan_piece) {
   const uint32_t count = min(s.ctr->n_nodes, s.cap_nodes);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_SELECT], [&](uint32_t w) { select_item<IdxT>(v, sl, s, scan_piece, w); });
+  for_items(count, &s.ctr->claim[ITEM_SELECT], [&](uint32_t w) { select_item<IdxT, Q>(v, sl, s, scan_piece, w); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void scan_hist_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void scan_hist_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                                uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
-  const uint32_t C = v.n_classes;
+  const uint32_t C = vb.n_classes;
   const uint32_t lane = lane_id();
   const ScanPiece pc = s.pieces[pi];
   if (pc.npieces <= 1 || pc.j + 1 == pc.npieces) return;
   const ct_node nd = lists.nodes[pc.node];
-  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
+  CT_JOB_VIEW(v, vb, nd.slot);
+  const uint32_t f = s.sel[(size_t)pc.node * v.sel_stride + pc.slot];
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const uint32_t lo = pc.j * scan_piece;
   const uint32_t hi = min(lo + scan_piece, nd.n);
@@ -306,14 +308,14 @@ __device__ __forceinline__ void scan_hist_item(const View& v, const StepLists& l
   for (uint32_t c = lane; c < C; c += 32) out[c] = cnt[c];
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_hist(View v, LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_HIST],
-            [&](uint32_t pi) { scan_hist_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t pi) { scan_hist_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
 }
 
 __device__ __forceinline__ void scan_carry_item(const LevelScratch& s, uint32_t C, uint32_t pi) {
@@ -349,16 +351,17 @@ __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_carry(LevelScratch s
 // a 32-way search over x and scores it with the scan's exact arithmetic; the
 // other pieces report no candidate.  Same result as the general scan, with
 // a few gathers per piece instead of one per position.
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void two_valued_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void two_valued_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                                 uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
-  const uint32_t C = v.n_classes;
+  const uint32_t C = vb.n_classes;
   const uint32_t* tot = lists.tot;
   const uint32_t lane = lane_id();
   const ScanPiece pc = s.pieces[pi];
-  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
-  if (!two_valued(v, f)) return;  // k_split_scan's piece
   const ct_node nd = lists.nodes[pc.node];
+  CT_JOB_VIEW(v, vb, nd.slot);
+  const uint32_t f = s.sel[(size_t)pc.node * v.sel_stride + pc.slot];
+  if (!two_valued(v, f)) return;  // k_split_scan's piece
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const float* xf = v.x_fm + (size_t)f * v.n_rows;
   const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
@@ -434,28 +437,29 @@ __device__ __forceinline__ void two_valued_item(const View& v, const StepLists& 
   if (lane == 0) *out = pb;
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_two_valued(View v, LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_TWO_VALUED],
-            [&](uint32_t pi) { two_valued_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t pi) { two_valued_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void split_scan_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void split_scan_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                                 uint32_t scan_piece, uint32_t* cnt, uint32_t pi) {
-  const uint32_t C = v.n_classes;
+  const uint32_t C = vb.n_classes;
   const uint32_t* tot = lists.tot;
   uint32_t* T = cnt + C;
   const uint32_t lane = lane_id();
   const ScanPiece pc = s.pieces[pi];
-  const uint32_t f = s.sel[(size_t)pc.node * v.max_features + pc.slot];
-  if (two_valued(v, f)) return;  // k_scan_two_valued's piece
   const ct_node nd = lists.nodes[pc.node];
+  CT_JOB_VIEW(v, vb, nd.slot);
+  const uint32_t f = s.sel[(size_t)pc.node * v.sel_stride + pc.slot];
+  if (two_valued(v, f)) return;  // k_scan_two_valued's piece
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, f) + nd.start;
   const float* xf = v.x_fm + (size_t)f * v.n_rows;
   const uint32_t* carry = pc.npieces > 1 ? s.carry + (size_t)pc.carry * C : nullptr;
@@ -590,7 +594,7 @@ __device__ __forceinline__ void split_scan_item(const View& v, const StepLists& 
   }
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
 k_split_scan(View v, LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
@@ -598,17 +602,18 @@ k_split_scan(View v, LevelScratch s, uint32_t scan_piece) {
   const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_SCAN],
-            [&](uint32_t pi) { split_scan_item<IdxT, LabT>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t pi) { split_scan_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT>
-__device__ __forceinline__ void split_reduce_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, bool Q>
+__device__ __forceinline__ void split_reduce_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                                   uint32_t w) {
   const uint32_t lane = lane_id();
   const uint32_t base = s.piece_base[w];
   const uint32_t cnt = s.piece_cnt[w];
-  const uint32_t m = v.max_features;
+  CT_JOB_VIEW(v, vb, Q ? lists.nodes[w].slot : 0u);
+  const uint32_t m = v.sel_stride;
   double best = dinf();
   uint32_t bf = NONE, bp = NONE;
   float il = 0.f, ir = 0.f;
@@ -690,19 +695,20 @@ __device__ __forceinline__ void split_reduce_item(const View& v, const StepLists
   }
 }
 
-template <typename IdxT>
+template <typename IdxT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_split_reduce(View v, LevelScratch s) {
   const uint32_t count = live_count(s, s.ctr->n_nodes, s.cap_nodes);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_REDUCE], [&](uint32_t w) { split_reduce_item<IdxT>(v, sl, s, w); });
+  for_items(count, &s.ctr->claim[ITEM_REDUCE], [&](uint32_t w) { split_reduce_item<IdxT, Q>(v, sl, s, w); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void plan_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void plan_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                           const TreeView& tv, uint32_t w) {
   const uint32_t lane = lane_id();
   const ct_node nd = lists.nodes[w];
+  CT_JOB_VIEW(v, vb, nd.slot);
   const ct_split_result r = s.result[w];
   uint32_t split = r.feature != NONE;
   uint32_t children = 0;
@@ -738,7 +744,7 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   const bool big = nd.n > SMALL_SEG;
   const bool huge = big && nd.n >= s.huge_rows && s.huge_segs && huge_partition_ok(v.bit_words);
   const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
-  const uint64_t* nmask = lists.node_mask ? lists.node_mask + (size_t)w * mask_words(v.n_features) : nullptr;
+  const uint64_t* nmask = lists.node_mask ? lists.node_mask + (size_t)w * v.mask_stride : nullptr;
   const uint64_t skip = (nmask ? nmask[0] : 0ull) | virtual_skip(v);
   const uint64_t* skip_hi = nmask && v.n_features > 64 ? nmask + 1 : nullptr;
   // features whose lists move
@@ -772,9 +778,11 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
       PartSeg sg;
       sg.in = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
       sg.out = list_ptr<IdxT>(v, nd.buf ^ 1u, nd.slot, 0) + nd.start;
-      sg.bits = v.bits + (size_t)nd.slot * v.bit_words;
+      sg.bits = slot_bits(v, nd.slot);
       sg.in_fstride = v.stride;
       sg.out_fstride = v.stride;
+      sg.n_features = v.n_features;
+      sg.row_mask = v.row_mask;
       sg.n = nd.n;
       sg.nl = r.pos + 1;
       sg.status = tbase;
@@ -838,27 +846,28 @@ __device__ __forceinline__ void plan_item(const View& v, const StepLists& lists,
   }
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_plan(View v, LevelScratch s, TreeView tv) {
   const uint32_t count = live_count(s, s.ctr->n_nodes, s.cap_nodes);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_PLAN], [&](uint32_t w) { plan_item<IdxT, LabT>(v, sl, s, tv, w); });
+  for_items(count, &s.ctr->claim[ITEM_PLAN], [&](uint32_t w) { plan_item<IdxT, LabT, Q>(v, sl, s, tv, w); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void fill_mark_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void fill_mark_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                                uint32_t* cnt, uint32_t pi) {
-  const uint32_t C = v.n_classes;
+  const uint32_t C = vb.n_classes;
   const uint32_t lane = lane_id();
   const PartPiece pp = s.part[pi];
   const SplitRec sr = s.splits[pp.split];
   const ct_node nd = lists.nodes[sr.node];
+  CT_JOB_VIEW(v, vb, nd.slot);
   // a virtual split feature: its left rows are the node's rows with its low
   // value, read from the row list (row order) and the rows' value bits
   const bool virt = is_virtual(v, sr.feature);
   const IdxT* lst = list_ptr<IdxT>(v, nd.buf, nd.slot, virt ? v.vslot : sr.feature) + nd.start;
-  uint32_t* bw = v.bits + (size_t)nd.slot * v.bit_words;
+  uint32_t* bw = slot_bits(v, nd.slot);
   for (uint32_t c = lane; c < C; c += 32) cnt[c] = 0;
   __syncwarp();
   const uint32_t lo = pp.j * PART_PIECE;
@@ -897,18 +906,18 @@ __device__ __forceinline__ void fill_mark_item(const View& v, const StepLists& l
     if (cnt[c]) atomicAdd(&out[c], cnt[c]);
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_fill_mark(View v, LevelScratch s) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_part_pieces, s.cap_part);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_FILL], [&](uint32_t pi) { fill_mark_item<IdxT, LabT>(v, sl, s, cnt, pi); });
+  for_items(count, &s.ctr->claim[ITEM_FILL], [&](uint32_t pi) { fill_mark_item<IdxT, LabT, Q>(v, sl, s, cnt, pi); });
 }
 
 // ------------------------------------------------------------------------
-template <typename IdxT, typename LabT>
-__device__ __forceinline__ void children_item(const View& v, const StepLists& lists, const LevelScratch& s,
+template <typename IdxT, typename LabT, bool Q>
+__device__ __forceinline__ void children_item(const View& vb, const StepLists& lists, const LevelScratch& s,
                                               const TreeView& tv, uint32_t cap_next, uint32_t small_cut,
                                               ct_node* small, uint32_t cap_small, uint32_t w) {
   const uint32_t lane = lane_id();
@@ -917,6 +926,7 @@ __device__ __forceinline__ void children_item(const View& v, const StepLists& li
   uint32_t* next_tot = lists.next_tot;
   const SplitRec sr = s.splits[w];
   const ct_node nd = lists.nodes[sr.node];
+  CT_JOB_VIEW(v, vb, nd.slot);
   const ct_split_result r = s.result[sr.node];
   const uint32_t nl = sr.pos + 1;
   const uint32_t C = v.n_classes;
@@ -976,8 +986,9 @@ __device__ __forceinline__ void children_item(const View& v, const StepLists& li
       // agree at the child's first and last positions (the child's lists of
       // the others were just partitioned); one mask word per 64 features
       const uint32_t mw = mask_words(v.n_features);
-      const uint64_t* pm = lists.node_mask + (size_t)sr.node * mw;
-      uint64_t* cmw = lists.next_mask + (size_t)idx * mw;
+      const uint32_t stride = Q ? v.mask_stride : mw;  // equal in a fit of one job
+      const uint64_t* pm = lists.node_mask + (size_t)sr.node * stride;
+      uint64_t* cmw = lists.next_mask + (size_t)idx * stride;
       for (uint32_t k = 0; k < mw; ++k) {
         const uint64_t pw = pm[k];
         uint64_t cw = pw;
@@ -998,14 +1009,14 @@ __device__ __forceinline__ void children_item(const View& v, const StepLists& li
   }
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK)
 k_children(View v, LevelScratch s, TreeView tv, uint32_t cap_next, uint32_t small_cut, ct_node* small,
            uint32_t cap_small) {
   const uint32_t count = live_count(s, s.ctr->n_splits, s.cap_nodes);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_CHILDREN], [&](uint32_t w) {
-    children_item<IdxT, LabT>(v, sl, s, tv, cap_next, small_cut, small, cap_small, w);
+    children_item<IdxT, LabT, Q>(v, sl, s, tv, cap_next, small_cut, small, cap_small, w);
   });
 }
 
@@ -1484,15 +1495,16 @@ __device__ void grow_wide(const View& v, const LevelScratch& s, const TreeView& 
 
 
 // Subtree roots of at most 32 rows (the others are skipped).
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
+k_subtree(View vb, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
   __shared__ SubEntry stack_all[WARPS_PER_BLOCK][33];
   const uint32_t lane = lane_id();
   const uint32_t count = live_count(s, s.ctr->n_small, cap_small);
   for_items(count, &s.ctr->claim[ITEM_SUBTREE], [&](uint32_t w) {
     const ct_node nd = small[w];
     if (nd.n > 32) return;
+    CT_JOB_VIEW(v, vb, nd.slot);
     const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
     const IdxT* l0 = list_ptr<IdxT>(v, nd.buf, nd.slot, 0) + nd.start;
     const bool have = lane < nd.n;
@@ -1506,16 +1518,17 @@ k_subtree(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv
 }
 
 // Subtree roots of 33..128 rows (the others are skipped).
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK)
-k_subtree_wide(View v, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
+k_subtree_wide(View vb, const ct_node* __restrict__ small, LevelScratch s, TreeView tv, uint32_t cap_small) {
   extern __shared__ __align__(16) uint32_t sub_smem[];
   const uint32_t lane = lane_id();
   const uint32_t count = live_count(s, s.ctr->n_small, cap_small);
-  uint32_t* wsm = sub_smem + (threadIdx.x >> 5) * subtree_warp_words(v.n_classes);
+  uint32_t* wsm = sub_smem + (threadIdx.x >> 5) * subtree_warp_words(vb.n_classes);
   for_items(count, &s.ctr->claim[ITEM_SUBTREE_WIDE], [&](uint32_t w) {
     const ct_node nd = small[w];
     if (nd.n <= 32) return;
+    CT_JOB_VIEW(v, vb, nd.slot);
     const size_t toff = (size_t)(nd.slot + tv.slot_base) * tv.capacity;
     grow_wide<IdxT, LabT>(v, s, tv, nd, toff, wsm, lane);
   });
@@ -1544,7 +1557,7 @@ uint32_t grid_for(K kernel, uint64_t warps, size_t smem, bool persistent) {
   return item_blocks(warps, cap);
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uint32_t scan_piece, bool persistent,
                 cudaStream_t st) {
   Prof* pf = current_prof();
@@ -1559,27 +1572,27 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
     pf->launched(CT_K_SCAN, 2);
   }
   pf->begin(CT_K_SELECT);
-  k_select<IdxT><<<grid_for(k_select<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s, scan_piece);
+  k_select<IdxT, Q><<<grid_for(k_select<IdxT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s, scan_piece);
   pf->end();
   pf->launched(CT_K_SELECT);
   pf->begin(CT_K_SCAN);
-  k_scan_hist<IdxT, LabT><<<grid_for(k_scan_hist<IdxT, LabT>, caps.scan, sm1, persistent), THREADS_PER_BLOCK, sm1,
+  k_scan_hist<IdxT, LabT, Q><<<grid_for(k_scan_hist<IdxT, LabT, Q>, caps.scan, sm1, persistent), THREADS_PER_BLOCK, sm1,
                             st>>>(v, s, scan_piece);
   k_scan_carry<<<grid_for(k_scan_carry, caps.scan, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
-  k_split_scan<IdxT, LabT><<<grid_for(k_split_scan<IdxT, LabT>, caps.scan, 2 * sm1, persistent), THREADS_PER_BLOCK,
+  k_split_scan<IdxT, LabT, Q><<<grid_for(k_split_scan<IdxT, LabT, Q>, caps.scan, 2 * sm1, persistent), THREADS_PER_BLOCK,
                              2 * sm1, st>>>(v, s, scan_piece);
   if (v.fbin)
-    k_scan_two_valued<IdxT, LabT><<<grid_for(k_scan_two_valued<IdxT, LabT>, caps.scan, sm1, persistent),
+    k_scan_two_valued<IdxT, LabT, Q><<<grid_for(k_scan_two_valued<IdxT, LabT, Q>, caps.scan, sm1, persistent),
                                     THREADS_PER_BLOCK, sm1, st>>>(v, s, scan_piece);
   pf->end();
   pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
   pf->begin(CT_K_REDUCE);
-  k_split_reduce<IdxT><<<grid_for(k_split_reduce<IdxT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
+  k_split_reduce<IdxT, Q><<<grid_for(k_split_reduce<IdxT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
   pf->end();
   pf->launched(CT_K_REDUCE);
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 void partition_impl(const View& v, const LevelScratch& s_all, const LevelCaps& caps, const TreeView& tv,
                     bool persistent, cudaStream_t st) {
   Prof* pf = current_prof();
@@ -1588,9 +1601,9 @@ void partition_impl(const View& v, const LevelScratch& s_all, const LevelCaps& c
   s.cap_status = caps.status;
   const size_t sm1 = (size_t)WARPS_PER_BLOCK * v.n_classes * sizeof(uint32_t);
   pf->begin(CT_K_MARK);
-  k_plan<IdxT, LabT><<<grid_for(k_plan<IdxT, LabT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s,
+  k_plan<IdxT, LabT, Q><<<grid_for(k_plan<IdxT, LabT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s,
                                                                                                             tv);
-  k_fill_mark<IdxT, LabT><<<grid_for(k_fill_mark<IdxT, LabT>, caps.part, sm1, persistent), THREADS_PER_BLOCK, sm1,
+  k_fill_mark<IdxT, LabT, Q><<<grid_for(k_fill_mark<IdxT, LabT, Q>, caps.part, sm1, persistent), THREADS_PER_BLOCK, sm1,
                             st>>>(v, s);
   pf->launched(CT_K_MARK, 2);
   pf->end();
@@ -1601,12 +1614,12 @@ void partition_impl(const View& v, const LevelScratch& s_all, const LevelCaps& c
   pf->launched(CT_K_PARTITION, 2);
 }
 
-template <typename IdxT, typename LabT>
+template <typename IdxT, typename LabT, bool Q>
 void children_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, const TreeView& tv, uint32_t cap_next,
                    uint32_t small_cut, ct_node* small, uint32_t cap_small, bool persistent, cudaStream_t st) {
   Prof* pf = current_prof();
   pf->begin(CT_K_CHILDREN);
-  k_children<IdxT, LabT><<<grid_for(k_children<IdxT, LabT>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(
+  k_children<IdxT, LabT, Q><<<grid_for(k_children<IdxT, LabT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(
       v, s, tv, cap_next, small_cut, small, cap_small);
   pf->end();
   pf->launched(CT_K_CHILDREN);
@@ -1702,56 +1715,89 @@ uint32_t item_blocks(uint64_t warps, uint32_t grid_cap) {
   return (uint32_t)std::min<uint64_t>(b, 0x7fffffffull);
 }
 
-int launch_split(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b, uint32_t scan_piece,
-                 bool persistent, cudaStream_t st) {
+// Q: the view is a forest queue's batch view (View::jobs); the kernels of
+// one fit are instantiated without the job lookup.
+template <bool Q>
+int launch_split_q(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
+                   uint32_t scan_piece, bool persistent, cudaStream_t st) {
   LevelCaps caps = level_caps(v, scan_piece, b);
   caps.scan = min(caps.scan, s.cap_scan);
   caps.carry = min(caps.carry, s.cap_carry);
-#define CALL(I, L) split_impl<I, L>(v, s, caps, scan_piece, persistent, st)
+#define CALL(I, L) split_impl<I, L, Q>(v, s, caps, scan_piece, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
+int launch_split(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b, uint32_t scan_piece,
+                 bool persistent, cudaStream_t st) {
+  return v.jobs ? launch_split_q<true>(v, ib, lb, s, b, scan_piece, persistent, st)
+                : launch_split_q<false>(v, ib, lb, s, b, scan_piece, persistent, st);
+}
 
-int launch_partition(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
-                     const TreeView& tv, bool persistent, cudaStream_t st) {
+template <bool Q>
+int launch_partition_q(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
+                       const TreeView& tv, bool persistent, cudaStream_t st) {
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
   caps.part = min(caps.part, s.cap_part);
   caps.status = min(caps.status, s.cap_status);
-#define CALL(I, L) partition_impl<I, L>(v, s, caps, tv, persistent, st)
+#define CALL(I, L) partition_impl<I, L, Q>(v, s, caps, tv, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }
+int launch_partition(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
+                     const TreeView& tv, bool persistent, cudaStream_t st) {
+  return v.jobs ? launch_partition_q<true>(v, ib, lb, s, b, tv, persistent, st)
+                : launch_partition_q<false>(v, ib, lb, s, b, tv, persistent, st);
+}
 
+template <bool Q>
+int launch_children_q(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b,
+                      const TreeView& tv, uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small,
+                      bool persistent, cudaStream_t st) {
+  LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
+#define CALL(I, L) children_impl<I, L, Q>(v, s, caps, tv, cap_next, small_cut, small, cap_small, persistent, st)
+  CT_DISPATCH(ib, lb, CALL);
+#undef CALL
+  CT_CUDA_TRY(cudaGetLastError());
+  return CT_OK;
+}
 int launch_children(const View& v, uint32_t ib, uint32_t lb, const LevelScratch& s, LevelBounds b, const TreeView& tv,
                     uint32_t cap_next, uint32_t small_cut, ct_node* small, uint32_t cap_small, bool persistent,
                     cudaStream_t st) {
-  LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
-#define CALL(I, L) children_impl<I, L>(v, s, caps, tv, cap_next, small_cut, small, cap_small, persistent, st)
-  CT_DISPATCH(ib, lb, CALL);
-#undef CALL
-  CT_CUDA_TRY(cudaGetLastError());
-  return CT_OK;
+  return v.jobs ? launch_children_q<true>(v, ib, lb, s, b, tv, cap_next, small_cut, small, cap_small, persistent, st)
+                : launch_children_q<false>(v, ib, lb, s, b, tv, cap_next, small_cut, small, cap_small, persistent, st);
 }
 
+template <bool Q>
+int launch_subtrees_q(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
+                      uint32_t bound, bool wide, bool persistent, const LevelScratch& s, const TreeView& tv,
+                      cudaStream_t st);
 int launch_subtrees(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small, uint32_t bound,
                     bool wide, bool persistent, const LevelScratch& s, const TreeView& tv, cudaStream_t st) {
+  return v.jobs ? launch_subtrees_q<true>(v, ib, lb, small, cap_small, bound, wide, persistent, s, tv, st)
+                : launch_subtrees_q<false>(v, ib, lb, small, cap_small, bound, wide, persistent, s, tv, st);
+}
+
+template <bool Q>
+int launch_subtrees_q(const View& v, uint32_t ib, uint32_t lb, const ct_node* small, uint32_t cap_small,
+                      uint32_t bound, bool wide, bool persistent, const LevelScratch& s, const TreeView& tv,
+                      cudaStream_t st) {
   if (cap_small == 0 || bound == 0) return CT_OK;
   Prof* pf = current_prof();
   pf->begin(CT_K_SUBTREE);
   const uint32_t items = std::min(bound, cap_small);
 #define CALL(I, L)                                                                                           \
-  k_subtree<I, L><<<grid_for(k_subtree<I, L>, items, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, \
+  k_subtree<I, L, Q><<<grid_for(k_subtree<I, L, Q>, items, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, small, s, tv, \
                                                                                                 cap_small)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
   if (wide) {
     const size_t smem = (size_t)WARPS_PER_BLOCK * subtree_warp_words(v.n_classes) * sizeof(uint32_t);
 #define CALL(I, L)                                                                                      \
-  k_subtree_wide<I, L><<<grid_for(k_subtree_wide<I, L>, items, smem, persistent), THREADS_PER_BLOCK, smem, st>>>( \
+  k_subtree_wide<I, L, Q><<<grid_for(k_subtree_wide<I, L, Q>, items, smem, persistent), THREADS_PER_BLOCK, smem, st>>>( \
       v, small, s, tv, cap_small)
     CT_DISPATCH(ib, lb, CALL);
 #undef CALL
@@ -1795,7 +1841,6 @@ PartWork level_part_work(const View& v, const LevelScratch& s) {
   w.ticket = &s.ctr->ticket;
   w.error = &s.ctr->error;
   w.n_features = v.n_features;
-  w.row_mask = v.row_mask;
   return w;
 }
 
@@ -1921,6 +1966,11 @@ View make_view(const ct_problem* p, const ct_lists* l) {
   v.vrow = nullptr;
   v.vval = nullptr;
   v.vslot = 0;
+  v.jobs = nullptr;
+  v.slot_job = nullptr;
+  v.slot_base = 0;
+  v.sel_stride = p->max_features;
+  v.mask_stride = mask_words(p->n_features);
   return v;
 }
 

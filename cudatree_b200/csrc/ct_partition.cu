@@ -55,8 +55,9 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
   for (uint64_t it = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; it < items; it += nwarps) {
     const uint32_t si = (uint32_t)(it / nfb);
     const uint32_t f_lo = (uint32_t)(it - (uint64_t)si * nfb) * FEAT_BLOCK;
-    const uint32_t f_hi = min(f_lo + FEAT_BLOCK, F);
     const PartSeg sg = w.small[si];
+    if (f_lo >= sg.n_features) continue;  // a job of fewer features than the batch's most
+    const uint32_t f_hi = min(f_lo + FEAT_BLOCK, sg.n_features);
     const IdxT* in = reinterpret_cast<const IdxT*>(sg.in);
     IdxT* out = reinterpret_cast<IdxT*>(sg.out);
     const uint32_t n = sg.n, nl = sg.nl;
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
       for (uint32_t r = 0; r < R; ++r) {
         if (f_lo + r * per >= f_hi) break;
         const uint32_t f = f_lo + r * per + sub;
-        const bool left = valid[r] && left_bit(sg.bits, rows[r] & w.row_mask);
+        const bool left = valid[r] && left_bit(sg.bits, rows[r] & sg.row_mask);
         const unsigned lm = __ballot_sync(FULL, left) & gmask;
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (p - rl);
@@ -98,7 +99,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         if (f >= f_hi) break;
         if (seg_skips(sg, f)) continue;
         const bool valid = lane < n;
-        const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
+        const bool left = valid && left_bit(sg.bits, rows[r] & sg.row_mask);
         const unsigned lm = __ballot_sync(FULL, left);
         const uint32_t rl = __popc(lm & lt);
         const uint32_t dst = left ? rl : nl + (lane - rl);
@@ -122,7 +123,7 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
           if (r >= rounds) break;
           const uint32_t p = r * 32 + lane;
           const bool valid = p < n;
-          const bool left = valid && left_bit(sg.bits, rows[r] & w.row_mask);
+          const bool left = valid && left_bit(sg.bits, rows[r] & sg.row_mask);
           const unsigned lm = __ballot_sync(FULL, left);
           const uint32_t rl = run + __popc(lm & lt);
           const uint32_t dst = left ? rl : nl + (p - rl);
@@ -329,8 +330,8 @@ __device__ __forceinline__ bool run_chain(const Env& env, const PartWork& w, con
     const uint32_t lo = j * TILE;
     const uint32_t cnt = min(TILE, n - lo);
     const IdxT* rows = reinterpret_cast<const IdxT*>(sbuf[b]) + s_off[b];
-    carry += cnt == TILE ? part_tile<IdxT, ROUNDS, true>(env, rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt)
-                         : part_tile<IdxT, ROUNDS, false>(env, rows, cnt, lo, sg, w.row_mask, out, n, carry, s_wcnt);
+    carry += cnt == TILE ? part_tile<IdxT, ROUNDS, true>(env, rows, cnt, lo, sg, sg.row_mask, out, n, carry, s_wcnt)
+                         : part_tile<IdxT, ROUNDS, false>(env, rows, cnt, lo, sg, sg.row_mask, out, n, carry, s_wcnt);
     env.sync();  // tile buffer and s_wcnt free for reuse
   }
   return true;
@@ -449,13 +450,12 @@ __global__ void __launch_bounds__(SEG_THREADS, 1) k_part_seg(PartWork w) {
 
 template <typename K>
 int resident_blocks(K kernel, int threads, size_t dyn_smem = 0) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
+  static const int sms = [] {  // initialized once, thread-safe
+    int dev = 0, n = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (sms <= 0) sms = 148;
-  }
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+  }();
   int per = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, dyn_smem);
   return sms * (per > 0 ? per : 1);
@@ -464,12 +464,10 @@ int resident_blocks(K kernel, int threads, size_t dyn_smem = 0) {
 template <typename IdxT, uint32_t ROUNDS, uint32_t RING, uint32_t MINB>
 int launch_big_v(const PartWork& w, uint64_t want, cudaStream_t st) {
   const size_t smem = RING * ring_buf_bytes<IdxT, ROUNDS>();
-  static bool configured = false;  // per instantiation; the attribute is per device function
-  if (!configured) {
-    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_big<IdxT, ROUNDS, RING, MINB>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    configured = true;
-  }
+  // per instantiation (the attribute is per device function); once, thread-safe
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      k_part_big<IdxT, ROUNDS, RING, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  CT_CUDA_TRY(configured);
   const int cap = resident_blocks(k_part_big<IdxT, ROUNDS, RING, MINB>, BIG_THREADS, smem);
   k_part_big<IdxT, ROUNDS, RING, MINB><<<(uint32_t)std::min<uint64_t>(want, cap), BIG_THREADS, smem, st>>>(w);
   CT_CUDA_TRY(cudaGetLastError());
@@ -498,13 +496,11 @@ int launch_seg(const PartWork& w, cudaStream_t st) {
   constexpr uint32_t ROUNDS = 8, RING = 2;
   const size_t smem = (((size_t)w.bit_words * 4 + 127) & ~size_t(127)) +
                       (size_t)SEG_GROUPS * RING * ring_buf_bytes<IdxT, ROUNDS>();
-  static bool configured = false;  // per instantiation: the largest staging it can take
-  if (!configured) {
-    const size_t most = (size_t)HUGE_BITS_MAX + 128 + (size_t)SEG_GROUPS * RING * ring_buf_bytes<IdxT, ROUNDS>();
-    CT_CUDA_TRY(cudaFuncSetAttribute(k_part_seg<IdxT, ROUNDS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)most));
-    configured = true;
-  }
+  // per instantiation, the largest staging it can take; once, thread-safe
+  static const cudaError_t configured = cudaFuncSetAttribute(
+      k_part_seg<IdxT, ROUNDS, RING>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      (int)((size_t)HUGE_BITS_MAX + 128 + (size_t)SEG_GROUPS * RING * ring_buf_bytes<IdxT, ROUNDS>()));
+  CT_CUDA_TRY(configured);
   int dev = 0, sms = 0;
   CT_CUDA_TRY(cudaGetDevice(&dev));
   CT_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));

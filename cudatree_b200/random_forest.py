@@ -120,6 +120,20 @@ def compact_labels(y):
     return np.unique(y, return_inverse=True)
 
 
+def fetch_tree_columns(tb, n_nodes, kk, dev):
+    """(node counts, [left, right, feature, threshold, value]) of the trees in
+    slots 0..kk-1 of raw tree buffers, canonical order, concatenated (one
+    device canonicalization and one read-back)."""
+    counts = n_nodes[:kk].cpu().numpy().astype(np.uint32)
+    total = int(counts.sum())
+    cols = [np.empty(total, dt) for dt in (np.uint32, np.uint32, np.uint16, np.float32, np.uint32)]
+    sb = int(_lib.load().ct_fetch_trees_scratch(total, kk))
+    scratch = _dev_bytes(sb, dev)
+    _lib.call("ct_fetch_trees", C.byref(tb), kk, counts.ctypes.data, _ptr(scratch), sb,
+              *[c.ctypes.data for c in cols], _stream())
+    return counts, cols
+
+
 def unpack_trees(packed, offsets, n_features, dtype_labels):
     """Inverse of pack_trees: RandomClassifierTree objects from packed nodes."""
     from .random_tree import restore_tree
@@ -396,13 +410,7 @@ class RandomForestClassifier:
     def _fetch_trees(self, tb, n_nodes, kk, dev):
         """The kk trees of the last ct_fit call, canonical order, as tree objects
         over slices of five concatenated host arrays (one read-back)."""
-        counts = n_nodes[:kk].cpu().numpy().astype(np.uint32)
-        total = int(counts.sum())
-        cols = [np.empty(total, dt) for dt in (np.uint32, np.uint32, np.uint16, np.float32, np.uint32)]
-        sb = int(_lib.load().ct_fetch_trees_scratch(total, kk))
-        scratch = _dev_bytes(sb, dev)
-        _lib.call("ct_fetch_trees", C.byref(tb), kk, counts.ctypes.data, _ptr(scratch), sb,
-                  *[c.ctypes.data for c in cols], _stream())
+        counts, cols = fetch_tree_columns(tb, n_nodes, kk, dev)
         out, o = [], 0
         for c in counts.tolist():
             out.append(self._make_tree(*[col[o:o + c] for col in cols]))

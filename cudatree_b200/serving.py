@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .forest_queue import fit_forests  # noqa: F401  (the forest queue: shared level steps)
 from .random_forest import PACKED_DTYPE, RandomForestClassifier, pack_trees, restore_forest, unpack_trees
 
 CT_REQ_PREDICT = 0
@@ -47,46 +48,6 @@ class ServerStats(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
-
-
-def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, workers=8):
-    """Forest queue: fit many independent forests concurrently, one CUDA
-    stream and device arena per fit worker, and return them as
-    RandomForestClassifier objects.  jobs: sequence of (x, y).  Each forest
-    is the one RandomForestClassifier(n_estimators, max_features, seed=seeds[i])
-    .fit(x, y) grows alone (same canonical rule, same seed)."""
-    jobs = list(jobs)
-    if not jobs:
-        return []
-    seeds = list(range(len(jobs))) if seeds is None else list(seeds)
-    prepared = []
-    for x, y in jobs:
-        x = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
-        table, ids = np.unique(np.asarray(y), return_inverse=True)
-        prepared.append((x, table, ids.astype(np.uint32)))
-    max_rows = max(p[0].shape[0] for p in prepared)
-    max_f = max(p[0].shape[1] for p in prepared)
-    max_c = max(p[1].shape[0] for p in prepared)
-    srv = ForestServer(max_batch_rows=4096, max_features=max_f, small_rows=1024, fit_workers=workers,
-                       max_fit_rows=max_rows, max_fit_trees=n_estimators, max_classes=max(64, max_c))
-    try:
-        reqs, keep = [], []
-        for (x, table, ids), seed in zip(prepared, seeds):
-            xp, yp = x, np.ascontiguousarray(ids, dtype=np.uint32)  # pageable: no page-locking per job
-            m = 0 if max_features is None else int(max_features)
-            r = srv.fit_request(xp, yp, n_classes=int(table.shape[0]), n_trees=n_estimators, seed=int(seed),
-                                max_features=m)
-            srv.submit(r)
-            reqs.append(r)
-            keep.append((xp, yp))
-        out = []
-        for r, (x, table, ids), seed in zip(reqs, prepared, seeds):
-            _lib.check(srv.wait(r, 600.0))
-            params = {"max_features": max_features, "seed": int(seed)}
-            out.append(srv.forest(r.result_forest, table=table, params=params))
-        return out
-    finally:
-        srv.close()
 
 
 def _host_ptr(a) -> int:

@@ -229,6 +229,28 @@ int ct_fit(const ct_problem* p, const ct_lists* lists, uint32_t first_tree, uint
            const ct_fit_options* opt, const ct_tree_buffers* trees, void* workspace,
            size_t workspace_bytes, void* stream);
 
+/* Forest queue: the batched fit of n_jobs independent forests through
+ * shared level steps (one node list and one set of launches for all jobs'
+ * nodes; the reference runs a queue as independent fits,
+ * hybridforest/builder.py:79-141).  Job j grows trees first_tree ..
+ * first_tree+n_trees-1 of its own problem into its lists, exactly the trees
+ * ct_fit grows for it alone.  Its trees go to consecutive slots of `trees`,
+ * after the slots of the jobs before it; trees->capacity must be at least
+ * 2 * every job's n_rows.  Every job has the same index_bytes and
+ * label_bytes; opt->mode must be CT_FIT_BATCHED (huge_rows is ignored: the
+ * partition of big nodes reads marks from global memory).  ct_fit_stats
+ * reports the whole queue. */
+typedef struct ct_fit_job {
+  ct_problem problem;
+  ct_lists lists;            /* n_slots >= n_trees                            */
+  uint32_t n_trees;
+  uint32_t first_tree;
+} ct_fit_job;
+int ct_fit_queue_workspace_size(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* opt,
+                                size_t* bytes);
+int ct_fit_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* opt,
+                 const ct_tree_buffers* trees, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Per-kernel-group statistics of the last ct_fit on the calling thread.
  * Launch counts and algorithmic bytes are always recorded; ms[] is filled
  * with CT_FIT_PROFILE (CUDA events recorded on the fit's stream around each

@@ -221,3 +221,34 @@ def test_fit_rejects_bad_partition_options_before_any_launch():
         st = lib.ct_fit(C.byref(prob), C.byref(lists), 0, 4, C.byref(opts), C.byref(trees), C.c_void_p(fake), 0,
                         None)
         assert st == 1 and text in _lib.last_error()
+
+
+def test_queue_fit_checks_jobs_before_any_launch():
+    """ct_fit_queue refuses, with CT_ERR_ARG and no device work, jobs of
+    different index widths, a job without trees and tree buffers too small
+    for a job (the pointers here are never dereferenced)."""
+    lib = _lib.load()
+    fake = 256
+    jobs = (_lib.FitJob * 2)()
+    for k in range(2):
+        jobs[k].problem = _lib.Problem(fake, fake, fake, 1000, 8, 3, 2, 1, 3, 1, 1, k)
+        jobs[k].lists = _lib.Lists(fake, fake, fake, 1000, 4)
+        jobs[k].n_trees = 4
+    trees = _lib.TreeBuffers(fake, fake, fake, fake, fake, fake, 2000)
+    opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, 0, 0)
+    ws = C.c_size_t()
+    assert lib.ct_fit_queue_workspace_size(jobs, 2, C.byref(opts), C.byref(ws)) == 0 and ws.value > 0
+    jobs[1].problem.index_bytes = 4
+    st = lib.ct_fit_queue(jobs, 2, C.byref(opts), C.byref(trees), C.c_void_p(fake), ws.value, None)
+    assert st == 1 and "index_bytes" in _lib.last_error()
+    jobs[1].problem.index_bytes = 2
+    jobs[1].n_trees = 0
+    st = lib.ct_fit_queue(jobs, 2, C.byref(opts), C.byref(trees), C.c_void_p(fake), ws.value, None)
+    assert st == 1 and "no trees" in _lib.last_error()
+    jobs[1].n_trees = 4
+    small = _lib.TreeBuffers(fake, fake, fake, fake, fake, fake, 100)
+    st = lib.ct_fit_queue(jobs, 2, C.byref(opts), C.byref(small), C.c_void_p(fake), ws.value, None)
+    assert st == 1 and "capacity" in _lib.last_error()
+    plain = _lib.FitOptions(_lib.CT_FIT_PLAIN, 0, 0, 0)
+    st = lib.ct_fit_queue(jobs, 2, C.byref(plain), C.byref(trees), C.c_void_p(fake), ws.value, None)
+    assert st == 1 and "batched" in _lib.last_error()

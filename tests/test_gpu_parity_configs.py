@@ -117,7 +117,7 @@ def test_digits_shaped_all_50_trees_match_oracle(cuda_device, pool):
 def test_forest_queue_sample_matches_oracle(cuda_device, pool):
     futs = {j: oracle_jobs.submit_forest(pool, "blob_job", j, 10, j, None, True) for j in QUEUE_SAMPLE}
     jobs = [synthetic.blob_job(j) for j in QUEUE_SAMPLE]
-    forests = fit_forests(jobs, n_estimators=10, seeds=QUEUE_SAMPLE, workers=4)
+    forests = fit_forests(jobs, n_estimators=10, seeds=QUEUE_SAMPLE)
     for j, (x, y), f in zip(QUEUE_SAMPLE, jobs, forests):
         ref = [fu.result() for fu in futs[j]]
         _assert_same_trees(f._trees, ref, f"queue job {j} {x.shape}")

@@ -186,7 +186,7 @@ def test_forest_queue_matches_solo_fits(cuda_device):
         x, y = _blobs(n, f, c, 100 + j)
         jobs.append((x, y * 3 + 1))  # labels that need compaction
     seeds = [1000 + j for j in range(len(jobs))]
-    got = fit_forests(jobs, n_estimators=6, seeds=seeds, workers=3)
+    got = fit_forests(jobs, n_estimators=6, seeds=seeds)
     for (x, y), seed, g in zip(jobs, seeds, got):
         solo = RandomForestClassifier(n_estimators=6, seed=seed).fit(x, y)
         _same_trees(g, solo)
