@@ -34,7 +34,11 @@ WORKLOAD = ("covtype-shaped synthetic 581012x54 f32 (10 Gaussian + 44 one-hot), 
             "100 trees, bootstrap, max_features=7, uint32 indices, fully grown")
 N_TREES = 100
 MAX_FEATURES = 7
-PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.85
+# DRAM bytes (ncu dram__bytes_read.sum + dram__bytes_write.sum) per
+# algorithmic byte of the partition and the split-scan kernel groups, over
+# every launch of one profiled 16-tree fit of this workload
+PARTITION_DRAM_PER_ALGORITHMIC_BYTE = 0.71
+SCAN_DRAM_PER_ALGORITHMIC_BYTE = 1.00
 
 
 def peaks():
@@ -532,6 +536,9 @@ def run_ours(args, world, rank, local):
     traffic = (PARTITION_DRAM_PER_ALGORITHMIC_BYTE * stats["bytes"][pi] / p_launches) if p_launches else None
     si = groups.index("scan")
     s_ms = stats["ms"][si]
+    s_gbs = stats["bytes"][si] / (s_ms * 1e6) if s_ms > 0 else None
+    s_launches = stats["launches"][si]
+    s_traffic = (SCAN_DRAM_PER_ALGORITHMIC_BYTE * stats["bytes"][si] / s_launches) if s_launches else None
     cpu = None
     if not args.skip_cpu:
         cores = len(os.sched_getaffinity(0))
@@ -558,9 +565,15 @@ def run_ours(args, world, rank, local):
                      "traffic_unit": f"DRAM bytes per launch (ncu ratio {PARTITION_DRAM_PER_ALGORITHMIC_BYTE} x algorithmic, 16-tree capture)",
                      "algorithmic_bytes_per_launch": round(stats["bytes"][pi] / p_launches) if p_launches else None,
                      "algorithmic_bytes_per_element": "n_features x (2 x index_bytes + 1)"},
-        "scan_roofline": {"kernel": "k_split_scan (+hist/carry)",
-                          "achieved": round(stats["bytes"][si] / (s_ms * 1e6), 1) if s_ms > 0 else None,
-                          "peak": peak, "unit": "GB/s"},
+        "scan_roofline": {"bound": "hbm", "kernel": "k_split_scan (+hist, carry, two-valued, virtual counts)",
+                          "achieved": round(s_gbs, 1) if s_gbs else None, "peak": peak, "unit": "GB/s",
+                          "frac": round(s_gbs / peak, 4) if s_gbs else None, "peak_kind": peak_kind,
+                          "traffic": round(s_traffic) if s_traffic else None,
+                          "traffic_unit": f"DRAM bytes per launch (ncu ratio {SCAN_DRAM_PER_ALGORITHMIC_BYTE} x "
+                                          f"algorithmic, 16-tree capture)",
+                          "algorithmic_bytes_per_launch": round(stats["bytes"][si] / s_launches) if s_launches else None,
+                          "algorithmic_bytes_per_element": "per (node, selected feature, position): index_bytes "
+                                                           "+ 4 (x gather) + label gather when labels are not packed"},
         "predict": serving,
         "configs": configs,
         "cpu_baseline": cpu,
