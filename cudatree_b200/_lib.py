@@ -70,7 +70,7 @@ class FitOptions(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("bfs_threshold", C.c_uint32), ("subtree_cutoff", C.c_uint32),
                 ("scan_piece", C.c_uint32), ("flags", C.c_uint32), ("step_nodes", C.c_uint32),
                 ("graph_samples", C.c_uint32), ("part_shape", C.c_uint32), ("huge_rows", C.c_uint32),
-                ("reserved", C.c_uint32)]
+                ("small_rows", C.c_uint32)]
 
 
 class FitJob(C.Structure):

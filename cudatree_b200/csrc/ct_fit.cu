@@ -216,6 +216,7 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   carve_level_scratch(a, v, caps, &L->s, L->virt);
   L->s.huge_rows = o->huge_rows ? o->huge_rows : HUGE_SEG;
   L->s.part_shape = o->part_shape;
+  L->s.small_rows = o->small_rows ? o->small_rows : default_small_rows(p->index_bytes);
   L->ctl = a.take<LoopCtl>(1);
   L->bytes = a.used + 256;
   return base != nullptr && a.ok();
@@ -836,11 +837,12 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
 }  // namespace
 
 // Autotuner candidates.  Every option here grows the same trees, so they are
-// chosen by timing.  The batched form is tuned in two stages: the scan piece
-// length x the warp-subtree cutoff with the default partition, then the
-// partition shape of big segments (tile, ring buffers, CTAs per SM) x the
-// size from which a node partitions with its tree's mark bits in shared
-// memory, around the first stage's choice.  The plain form tunes the
+// chosen by timing.  The batched form is tuned in three stages, each around
+// the choice before it: the scan piece length x the warp-subtree cutoff
+// with the default partition; the partition shape of big segments (tile,
+// ring buffers, CTAs per SM) x the size from which a node partitions with
+// its tree's mark bits in shared memory; the size up to which a node
+// partitions one warp per (node, 8 features).  The plain form tunes the
 // depth-first/breadth-first switch (the quantity the reference fits offline,
 // estimate_threshold.py, and predicts with random_forest.py:278-289).
 std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode, int stage,
@@ -855,7 +857,13 @@ std::vector<ct_fit_options> tune_candidates(const ct_problem* p, uint32_t mode, 
         o.scan_piece = sp;
         c.push_back(o);
       }
-  } else if (mode == CT_FIT_BATCHED) {
+  } else if (mode == CT_FIT_BATCHED && stage == 2) {
+    for (uint32_t small : {0u, 512u, 2048u, 8192u}) {
+      ct_fit_options o = base;
+      o.small_rows = small;
+      c.push_back(o);
+    }
+  } else if (mode == CT_FIT_BATCHED && stage == 1) {
     for (uint32_t shape = 0; shape < CT_PART_SHAPES; ++shape)
       for (uint32_t huge : {0u, 16384u, 0xffffffffu}) {
         ct_fit_options o = base;
@@ -899,8 +907,8 @@ int autotune(const ct_problem* p, const ct_lists* l, uint32_t n_trees, uint32_t 
   float top = 3.0e38f;
   int rc = CT_OK;
   bool any = false;
-  for (int stage = 0; stage < 2 && rc == CT_OK; ++stage) {
-    if (stage == 1 && !any) break;
+  for (int stage = 0; stage < 3 && rc == CT_OK; ++stage) {
+    if (stage > 0 && !any) break;
     const ct_fit_options base = *best;
     for (const ct_fit_options& o : tune_candidates(p, mode, stage, base)) {
       if (fit_workspace_bytes(p, n_trees, &o) > wsb) continue;
@@ -948,6 +956,8 @@ int fit(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint32_t n_
   CT_ARG_CHECK(o && (o->mode == CT_FIT_PLAIN || o->mode == CT_FIT_BATCHED), "bad fit mode");
   CT_ARG_CHECK(o->part_shape < CT_PART_SHAPES, "part_shape out of range");
   CT_ARG_CHECK(o->huge_rows == 0 || o->huge_rows >= CT_HUGE_ROWS_MIN, "huge_rows must be 0 or >= 4096");
+  CT_ARG_CHECK(o->small_rows == 0 || (o->small_rows >= 512 && o->small_rows <= 65536),
+               "small_rows must be 0 or in [512, 65536]");
   CT_ARG_CHECK(n_trees >= 1, "n_trees must be >= 1");
   CT_ARG_CHECK(trees->capacity >= 2u * p->n_rows, "tree capacity must be >= 2 * n_rows");
   CT_ARG_CHECK(l->stride >= p->n_rows, "list stride must be >= n_rows");
@@ -1206,6 +1216,7 @@ bool layout_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options*
   L->s.cap_huge = 0;
   L->s.huge_rows = 0xffffffffu;
   L->s.part_shape = o->part_shape;
+  L->s.small_rows = o->small_rows ? o->small_rows : default_small_rows(jobs[0].problem.index_bytes);
   L->ctl = a.take<LoopCtl>(1);
   *views_dev = a.take<View>(n_jobs);
   *slot_job_dev = a.take<uint32_t>(q.slots);
@@ -1227,6 +1238,8 @@ int check_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o
   CT_ARG_CHECK(jobs && n_jobs >= 1, "no jobs");
   CT_ARG_CHECK(o && o->mode == CT_FIT_BATCHED, "a forest queue takes the batched form");
   CT_ARG_CHECK(o->part_shape < CT_PART_SHAPES, "part_shape out of range");
+  CT_ARG_CHECK(o->small_rows == 0 || (o->small_rows >= 512 && o->small_rows <= 65536),
+               "small_rows must be 0 or in [512, 65536]");
   CT_ARG_CHECK(trees && trees->left && trees->right && trees->feature && trees->threshold && trees->value &&
                    trees->n_nodes,
                "tree buffers are NULL");

@@ -384,6 +384,7 @@ struct LevelScratch {
   StepLists* step;
   uint32_t huge_rows;     // segments of at least this many rows take k_part_seg (>= HUGE_SEG)
   uint32_t part_shape;    // CT_PART_* of k_part_big
+  uint32_t small_rows;    // segments of at most this many rows take k_part_small (>= SMALL_SEG)
   // Virtual features (View::vmask), else NULL / 0:
   uint32_t* vcnt;         // [cap_nodes][64] rows of each node with the feature's high value
   uint32_t* vcls;         // [cap_nodes][n_features][n_classes] those rows by class
@@ -471,6 +472,10 @@ __host__ __device__ __forceinline__ bool huge_partition_ok(uint32_t bit_words) {
   return (uint64_t)bit_words * 4u <= HUGE_BITS_MAX;
 }
 constexpr uint32_t SMALL_SEG = 32 * PART_ROUNDS; // segments up to this size: one warp
+// Default ct_fit_options.small_rows: with 16-bit entries a warp per (segment,
+// 8 features) beats a CTA per chain up to a few thousand rows (the CTA's tile
+// of 2,048 entries is mostly idle there); with 32-bit entries from 513 rows on.
+inline uint32_t default_small_rows(uint32_t index_bytes) { return index_bytes == 2 ? 4096u : SMALL_SEG; }
 constexpr int WARPS_PER_BLOCK = 4;
 constexpr int THREADS_PER_BLOCK = 32 * WARPS_PER_BLOCK;
 

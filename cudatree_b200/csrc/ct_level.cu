@@ -741,7 +741,7 @@ __device__ __forceinline__ void plan_item(const View& vb, const StepLists& lists
   children = __shfl_sync(FULL, children, 0);
   if (!split) return;
   const uint32_t npp = ceil_div(nd.n, PART_PIECE);
-  const bool big = nd.n > SMALL_SEG;
+  const bool big = nd.n > s.small_rows;
   const bool huge = big && nd.n >= s.huge_rows && s.huge_segs && huge_partition_ok(v.bit_words);
   const uint32_t ntiles = big ? ceil_div(nd.n, TILE_ELEMS) : 0u;
   const uint64_t* nmask = lists.node_mask ? lists.node_mask + (size_t)w * v.mask_stride : nullptr;
@@ -1677,6 +1677,7 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.step = a.take<StepLists>(1);
   t.huge_rows = HUGE_SEG;
   t.part_shape = 0;
+  t.small_rows = SMALL_SEG;
   t.vcnt = virt ? a.take<uint32_t>((size_t)c.nodes * 64) : nullptr;
   t.vcls = virt ? a.take<uint32_t>((size_t)c.nodes * v.n_features * C) : nullptr;
   t.vpieces = virt ? a.take<uint2>(c.vpieces) : nullptr;

@@ -8,11 +8,12 @@
 // entry & row_mask, since fit lists carry the label above the row id.
 // Two kernels by segment size:
 //
-//   k_part_small  n <= SMALL_SEG: one warp per segment loops over all
+//   k_part_small  n <= small_rows (ct_fit_options, default SMALL_SEG): one
+//                 warp per segment loops over all
 //                 features; ranks are popc of a ballot.  For n <= 16 a warp
 //                 packs 32/g features per round in lane groups of width
 //                 g = next_pow2(n), so tiny nodes keep the lanes busy.
-//   k_part_big    n > SMALL_SEG: persistent CTAs claim whole (segment,
+//   k_part_big    larger n: persistent CTAs claim whole (segment,
 //                 feature) chains from a ticket counter and stream the chain's
 //                 tiles of TILE elements in order through a ring of shared-
 //                 memory buffers filled by TMA bulk copies; the running left
@@ -106,29 +107,34 @@ __global__ void __launch_bounds__(SMALL_THREADS, 4) k_part_small(PartWork w) {
         if (valid && dst < n) __stcs(out + (size_t)f * sg.out_fstride + dst, (IdxT)rows[r]);
       }
     } else {
-      const uint32_t rounds = ceil_div(n, 32);
+      // blocks of PART_ROUNDS rounds held in registers; the left count of the
+      // earlier blocks (run) carries over, so segments longer than one block
+      // (up to the fit's small_rows) stay with one warp
       for (uint32_t f = f_lo; f < f_hi; ++f) {
         if (seg_skips(sg, f)) continue;
         const IdxT* fin = in + (size_t)f * sg.in_fstride;
         IdxT* fout = out + (size_t)f * sg.out_fstride;
-        uint32_t rows[PART_ROUNDS];
-#pragma unroll
-        for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-          const uint32_t p = r * 32 + lane;
-          rows[r] = (r < rounds && p < n) ? (uint32_t)__ldcs(fin + p) : 0u;
-        }
         uint32_t run = 0;
+        for (uint32_t b0 = 0; b0 < n; b0 += PART_PIECE) {
+          const uint32_t rounds = min(ceil_div(n - b0, 32), PART_ROUNDS);
+          uint32_t rows[PART_ROUNDS];
 #pragma unroll
-        for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
-          if (r >= rounds) break;
-          const uint32_t p = r * 32 + lane;
-          const bool valid = p < n;
-          const bool left = valid && left_bit(sg.bits, rows[r] & sg.row_mask);
-          const unsigned lm = __ballot_sync(FULL, left);
-          const uint32_t rl = run + __popc(lm & lt);
-          const uint32_t dst = left ? rl : nl + (p - rl);
-          if (valid && dst < n) __stcs(fout + dst, (IdxT)rows[r]);
-          run += __popc(lm);
+          for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+            const uint32_t p = b0 + r * 32 + lane;
+            rows[r] = (r < rounds && p < n) ? (uint32_t)__ldcs(fin + p) : 0u;
+          }
+#pragma unroll
+          for (uint32_t r = 0; r < PART_ROUNDS; ++r) {
+            if (r >= rounds) break;
+            const uint32_t p = b0 + r * 32 + lane;
+            const bool valid = p < n;
+            const bool left = valid && left_bit(sg.bits, rows[r] & sg.row_mask);
+            const unsigned lm = __ballot_sync(FULL, left);
+            const uint32_t rl = run + __popc(lm & lt);
+            const uint32_t dst = left ? rl : nl + (p - rl);
+            if (valid && dst < n) __stcs(fout + dst, (IdxT)rows[r]);
+            run += __popc(lm);
+          }
         }
       }
     }

@@ -171,6 +171,7 @@ def _fit_group(jobs, seeds, n_estimators, max_features, tuned, profile):
     opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, int(tuned.get("subtree_cutoff", 32)),
                            int(tuned.get("scan_piece", 0)))
     opts.part_shape = int(tuned.get("part_shape", 0))
+    opts.small_rows = int(tuned.get("small_rows", 0))
     if profile:
         opts.flags |= _lib.CT_FIT_PROFILE
     ws = C.c_size_t()

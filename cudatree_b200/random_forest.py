@@ -463,6 +463,7 @@ class RandomForestClassifier:
         o.graph_samples = int(self.graph_samples)
         o.part_shape = int(t.get("part_shape", 0))
         o.huge_rows = int(t.get("huge_rows", 0))
+        o.small_rows = int(t.get("small_rows", 0))
         return o
 
     def _shape_key(self, mode):
@@ -496,6 +497,7 @@ class RandomForestClassifier:
         self._tuned = {"scan_piece": int(best.scan_piece), "subtree_cutoff": int(best.subtree_cutoff),
                        "bfs_threshold": int(best.bfs_threshold) or self.bfs_threshold,
                        "part_shape": int(best.part_shape), "huge_rows": int(best.huge_rows),
+                       "small_rows": int(best.small_rows),
                        "sample_trees": sample_trees, "sample_ms": float(ms.value)}
         tune_cache.put(self._tune_key(mode), self._tuned)
         return self._tuned

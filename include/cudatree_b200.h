@@ -130,7 +130,9 @@ typedef struct ct_fit_options {
   uint32_t huge_rows;       /* nodes of at least this many rows partition with the
                                tree's mark bits in shared memory (0 = 4096, at
                                least 4096; 0xffffffff = never)                      */
-  uint32_t reserved;        /* 0                                                    */
+  uint32_t small_rows;      /* nodes of at most this many rows partition one warp per
+                               (node, 8 features) (0 = 4096 with 16-bit lists, 512
+                               with 32-bit; else 512 .. 65536)                      */
 } ct_fit_options;
 /* ct_fit_options.part_shape: tile of a big segment's chain x ring buffers x
  * CTAs per SM of its partition.  Every shape partitions the same way. */
@@ -280,8 +282,9 @@ int ct_tree_canonicalize(const uint32_t* left, const uint32_t* right, const uint
  * option set of the given mode and returns the fastest in *best (its time in
  * *best_ms).  Every candidate grows the same trees, so the choice changes
  * speed only.  Batched, in two stages: scan piece length (1024, 2048, 4096)
- * x warp-subtree cutoff (0, 32, 128); then, around that choice, the
- * partition shape (CT_PART_*) x huge_rows (4096, 16384, never).  Plain: the
+ * x warp-subtree cutoff (0, 32, 128); then, around each choice, the
+ * partition shape (CT_PART_*) x huge_rows (4096, 16384, never), then
+ * small_rows (default, 512, 2048, 8192).  Plain: the
  * depth-first/breadth-first switch, which the reference sets with an offline
  * regression (estimate_threshold.py, random_forest.py:278-289).  The
  * workspace must hold ct_autotune_workspace_size bytes; lists and trees as

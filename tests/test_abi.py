@@ -215,9 +215,9 @@ def test_fit_rejects_bad_partition_options_before_any_launch():
     prob = _lib.Problem(fake, fake, fake, 1000, 8, 3, 4, 1, 3, 1, 1, 0)
     lists = _lib.Lists(fake, fake, fake, 1000, 4)
     trees = _lib.TreeBuffers(fake, fake, fake, fake, fake, fake, 2000)
-    for shape, huge, text in ((4, 0, "part_shape"), (0, 100, "huge_rows")):
+    for shape, huge, small, text in ((4, 0, 0, "part_shape"), (0, 100, 0, "huge_rows"), (0, 0, 100, "small_rows")):
         opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, 0, 0)
-        opts.part_shape, opts.huge_rows = shape, huge
+        opts.part_shape, opts.huge_rows, opts.small_rows = shape, huge, small
         st = lib.ct_fit(C.byref(prob), C.byref(lists), 0, 4, C.byref(opts), C.byref(trees), C.c_void_p(fake), 0,
                         None)
         assert st == 1 and text in _lib.last_error()

@@ -179,6 +179,7 @@ def test_autotune_keeps_the_trees(cuda_device):
     assert tuned._tuned is not None and tuned._tuned["scan_piece"] in (1024, 2048, 4096)
     assert tuned._tuned["subtree_cutoff"] in (0, 32, 128)
     assert tuned._tuned["part_shape"] in range(4) and tuned._tuned["huge_rows"] in (0, 16384, 0xFFFFFFFF)
+    assert tuned._tuned["small_rows"] in (0, 512, 2048, 8192)
     # a later forest of the same shape takes the stored choice (the tune cache)
     again = RandomForestClassifier(n_estimators=6, seed=5, autotune=True).fit(x, y)
     assert again._tuned == tuned._tuned
@@ -367,19 +368,20 @@ def test_constant_feature_masks_beyond_64_features_match_oracle(cuda_device, f):
 
 @pytest.mark.parametrize("n,f,c", [(70000, 6, 5), (30000, 7, 3)])
 def test_partition_shapes_grow_the_same_trees(cuda_device, n, f, c):
-    """Every partition shape (CT_PART_*) and huge-segment threshold the
-    autotuner picks among grows the same trees: 70,000 rows take 32-bit
-    entries, 30,000 rows 16-bit ones."""
+    """Every partition shape (CT_PART_*), huge-segment threshold and
+    small-segment cutoff the autotuner picks among grows the same trees:
+    70,000 rows take 32-bit entries, 30,000 rows 16-bit ones."""
     x, y = _synthetic(n, f, c, 61)
     ref = RandomForestClassifier(n_estimators=3, seed=61).fit(x, y)
-    for shape in range(4):
-        for huge in (0, 16384, 0xFFFFFFFF):
-            g = RandomForestClassifier(n_estimators=3, seed=61)
-            g._tuned = {"part_shape": shape, "huge_rows": huge}
-            g.fit(x, y)
-            for a, b in zip(g._trees, ref._trees):
-                np.testing.assert_array_equal(a.left_children, b.left_children)
-                np.testing.assert_array_equal(a.feature_idx_array, b.feature_idx_array)
-                np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
-                np.testing.assert_array_equal(a.values_array, b.values_array)
+    options = [(s, h, 0) for s in range(4) for h in (0, 16384, 0xFFFFFFFF)]
+    options += [(0, 0, 1024), (1, 16384, 2048), (2, 0, 4096), (0, 0xFFFFFFFF, 65536)]
+    for shape, huge, small in options:
+        g = RandomForestClassifier(n_estimators=3, seed=61)
+        g._tuned = {"part_shape": shape, "huge_rows": huge, "small_rows": small}
+        g.fit(x, y)
+        for a, b in zip(g._trees, ref._trees):
+            np.testing.assert_array_equal(a.left_children, b.left_children)
+            np.testing.assert_array_equal(a.feature_idx_array, b.feature_idx_array)
+            np.testing.assert_array_equal(a.feature_threshold_array, b.feature_threshold_array)
+            np.testing.assert_array_equal(a.values_array, b.values_array)
     _assert_same_trees(ref._trees, O.fit_forest(x, y, n_estimators=3, seed=61).trees)
