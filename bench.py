@@ -260,7 +260,7 @@ def run_configs(args):
         "sklearn_fit_s": sk, "sklearn_cores": cores}
     n_jobs = args.queue_jobs
     jobs = [synthetic.blob_job(j) for j in range(n_jobs)]
-    fit_forests(jobs[:4], n_estimators=10, seeds=range(4))  # warm-up
+    fit_forests(jobs, n_estimators=10, seeds=range(n_jobs))  # warm-up: library, graphs and device buffers
     t0 = time.perf_counter()
     forests = fit_forests(jobs, n_estimators=10, seeds=range(n_jobs))
     q_s = time.perf_counter() - t0

@@ -27,8 +27,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .random_forest import (PAD_BYTES, RandomForestClassifier, _dev_bytes, _device, _ptr, _stream, best_index_bytes,
-                            compact_labels, fetch_tree_columns)
+from .random_forest import (PAD_BYTES, RandomForestClassifier, _device, _stream, best_index_bytes, compact_labels,
+                            fetch_tree_columns)
 
 
 def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, group_bytes=None, fit_options=None,
@@ -77,17 +77,31 @@ def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, group_byte
             groups.append(sorted(cur))
     forests = [None] * len(jobs)
     dev = _device()
+    plans = [_GroupPlan([jobs[i] for i in g], fit_options or {}, profile) for g in groups]
+    # waves of `streams` groups; a wave's buffers are one allocation (a queue
+    # of the same shape later reuses it from the caching allocator)
+    for w0 in range(0, len(groups), streams):
+        wave = list(range(w0, min(w0 + streams, len(groups))))
+        offs, total = {}, 0
+        for k in wave:
+            offs[k] = total
+            total += (plans[k].size + 255) & ~255
+        arena = torch.empty(total, dtype=torch.uint8, device=dev)
+        torch.cuda.current_stream(dev).synchronize()  # the allocation is ready for the groups' streams
 
-    def run(g):
-        st = torch.cuda.Stream(dev)
-        with torch.cuda.stream(st):
-            res = _fit_group([jobs[i] for i in g], [seeds[i] for i in g], n_estimators, max_features,
-                             fit_options or {}, profile)
-        for i, f in zip(g, res):
-            forests[i] = f
+        def run(k):
+            g = groups[k]
+            st = torch.cuda.Stream(dev)
+            with torch.cuda.stream(st):
+                res = _fit_group([jobs[i] for i in g], [seeds[i] for i in g], n_estimators, max_features, plans[k],
+                                 arena, offs[k])
+            st.synchronize()
+            for i, f in zip(g, res):
+                forests[i] = f
 
-    with ThreadPoolExecutor(max_workers=streams) as ex:
-        list(ex.map(run, groups))
+        with ThreadPoolExecutor(max_workers=len(wave)) as ex:
+            list(ex.map(run, wave))
+        del arena
     return forests
 
 
@@ -135,54 +149,78 @@ class _Arena:
         return off
 
 
-def _fit_group(jobs, seeds, n_estimators, max_features, tuned, profile):
+class _GroupPlan:
+    """Offsets of one group's device buffers inside the queue's allocation:
+    per job its row-major upload, feature-major samples, labels, presort,
+    index lists and marks; NaN flags, the presort workspace, the raw trees
+    and the fit's workspace."""
+
+    def __init__(self, jobs, tuned, profile):
+        ar = _Arena()
+        self.lay = []
+        for j in jobs:
+            self.lay.append({"x_rm": ar.take(4 * j.n * j.f), "x_fm": ar.take(4 * j.n * j.f),
+                             "lab": ar.take(j.labels.nbytes), "pre": ar.take(j.f * j.n * j.index_bytes),
+                             "si0": ar.take(j.trees * j.f * j.n * j.index_bytes),
+                             "si1": ar.take(j.trees * j.f * j.n * j.index_bytes),
+                             "mark": ar.take(_lib.mark_bytes(j.n, j.trees))})
+        self.nan = ar.take(4 * len(jobs))
+        self.pws = ar.take(max(_presort_ws(j) for j in jobs))
+        self.total = sum(j.trees for j in jobs)
+        self.cap = 2 * max(j.n for j in jobs)
+        self.raw = [ar.take(4 * self.total * self.cap) for _ in range(5)]
+        self.n_nodes = ar.take(4 * self.total)
+        self.opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, int(tuned.get("subtree_cutoff", 32)),
+                                    int(tuned.get("scan_piece", 0)))
+        self.opts.part_shape = int(tuned.get("part_shape", 0))
+        self.opts.small_rows = int(tuned.get("small_rows", 0))
+        if profile:
+            self.opts.flags |= _lib.CT_FIT_PROFILE
+        self.arr = (_lib.FitJob * len(jobs))()
+        for k, j in enumerate(jobs):  # sizes only: the workspace query reads no pointer
+            self.arr[k].problem = _lib.Problem(None, None, None, j.n, j.f, j.c, j.index_bytes, j.label_bytes, j.m,
+                                               1, 1, 0)
+            self.arr[k].lists = _lib.Lists(None, None, None, j.n, j.trees)
+            self.arr[k].n_trees = j.trees
+        ws = C.c_size_t()
+        _lib.call("ct_fit_queue_workspace_size", self.arr, len(jobs), C.byref(self.opts), C.byref(ws))
+        self.ws_bytes = ws.value
+        self.work = ar.take(ws.value)
+        self.size = ar.size
+
+
+def _fit_group(jobs, seeds, n_estimators, max_features, plan, arena, off):
+    """One group's shared fit in arena[off:off + plan.size], on the current
+    stream; returns its forests."""
     dev = _device()
-    ar = _Arena()
-    lay = []
-    for j in jobs:
-        lay.append({"x_rm": ar.take(4 * j.n * j.f), "x_fm": ar.take(4 * j.n * j.f), "lab": ar.take(j.labels.nbytes),
-                    "pre": ar.take(j.f * j.n * j.index_bytes), "si0": ar.take(j.trees * j.f * j.n * j.index_bytes),
-                    "si1": ar.take(j.trees * j.f * j.n * j.index_bytes), "mark": ar.take(_lib.mark_bytes(j.n, j.trees))})
-    nan_off = ar.take(4 * len(jobs))
-    pws_off = ar.take(max(_presort_ws(j) for j in jobs))
-    arena = torch.empty(ar.size, dtype=torch.uint8, device=dev)
-    base = arena.data_ptr()
-    arena[nan_off:nan_off + 4 * len(jobs)].zero_()
+    mem = arena[off:off + plan.size]
+    base = mem.data_ptr()
+    lay = plan.lay
+    mem[plan.nan:plan.nan + 4 * len(jobs)].zero_()
+    mem[plan.n_nodes:plan.n_nodes + 4 * plan.total].zero_()
     # samples and labels to the device (pageable copies, ordered on this stream)
     for j, l in zip(jobs, lay):
-        arena[l["x_rm"]:l["x_rm"] + 4 * j.n * j.f].copy_(torch.from_numpy(j.x.view(np.uint8).reshape(-1)))
-        arena[l["lab"]:l["lab"] + j.labels.nbytes].copy_(torch.from_numpy(j.labels.view(np.uint8)))
+        mem[l["x_rm"]:l["x_rm"] + 4 * j.n * j.f].copy_(torch.from_numpy(j.x.view(np.uint8).reshape(-1)))
+        mem[l["lab"]:l["lab"] + j.labels.nbytes].copy_(torch.from_numpy(j.labels.view(np.uint8)))
     st = _stream()
-    arr = (_lib.FitJob * len(jobs))()
+    arr = plan.arr
     for k, (j, l) in enumerate(zip(jobs, lay)):
-        _lib.call("ct_transpose_rows", base + l["x_rm"], j.n, j.f, base + l["x_fm"], base + nan_off + 4 * k, st)
-        _lib.call("ct_presort", base + l["x_fm"], j.n, j.f, j.index_bytes, base + l["pre"], base + pws_off,
+        _lib.call("ct_transpose_rows", base + l["x_rm"], j.n, j.f, base + l["x_fm"], base + plan.nan + 4 * k, st)
+        _lib.call("ct_presort", base + l["x_fm"], j.n, j.f, j.index_bytes, base + l["pre"], base + plan.pws,
                   _presort_ws(j), st)
         arr[k].problem = _lib.Problem(base + l["x_fm"], base + l["lab"], base + l["pre"], j.n, j.f, j.c,
                                       j.index_bytes, j.label_bytes, j.m, 1, 1, int(seeds[k]))
         arr[k].lists = _lib.Lists(base + l["si0"], base + l["si1"], base + l["mark"], j.n, j.trees)
         arr[k].n_trees = j.trees
         arr[k].first_tree = 0
-    total = sum(j.trees for j in jobs)
-    cap = 2 * max(j.n for j in jobs)
-    raw = torch.empty((5, total * cap), dtype=torch.int32, device=dev)
-    n_nodes = torch.zeros(total, dtype=torch.int32, device=dev)
-    tb = _lib.TreeBuffers(*[raw[i].data_ptr() for i in range(5)], _ptr(n_nodes), cap)
-    opts = _lib.FitOptions(_lib.CT_FIT_BATCHED, 0, int(tuned.get("subtree_cutoff", 32)),
-                           int(tuned.get("scan_piece", 0)))
-    opts.part_shape = int(tuned.get("part_shape", 0))
-    opts.small_rows = int(tuned.get("small_rows", 0))
-    if profile:
-        opts.flags |= _lib.CT_FIT_PROFILE
-    ws = C.c_size_t()
-    _lib.call("ct_fit_queue_workspace_size", arr, len(jobs), C.byref(opts), C.byref(ws))
-    work = _dev_bytes(ws.value, dev)
-    _lib.call("ct_fit_queue", arr, len(jobs), C.byref(opts), C.byref(tb), _ptr(work), ws.value, st)
+    n_nodes = mem[plan.n_nodes:plan.n_nodes + 4 * plan.total].view(torch.int32)
+    tb = _lib.TreeBuffers(*[base + r for r in plan.raw], n_nodes.data_ptr(), plan.cap)
+    _lib.call("ct_fit_queue", arr, len(jobs), C.byref(plan.opts), C.byref(tb), base + plan.work, plan.ws_bytes, st)
     stats = _lib.fit_stats()
-    nan = arena[nan_off:nan_off + 4 * len(jobs)].view(torch.int32).cpu().numpy()
+    nan = mem[plan.nan:plan.nan + 4 * len(jobs)].view(torch.int32).cpu().numpy()
     if nan.any():
         raise ValueError(f"samples of job {int(np.flatnonzero(nan)[0])} of the group contain NaN")
-    counts, cols = fetch_tree_columns(tb, n_nodes, total, dev)
+    counts, cols = fetch_tree_columns(tb, n_nodes, plan.total, dev)
     out, o, t = [], 0, 0
     for j, seed in zip(jobs, seeds):
         f = RandomForestClassifier(n_estimators, max_features=max_features, seed=seed)
