@@ -65,14 +65,16 @@ def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, group_byte
     for members in widths.values():
         total = sum(jobs[i].device_bytes for i in members)
         k = max(min(streams, len(members)), -(-total // budget))
-        share = -(-total // k)
-        cur, used = [], 0
+        # cut where the running bytes pass each k-th of the total, so exactly k
+        # groups of similar bytes come out (each within the budget when k
+        # came from it)
+        cur, used, cut = [], 0, 1
         for i in sorted(members, key=lambda i: (jobs[i].c, jobs[i].f)):
-            if cur and (used + jobs[i].device_bytes > share or used + jobs[i].device_bytes > budget):
-                groups.append(sorted(cur))
-                cur, used = [], 0
             cur.append(i)
             used += jobs[i].device_bytes
+            if cut < k and used * k >= cut * total:
+                groups.append(sorted(cur))
+                cur, cut = [], cut + 1
         if cur:
             groups.append(sorted(cur))
     forests = [None] * len(jobs)
@@ -94,7 +96,7 @@ def fit_forests(jobs, n_estimators=10, max_features=None, seeds=None, group_byte
             st = torch.cuda.Stream(dev)
             with torch.cuda.stream(st):
                 res = _fit_group([jobs[i] for i in g], [seeds[i] for i in g], n_estimators, max_features, plans[k],
-                                 arena, offs[k])
+                                 arena, offs[k], k - w0)
             st.synchronize()
             for i, f in zip(g, res):
                 forests[i] = f
@@ -189,19 +191,38 @@ class _GroupPlan:
         self.size = ar.size
 
 
-def _fit_group(jobs, seeds, n_estimators, max_features, plan, arena, off):
+_PINNED = {}  # page-locked upload staging per group slot, kept across calls (grow only)
+
+
+def _staging(slot: int, nbytes: int) -> torch.Tensor:
+    buf = _PINNED.get(slot)
+    if buf is None or buf.numel() < nbytes:
+        buf = torch.empty(max(nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        _PINNED[slot] = buf
+    return buf
+
+
+def _fit_group(jobs, seeds, n_estimators, max_features, plan, arena, off, slot):
     """One group's shared fit in arena[off:off + plan.size], on the current
-    stream; returns its forests."""
+    stream; returns its forests.  slot: the group's page-locked staging."""
     dev = _device()
     mem = arena[off:off + plan.size]
     base = mem.data_ptr()
     lay = plan.lay
     mem[plan.nan:plan.nan + 4 * len(jobs)].zero_()
     mem[plan.n_nodes:plan.n_nodes + 4 * plan.total].zero_()
-    # samples and labels to the device (pageable copies, ordered on this stream)
-    for j, l in zip(jobs, lay):
-        mem[l["x_rm"]:l["x_rm"] + 4 * j.n * j.f].copy_(torch.from_numpy(j.x.view(np.uint8).reshape(-1)))
-        mem[l["lab"]:l["lab"] + j.labels.nbytes].copy_(torch.from_numpy(j.labels.view(np.uint8)))
+    # samples and labels to the device: each job is copied into the group's
+    # page-locked staging (host) and from there asynchronously on this
+    # stream, so the host copy of the next job overlaps this one's transfer
+    up = [(j.x.view(np.uint8).reshape(-1), l["x_rm"]) for j, l in zip(jobs, lay)]
+    up += [(j.labels.view(np.uint8), l["lab"]) for j, l in zip(jobs, lay)]
+    stage = _staging(slot, sum(a.nbytes for a, _ in up))
+    host = stage.numpy()
+    o = 0
+    for a, dst in up:
+        host[o:o + a.nbytes] = a
+        mem[dst:dst + a.nbytes].copy_(stage[o:o + a.nbytes], non_blocking=True)
+        o += a.nbytes
     st = _stream()
     arr = plan.arr
     for k, (j, l) in enumerate(zip(jobs, lay)):
