@@ -112,10 +112,12 @@ def compact_labels(y):
     if y.dtype.kind in "iu" and y.size:
         lo, hi = int(y.min()), int(y.max())
         if hi - lo < (1 << 22) and -(1 << 62) < lo and hi < (1 << 62):
-            off = y.astype(np.int64) - lo
+            off = y if lo == 0 else y.astype(np.int64) - lo
             present = np.bincount(off, minlength=hi - lo + 1) > 0
             table = (np.flatnonzero(present) + lo).astype(y.dtype)
-            lut = np.cumsum(present, dtype=np.int64) - 1
+            # ids in the narrowest unsigned type (the label width of the fit)
+            dt = np.uint8 if table.size <= 0x100 else np.uint16 if table.size <= 0x10000 else np.int64
+            lut = (np.cumsum(present, dtype=np.int64) - 1).astype(dt)
             return table, lut[off]
     return np.unique(y, return_inverse=True)
 
