@@ -326,9 +326,12 @@ int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView&
     const LevelBounds b{cn, total};
     if (L.subtree_cut && L.small_bound + 2ull * cn > L.cap_small) CT_TRY(flush_subtrees(p, v, L, tv, st));
     CT_TRY(launch_reset_step(L.s, cn, step_lists(L, cur, lo, C), st));
-    CT_TRY(launch_split(v, ib, lb, L.s, b, L.scan_piece, false, st));
+    // Persistent split and children launches (at most the resident blocks):
+    // their grids would otherwise be sized by the capacity bounds, most of
+    // whose warps find no item.  The mark fill keeps one warp per piece.
+    CT_TRY(launch_split(v, ib, lb, L.s, b, L.scan_piece, true, st));
     CT_TRY(launch_partition(v, ib, lb, L.s, b, tv, false, st));
-    CT_TRY(launch_children(v, ib, lb, L.s, b, tv, L.cap_list, L.subtree_cut, L.small, L.cap_small, false, st));
+    CT_TRY(launch_children(v, ib, lb, L.s, b, tv, L.cap_list, L.subtree_cut, L.small, L.cap_small, true, st));
     if (L.subtree_cut) L.small_bound += 2ull * cn;
   }
   return CT_OK;

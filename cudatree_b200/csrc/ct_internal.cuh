@@ -103,6 +103,7 @@ struct Counters {
   uint32_t n_hchains;     // their chains (quads)
   uint32_t ticket_huge;   // k_part_seg's unit counter
   uint32_t n_bchains;     // active chains of k_part_big's segments
+  uint32_t n_tv;          // scan pieces of two-valued features
   uint32_t claim[16];     // item counters of persistent launches (ITEM_* slots)
   unsigned long long next_total;
   unsigned long long small_total;
@@ -132,6 +133,7 @@ __device__ __forceinline__ void reset_step_counters(Counters* c, uint32_t n_node
   c->n_nodes = n_nodes;
   c->n_scan_pieces = 0;
   c->n_carry = 0;
+  c->n_tv = 0;
   c->n_splits = 0;
   c->n_part_pieces = 0;
   c->n_status = 0;
@@ -359,6 +361,8 @@ struct LevelScratch {
   uint32_t* piece_cnt;    // [cap_nodes]
   ScanPiece* pieces;      // [cap_scan]
   uint32_t* carry;        // [cap_carry][n_classes]
+  uint32_t* carry_piece;  // [cap_carry] the scan piece of each carry row (pieces of multi-piece segments)
+  uint32_t* tv_pieces;    // [cap_scan] the scan pieces of two-valued features
   PieceBest* best;        // [cap_scan]
   ct_split_result* result;// [cap_nodes]
   SplitRec* splits;       // [cap_nodes]

@@ -223,22 +223,40 @@ __device__ __forceinline__ void select_item(const View& vb, const StepLists& lis
   npieces = __shfl_sync(FULL, npieces, 0);
   base = __shfl_sync(FULL, base, 0);
   cbase = __shfl_sync(FULL, cbase, 0);
-  for (uint32_t q = lane; q < npieces; q += 32) {
-    ScanPiece pc;
-    pc.node = w;
-    const uint32_t k = q / pps;  // k-th materialized slot
-    pc.slot = k;
-    if (vsel) {
-      uint32_t slot = 0;
-      for (uint32_t left = k;; ++slot)
-        if (!((vsel >> slot) & 1ull) && left-- == 0) break;
-      pc.slot = slot;
+  __syncwarp();  // the slots' features in s.sel, written by other lanes
+  // Besides the piece records, the piece of every carry row (k_scan_hist and
+  // k_scan_carry walk only the pieces of multi-piece segments) and the list
+  // of two-valued features' pieces (k_scan_two_valued walks only those), so
+  // that those kernels claim no item they have nothing to do for.
+  for (uint32_t q0 = 0; q0 < npieces; q0 += 32) {
+    const uint32_t q = q0 + lane;
+    bool tv = false;
+    if (q < npieces) {
+      ScanPiece pc;
+      pc.node = w;
+      const uint32_t k = q / pps;  // k-th materialized slot
+      pc.slot = k;
+      if (vsel) {
+        uint32_t slot = 0;
+        for (uint32_t left = k;; ++slot)
+          if (!((vsel >> slot) & 1ull) && left-- == 0) break;
+        pc.slot = slot;
+      }
+      pc.j = q - k * pps;
+      pc.npieces = pps;
+      pc.carry = cbase + q;
+      pc.pad[0] = pc.pad[1] = pc.pad[2] = 0;
+      s.pieces[base + q] = pc;
+      if (pps > 1) s.carry_piece[cbase + q] = base + q;
+      tv = two_valued(v, s.sel[(size_t)w * v.sel_stride + pc.slot]);
     }
-    pc.j = q - k * pps;
-    pc.npieces = pps;
-    pc.carry = cbase + q;
-    pc.pad[0] = pc.pad[1] = pc.pad[2] = 0;
-    s.pieces[base + q] = pc;
+    const unsigned tm = __ballot_sync(FULL, tv);
+    if (tm) {  // n_tv <= n_scan_pieces <= cap_scan
+      uint32_t tb = 0;
+      if (lane == 0) tb = atomicAdd(&s.ctr->n_tv, (uint32_t)__popc(tm));
+      tb = __shfl_sync(FULL, tb, 0);
+      if (tv) s.tv_pieces[tb + __popc(tm & lanemask_lt())] = base + q;
+    }
   }
 }
 
@@ -312,10 +330,10 @@ template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_hist(View v, LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
-  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  const uint32_t count = live_count(s, s.ctr->n_carry, s.cap_carry);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_HIST],
-            [&](uint32_t pi) { scan_hist_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t i) { scan_hist_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, s.carry_piece[i]); });
 }
 
 __device__ __forceinline__ void scan_carry_item(const LevelScratch& s, uint32_t C, uint32_t pi) {
@@ -337,8 +355,8 @@ __device__ __forceinline__ void scan_carry_item(const LevelScratch& s, uint32_t 
 }
 
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_carry(LevelScratch s, uint32_t C) {
-  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
-  for_items(count, &s.ctr->claim[ITEM_CARRY], [&](uint32_t pi) { scan_carry_item(s, C, pi); });
+  const uint32_t count = live_count(s, s.ctr->n_carry, s.cap_carry);
+  for_items(count, &s.ctr->claim[ITEM_CARRY], [&](uint32_t i) { scan_carry_item(s, C, s.carry_piece[i]); });
 }
 
 // ------------------------------------------------------------------------
@@ -441,10 +459,10 @@ template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_two_valued(View v, LevelScratch s, uint32_t scan_piece) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
-  const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
+  const uint32_t count = live_count(s, s.ctr->n_tv, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_TWO_VALUED],
-            [&](uint32_t pi) { two_valued_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t i) { two_valued_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, s.tv_pieces[i]); });
 }
 
 // ------------------------------------------------------------------------
@@ -1576,9 +1594,9 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
   pf->end();
   pf->launched(CT_K_SELECT);
   pf->begin(CT_K_SCAN);
-  k_scan_hist<IdxT, LabT, Q><<<grid_for(k_scan_hist<IdxT, LabT, Q>, caps.scan, sm1, persistent), THREADS_PER_BLOCK, sm1,
-                            st>>>(v, s, scan_piece);
-  k_scan_carry<<<grid_for(k_scan_carry, caps.scan, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
+  k_scan_hist<IdxT, LabT, Q><<<grid_for(k_scan_hist<IdxT, LabT, Q>, caps.carry, sm1, persistent), THREADS_PER_BLOCK,
+                            sm1, st>>>(v, s, scan_piece);
+  k_scan_carry<<<grid_for(k_scan_carry, caps.carry, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
   k_split_scan<IdxT, LabT, Q><<<grid_for(k_split_scan<IdxT, LabT, Q>, caps.scan, 2 * sm1, persistent), THREADS_PER_BLOCK,
                              2 * sm1, st>>>(v, s, scan_piece);
   if (v.fbin)
@@ -1658,6 +1676,8 @@ static size_t carve_or_size(Arena& a, const View& v, const LevelCaps& c, LevelSc
   t.piece_cnt = a.take<uint32_t>(c.nodes);
   t.pieces = a.take<ScanPiece>(c.scan);
   t.carry = a.take<uint32_t>((size_t)c.carry * C);
+  t.carry_piece = a.take<uint32_t>(c.carry);
+  t.tv_pieces = a.take<uint32_t>(c.scan);
   t.best = a.take<PieceBest>(c.scan);
   t.result = a.take<ct_split_result>(c.nodes);
   t.splits = a.take<SplitRec>(c.nodes);
