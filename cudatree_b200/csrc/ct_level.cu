@@ -135,11 +135,27 @@ __device__ __forceinline__ void vcount_item(const View& v, const StepLists& list
   const uint32_t hi = min(lo + VPIECE, nd.n);
   for (uint32_t i = lane; i < fc; i += 32) cnt[i] = 0;
   __syncwarp();
-  for (uint32_t i = lo + lane; i < hi; i += 32) {
-    const uint32_t e = (uint32_t)__ldcs(rl + i);
-    const uint32_t lab = entry_label<LabT>(v, e);
-    for (uint64_t b = __ldg(v.vrow + entry_row(v, e)); b; b &= b - 1)
-      atomicAdd(&cnt[((uint32_t)__ffsll((long long)b) - 1) * C + lab], 1u);
+  // VB rows per lane: their entry loads, then their value-bit gathers, are in
+  // flight together (one row at a time left the loop waiting on two loads)
+  constexpr uint32_t VB = 8;
+  for (uint32_t i0 = lo; i0 < hi; i0 += 32 * VB) {
+    uint32_t e[VB];
+    uint64_t bits[VB];
+#pragma unroll
+    for (uint32_t r = 0; r < VB; ++r) {
+      const uint32_t i = i0 + r * 32 + lane;
+      e[r] = i < hi ? (uint32_t)__ldcs(rl + i) : 0u;
+    }
+#pragma unroll
+    for (uint32_t r = 0; r < VB; ++r)
+      bits[r] = i0 + r * 32 + lane < hi ? __ldg(v.vrow + entry_row(v, e[r])) : 0ull;
+#pragma unroll
+    for (uint32_t r = 0; r < VB; ++r) {
+      if (!bits[r]) continue;
+      const uint32_t lab = entry_label<LabT>(v, e[r]);
+      for (uint64_t b = bits[r]; b; b &= b - 1)
+        atomicAdd(&cnt[((uint32_t)__ffsll((long long)b) - 1) * C + lab], 1u);
+    }
   }
   __syncwarp();
   if (lane == 0) atomicAdd(&s.ctr->vrows, (unsigned long long)(hi - lo));
@@ -907,7 +923,7 @@ __device__ __forceinline__ void fill_mark_item(const View& vb, const StepLists& 
       const uint32_t row = entry_row(v, rows[r]);
       const bool left = virt ? !((__ldg(v.vrow + row) >> sr.feature) & 1ull) : p <= sr.pos;
       if (left) atomicOr(bw + (row >> 5), 1u << (row & 31));
-      else atomicAnd(bw + (row >> 5), ~(1u << (row & 31)));
+      else if (Q) atomicAnd(bw + (row >> 5), ~(1u << (row & 31)));
       if (left) cls[r] = entry_label<LabT>(v, rows[r]);
     }
   }
@@ -1762,6 +1778,7 @@ int launch_partition_q(const View& v, uint32_t ib, uint32_t lb, const LevelScrat
   LevelCaps caps = level_caps(v, DEFAULT_SCAN_PIECE, b);
   caps.part = min(caps.part, s.cap_part);
   caps.status = min(caps.status, s.cap_status);
+  if (!Q && v.bits) CT_CUDA_TRY(cudaMemsetAsync(v.bits, 0, (size_t)v.n_slots * v.bit_words * sizeof(uint32_t), st));
 #define CALL(I, L) partition_impl<I, L, Q>(v, s, caps, tv, persistent, st)
   CT_DISPATCH(ib, lb, CALL);
 #undef CALL
