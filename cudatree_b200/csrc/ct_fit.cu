@@ -30,7 +30,9 @@ int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident,
 namespace {
 
 constexpr uint32_t CHUNK_NODES_MAX = 1u << 20;
-constexpr uint64_t DEFAULT_GRAPH_SAMPLES = 1u << 22;
+// every level in the loop graph: its launches are persistent like the host
+// loop's, so a larger level gains nothing from the host's round trip
+constexpr uint64_t DEFAULT_GRAPH_SAMPLES = UINT64_MAX;
 
 // Class histogram of every slot's in-bag rows: grid (blocks, slots), one
 // shared-memory histogram per block flushed with global atomics.
@@ -708,9 +710,8 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
   CT_TRY(root(p, v, L, 0, n_trees, first_tree, tv, 0, st));
   Counters h;
   if (!current_prof()->timing && !L.host_loop) {
-    // Levels holding more than graph_samples samples run from the host (their
-    // kernels dwarf a round trip; one warp per item); the rest, and the
-    // subtrees, run as the loop graph.
+    // Levels holding more than graph_samples samples run from the host (one
+    // round trip each); the rest, and the subtrees, run as the loop graph.
     uint32_t n = 0;
     uint64_t total = 0;
     if (L.graph_samples != UINT64_MAX) {

@@ -214,7 +214,7 @@ class RandomForestClassifier:
         # node and a value bit per row stand for them); False keeps them all
         self.virtual_features = True
         # batched form: levels of at most this many samples run in the loop
-        # graph (0: 2^22; 0xffffffff: all of them)
+        # graph, larger ones from the host (0 or 0xffffffff: all of them)
         self.graph_samples = 0
 
     # ------------------------------------------------------------ pickling

@@ -124,7 +124,7 @@ typedef struct ct_fit_options {
   uint32_t step_nodes;      /* nodes per level step (0 = 2^20): a wider level takes
                                several steps; the workspace grows with it           */
   uint32_t graph_samples;   /* batched: levels of at most this many samples run in
-                               the loop graph, larger ones from the host (0 = 2^22,
+                               the loop graph, larger ones from the host (0 or
                                0xffffffff = every level in the graph)               */
   uint32_t part_shape;      /* partition of big segments: CT_PART_* (0 = default)   */
   uint32_t huge_rows;       /* nodes of at least this many rows partition with the
