@@ -16,6 +16,8 @@
 // tree, with one block per feature.
 #include <algorithm>
 
+#include <cstring>
+
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -76,7 +78,15 @@ struct BootMulti {
   uint32_t segs;          // items per feature
   uint32_t stride;
   uint32_t row_mask;
+  // Lists written: n_lists of the n_features, list_feat[k] the k-th when
+  // n_lists < n_features (a fit's virtual features keep no list), else all.
+  // Items run over the written lists only.
+  uint32_t n_lists;
+  uint8_t list_feat[64];
 };
+__device__ __forceinline__ uint32_t list_feature(const BootMulti& b, uint32_t k) {
+  return b.n_lists < b.n_features ? b.list_feat[k] : k;
+}
 
 // Loads a round's entries and their rows' in-bag words.
 template <typename IdxT>
@@ -93,10 +103,11 @@ __device__ __forceinline__ void boot_round(const BootMulti& b, const IdxT* in, u
 template <typename IdxT>
 __global__ void __launch_bounds__(BOOT_WARPS * 32) k_boot_count(BootMulti b) {
   const uint32_t lane = lane_id();
-  const uint64_t items = (uint64_t)b.n_features * b.segs;
+  const uint64_t items = (uint64_t)b.n_lists * b.segs;
   const uint64_t nw = (uint64_t)gridDim.x * BOOT_WARPS;
   for (uint64_t it = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; it < items; it += nw) {
-    const uint32_t f = (uint32_t)(it / b.segs), j = (uint32_t)(it - (uint64_t)f * b.segs);
+    const uint32_t k = (uint32_t)(it / b.segs), j = (uint32_t)(it - (uint64_t)k * b.segs);
+    const uint32_t f = list_feature(b, k);
     const IdxT* in = reinterpret_cast<const IdxT*>(b.src) + (size_t)f * b.n_rows;
     const uint32_t lo = j * BOOT_SEG, hi = min(lo + BOOT_SEG, b.n_rows);
     uint32_t cnt[BOOT_MAXW];
@@ -127,7 +138,7 @@ __global__ void __launch_bounds__(BOOT_WARPS * 32) k_boot_count(BootMulti b) {
 
 // Pass 2: per (feature, slot), exclusive prefix of the items' counts.
 __global__ void k_boot_offsets(BootMulti b) {
-  const uint64_t total = (uint64_t)b.n_features * b.n_slots;
+  const uint64_t total = (uint64_t)b.n_lists * b.n_slots;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t f = (uint32_t)(i / b.n_slots), t = (uint32_t)(i - (uint64_t)f * b.n_slots);
     uint32_t* c = b.counts + (size_t)f * b.segs * b.n_slots + t;
@@ -150,9 +161,10 @@ __global__ void __launch_bounds__(BOOT_WARPS * 32) k_boot_write(BootMulti b) {
   __shared__ uint32_t s_carry[32 * BOOT_MAXW];
   const uint32_t warp = threadIdx.x >> 5, lane = lane_id();
   const unsigned lt = lanemask_lt();
-  const uint64_t items = (uint64_t)b.n_features * b.segs;
+  const uint64_t items = (uint64_t)b.n_lists * b.segs;
   for (uint64_t it = blockIdx.x; it < items; it += gridDim.x) {
-    const uint32_t f = (uint32_t)(it / b.segs), j = (uint32_t)(it - (uint64_t)f * b.segs);
+    const uint32_t k = (uint32_t)(it / b.segs), j = (uint32_t)(it - (uint64_t)k * b.segs);
+    const uint32_t f = list_feature(b, k);
     const IdxT* in = reinterpret_cast<const IdxT*>(b.src) + (size_t)f * b.n_rows;
     IdxT* out0 = reinterpret_cast<IdxT*>(b.out) + (size_t)f * b.stride;
     const uint32_t lo = j * BOOT_SEG, hi = min(lo + BOOT_SEG, b.n_rows);
@@ -255,10 +267,12 @@ size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_
 
 // Compacts slots [slot_lo, slot_lo + n_slots) for trees tree_lo...  src is the
 // [F][N] presort, or its packed copy (entries row | label << s, row ids under
-// row_mask).  The workspace's word [1] is an error word that the caller zeroes
-// once and reads after; nothing here waits, so it stays zero.
+// row_mask).  Bit f of skip (features below 64): feature f's lists are not
+// written (a fit's virtual features other than the row-list slot: nothing
+// reads them).  The workspace's word [1] is an error word that the caller
+// zeroes once and reads after; nothing here waits, so it stays zero.
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
-                   const void* src, uint32_t row_mask, uint32_t* n_in_dev, void* ws, size_t wsb,
+                   const void* src, uint32_t row_mask, uint64_t skip, uint32_t* n_in_dev, void* ws, size_t wsb,
                    cudaStream_t st) {
   const uint32_t N = p->n_rows, F = p->n_features;
   CT_ARG_CHECK(n_slots >= 1 && slot_lo + n_slots <= l->n_slots, "slot out of range");
@@ -290,7 +304,15 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const uint32_t segs = ceil_div(N, BOOT_SEG);
-  const uint64_t items = (uint64_t)F * segs;
+  uint32_t n_lists = 0;
+  uint8_t list_feat[64] = {};
+  if (skip && F <= 64) {
+    for (uint32_t f = 0; f < F; ++f)
+      if (!((skip >> f) & 1ull)) list_feat[n_lists++] = (uint8_t)f;
+  } else {
+    n_lists = F;
+  }
+  const uint64_t items = (uint64_t)n_lists * segs;
   for (uint32_t s0 = 0; s0 < n_slots; s0 += 32 * BOOT_MAXW) {  // at most 128 slots per pass
     const uint32_t ns = std::min<uint32_t>(n_slots - s0, 32 * BOOT_MAXW);
     const uint32_t words = ceil_div(ns, 32u);
@@ -310,8 +332,10 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
     b.segs = segs;
     b.stride = l->stride;
     b.row_mask = row_mask;
+    b.n_lists = n_lists;
+    std::memcpy(b.list_feat, list_feat, sizeof(list_feat));
     const uint32_t cblocks = (uint32_t)std::min<uint64_t>((items + BOOT_WARPS - 1) / BOOT_WARPS, (uint64_t)sms * 8);
-    const uint64_t pairs = (uint64_t)F * ns;
+    const uint64_t pairs = (uint64_t)n_lists * ns;
     const uint32_t oblocks = (uint32_t)std::min<uint64_t>((pairs + 255) / 256, (uint64_t)sms * 8);
     const uint32_t wblocks = (uint32_t)std::min<uint64_t>(items, (uint64_t)sms * 8);
     if (ib == 2) {
@@ -345,7 +369,7 @@ int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident,
 
 int bootstrap_compact(const ct_problem* p, const ct_lists* l, uint32_t slot, uint32_t tree, uint32_t* n_in_dev,
                       void* ws, size_t wsb, cudaStream_t st) {
-  return bootstrap_many(p, l, slot, 1, tree, p->presort, 0xffffffffu, n_in_dev, ws, wsb, st);
+  return bootstrap_many(p, l, slot, 1, tree, p->presort, 0xffffffffu, 0, n_in_dev, ws, wsb, st);
 }
 
 }  // namespace ct

@@ -23,7 +23,7 @@ namespace ct {
 
 size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_slots);
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
-                   const void* src, uint32_t row_mask, uint32_t* n_in_dev, void* ws, size_t wsb,
+                   const void* src, uint32_t row_mask, uint64_t skip, uint32_t* n_in_dev, void* ws, size_t wsb,
                    cudaStream_t st);
 int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, cudaStream_t st);
 
@@ -257,9 +257,9 @@ int check_boot_error(const FitLayout& L, cudaStream_t st) {
   return CT_OK;
 }
 
-void account_bootstrap(const ct_problem* p) {
+void account_bootstrap(const ct_problem* p, uint64_t skip) {
   Prof* pf = current_prof();
-  const double w = p->index_bytes, n = p->n_rows, f = p->n_features;
+  const double w = p->index_bytes, n = p->n_rows, f = p->n_features - (p->bootstrap ? __builtin_popcountll(skip) : 0);
   // read presort + gather mark, write the in-bag part (about 0.632 n per feature)
   pf->stats.bytes[CT_K_BOOTSTRAP] += n * f * (w + 1.0) + (p->bootstrap ? 0.632 : 1.0) * n * f * w;
   pf->launched(CT_K_BOOTSTRAP, p->bootstrap ? 3 : 1);
@@ -702,9 +702,10 @@ int fit_batched(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uin
   current_prof()->begin(CT_K_BOOTSTRAP);
   const void* src = nullptr;
   CT_TRY(seed_source(p, l, v, &src, st));
-  CT_TRY(bootstrap_many(p, l, 0, n_trees, first_tree, src, v.row_mask, L.n_in, L.boot_ws, L.boot_bytes, st));
+  CT_TRY(bootstrap_many(p, l, 0, n_trees, first_tree, src, v.row_mask, virtual_skip(v), L.n_in, L.boot_ws,
+                        L.boot_bytes, st));
   current_prof()->end();
-  for (uint32_t s = 0; s < n_trees; ++s) account_bootstrap(p);
+  for (uint32_t s = 0; s < n_trees; ++s) account_bootstrap(p, virtual_skip(v));
   CT_TRY(check_boot_error(L, st));
   begin_level(L.s.ctr, st);
   CT_TRY(root(p, v, L, 0, n_trees, first_tree, tv, 0, st));
@@ -761,9 +762,10 @@ int fit_plain(const ct_problem* p, const ct_lists* l, uint32_t first_tree, uint3
     current_prof()->begin(CT_K_BOOTSTRAP);
     const void* src = nullptr;  // packed again per tree: the previous tree's steps wrote buffer 1
     CT_TRY(seed_source(p, l, v, &src, st));
-    CT_TRY(bootstrap_many(p, l, 0, 1, first_tree + t, src, v.row_mask, L.n_in, L.boot_ws, L.boot_bytes, st));
+    CT_TRY(bootstrap_many(p, l, 0, 1, first_tree + t, src, v.row_mask, virtual_skip(v), L.n_in, L.boot_ws,
+                          L.boot_bytes, st));
     current_prof()->end();
-    account_bootstrap(p);
+    account_bootstrap(p, virtual_skip(v));
     CT_TRY(check_boot_error(L, st));
     begin_level(L.s.ctr, st);
     CT_TRY(root(p, v, L, 0, 1, first_tree + t, tv, 0, st));
@@ -1335,8 +1337,8 @@ int fit_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options* o, 
       const void* src = nullptr;
       CT_TRY(seed_source(&jb.problem, &jb.lists, views[j], &src, st));
       CT_TRY(bootstrap_many(&jb.problem, &jb.lists, 0, jb.n_trees, jb.first_tree, src, views[j].row_mask,
-                            L.n_in + first_slot[j], L.boot_ws, L.boot_bytes, st));
-      for (uint32_t t = 0; t < jb.n_trees; ++t) account_bootstrap(&jb.problem);
+                            virtual_skip(views[j]), L.n_in + first_slot[j], L.boot_ws, L.boot_bytes, st));
+      for (uint32_t t = 0; t < jb.n_trees; ++t) account_bootstrap(&jb.problem, virtual_skip(views[j]));
     }
     current_prof()->end();
     CT_TRY(check_boot_error(L, st));
