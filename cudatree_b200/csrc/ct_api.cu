@@ -152,7 +152,7 @@ int ct_split_nodes(const ct_problem* p, const ct_lists* lists, const ct_node* no
     CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
     s.result = out;
     CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
-    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, totals, nullptr, nullptr, nullptr, nullptr}, st));
+    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, totals, nullptr, nullptr, nullptr, nullptr, DEFAULT_SCAN_PIECE}, st));
     CT_TRY(launch_split(v, p->index_bytes, p->label_bytes, s, LevelBounds{n_nodes, total}, DEFAULT_SCAN_PIECE, false,
                         st));
     if (selected)
@@ -188,7 +188,7 @@ int ct_partition_nodes(const ct_problem* p, const ct_lists* lists, const ct_node
     CT_TRY(carve_api_scratch(p, lists, n_nodes, total, workspace, workspace_bytes, &v, &s));
     s.result = const_cast<ct_split_result*>(splits);
     CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
-    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, nullptr, nullptr, nullptr, nullptr, nullptr}, st));
+    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, nullptr, nullptr, nullptr, nullptr, nullptr, DEFAULT_SCAN_PIECE}, st));
     TreeView tv;
     std::memset(&tv, 0, sizeof(tv));
     CT_TRY(launch_partition(v, p->index_bytes, p->label_bytes, s, LevelBounds{n_nodes, total}, tv, false, st));

@@ -143,6 +143,7 @@ struct LoopCtl {
   unsigned long long split_total;
   unsigned long long part_elems;
   unsigned long long vrows;
+  unsigned long long level_samples;  // samples of the current level (its scan piece)
 };
 
 struct FitLayout {
@@ -150,6 +151,7 @@ struct FitLayout {
   uint32_t cap_list;
   uint32_t chunk;
   uint32_t scan_piece;
+  uint32_t mat16;        // 16 x the lists a node's split scan reads on average (step_piece)
   uint32_t subtree_cut;  // nodes of at most this many rows are grown by warp subtrees (0: off)
   uint32_t cap_small;
   bool host_loop;        // batched form: per-level host round trips instead of the loop graph
@@ -214,7 +216,8 @@ bool layout(const ct_problem* p, uint32_t n_trees, const ct_fit_options* o, char
   }
   L->boot_bytes = bootstrap_scratch_bytes(p->n_rows, p->n_features, slots);
   L->boot_ws = a.take<char>(L->boot_bytes);
-  LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, S});
+  L->mat16 = 16 * std::min(p->max_features, p->n_features);
+  LevelCaps caps = level_caps(v, step_piece(0, L->scan_piece, 1), LevelBounds{L->chunk, S});
   carve_level_scratch(a, v, caps, &L->s, L->virt);
   L->s.huge_rows = o->huge_rows ? o->huge_rows : HUGE_SEG;
   L->s.part_shape = o->part_shape;
@@ -308,8 +311,9 @@ int flush_subtrees(const ct_problem* p, const View& v, const FitLayout& L, const
 }
 
 // The lists of a step over list[cur][lo..): children go to list[1 - cur].
-StepLists step_lists(const FitLayout& L, int cur, uint32_t lo, uint32_t C) {
+StepLists step_lists(const FitLayout& L, int cur, uint32_t lo, uint32_t C, uint64_t level_samples) {
   StepLists sl;
+  sl.scan_piece = step_piece(level_samples, L.scan_piece, L.mat16);
   sl.nodes = L.list[cur] + lo;
   sl.tot = L.tot[cur] + (size_t)lo * C;
   sl.node_mask = L.mask[cur] ? L.mask[cur] + (size_t)lo * L.mask_words : nullptr;
@@ -327,7 +331,7 @@ int step(const ct_problem* p, const View& v, const FitLayout& L, const TreeView&
     const uint32_t cn = std::min(L.chunk, n - lo);
     const LevelBounds b{cn, total};
     if (L.subtree_cut && L.small_bound + 2ull * cn > L.cap_small) CT_TRY(flush_subtrees(p, v, L, tv, st));
-    CT_TRY(launch_reset_step(L.s, cn, step_lists(L, cur, lo, C), st));
+    CT_TRY(launch_reset_step(L.s, cn, step_lists(L, cur, lo, C, total), st));
     // Persistent split and children launches (at most the resident blocks):
     // their grids would otherwise be sized by the capacity bounds, most of
     // whose warps find no item.  The mark fill keeps one warp per piece.
@@ -390,13 +394,15 @@ __global__ void k_loop_init(LoopCtl* ctl, Counters* c, uint32_t cap_list, cudaGr
   ctl->split_total = 0;
   ctl->part_elems = 0;
   ctl->vrows = 0;
+  ctl->level_samples = c->next_total;
   reset_level_counters(c);
   c->claim[ITEM_SUBTREE] = 0;
   c->claim[ITEM_SUBTREE_WIDE] = 0;
   cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
 }
 
-__global__ void k_loop_step(LoopCtl* ctl, Counters* c, StepLists* step, LoopLists ll, uint32_t chunk, uint32_t C) {
+__global__ void k_loop_step(LoopCtl* ctl, Counters* c, StepLists* step, LoopLists ll, uint32_t chunk, uint32_t C,
+                            uint32_t scan_piece, uint32_t mat16) {
   const uint32_t cur = ctl->cur, lo = ctl->lo;
   reset_step_counters(c, min(chunk, ctl->n_level - lo));
   StepLists sl;
@@ -406,6 +412,7 @@ __global__ void k_loop_step(LoopCtl* ctl, Counters* c, StepLists* step, LoopList
   sl.next = ll.list[cur ^ 1u];
   sl.next_tot = ll.tot[cur ^ 1u];
   sl.next_mask = ll.mask[cur ^ 1u];
+  sl.scan_piece = step_piece(ctl->level_samples, scan_piece, mat16);
   *step = sl;
 }
 
@@ -429,6 +436,7 @@ __global__ void k_loop_end(LoopCtl* ctl, Counters* c, uint32_t chunk, uint32_t c
   ctl->n_level = n;
   ctl->cur ^= 1u;
   ctl->lo = 0;
+  ctl->level_samples = c->next_total;
   reset_level_counters(c);
   cudaGraphSetConditional(h, n > 0 ? 1u : 0u);
 }
@@ -521,7 +529,7 @@ int build_loop_graph(const ct_problem* p, const View& v, const FitLayout& L, con
   CT_CUDA_TRY(cudaGraphAddNode(&loop, lg.graph, &init, 1, &cp));
   const ct_kernel_stats s1 = pf->stats;
   CT_TRY(capture_into(cp.conditional.phGraph_out[0], nullptr, st, [&]() -> int {
-    k_loop_step<<<1, 1, 0, st>>>(L.ctl, L.s.ctr, L.s.step, ll, L.chunk, C);
+    k_loop_step<<<1, 1, 0, st>>>(L.ctl, L.s.ctr, L.s.step, ll, L.chunk, C, L.scan_piece, L.mat16);
     pf->launched(CT_K_CHILDREN);
     CT_TRY(launch_split(v, ib, lb, L.s, b, L.scan_piece, true, st));
     CT_TRY(launch_partition(v, ib, lb, L.s, b, tv, true, st));
@@ -569,6 +577,7 @@ int graph_level_loop(const ct_problem* p, const View& v, const FitLayout& L, con
   key_add(key, L.chunk);
   key_add(key, L.n_slots);
   key_add(key, L.scan_piece);
+  key_add(key, L.mat16);
   key_add(key, L.subtree_cut);
   LoopGraph& lg = t_loop_graph;
   if (!lg.exec || lg.key != key) {
@@ -677,6 +686,9 @@ int prepare_features(const ct_problem* p, FitLayout* L, View* v, cudaStream_t st
   if (!vm) return CT_OK;
   v->vmask = vm;
   v->vslot = (uint32_t)__builtin_ctzll(vm);
+  // virtual features make no scan pieces: a node scans m (F - virtual) / F lists on average
+  const uint64_t mat = (uint64_t)p->n_features - (uint64_t)__builtin_popcountll(vm);
+  L->mat16 = (uint32_t)std::max<uint64_t>(1, 16ull * std::min(p->max_features, p->n_features) * mat / p->n_features);
   v->vrow = Lc.vrow;
   v->vval = Lc.vval;
   return virtual_rows(p->x_fm, p->n_rows, vm, Lc.vval, Lc.vrow, st);
@@ -1224,7 +1236,8 @@ bool layout_queue(const ct_fit_job* jobs, uint32_t n_jobs, const ct_fit_options*
   }
   L->boot_bytes = q.boot_bytes;
   L->boot_ws = a.take<char>(L->boot_bytes);
-  LevelCaps caps = level_caps(v, L->scan_piece, LevelBounds{L->chunk, q.samples});
+  L->mat16 = 16 * q.m_max;
+  LevelCaps caps = level_caps(v, step_piece(0, L->scan_piece, 1), LevelBounds{L->chunk, q.samples});
   carve_level_scratch(a, v, caps, &L->s, false);
   // jobs of different row counts have mark bits of different sizes: no shared-memory staging
   L->s.huge_segs = nullptr;

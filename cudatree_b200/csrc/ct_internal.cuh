@@ -346,6 +346,7 @@ struct StepLists {
   ct_node* next;              // the next level's list: children are appended
   uint32_t* next_tot;         // their class totals
   uint64_t* next_mask;        // their masks, or NULL
+  uint32_t scan_piece;        // elements per split-scan piece in this step
 };
 
 // Scratch of one level step, carved from the caller's workspace.
@@ -465,6 +466,18 @@ struct Arena {
 
 // Tile shapes.
 constexpr uint32_t DEFAULT_SCAN_PIECE = 2048;   // elements per split-scan work item
+// Split-scan piece of a fit's level of `samples` samples whose nodes scan
+// mat16 / 16 lists each on average: the fit's piece, halved (not below
+// MIN_STEP_PIECE) while the level would make fewer than STEP_PIECES pieces,
+// so that a small level does not wait on a few warps' long pieces.  The
+// pieces do not change the result.  samples = 0 gives the smallest piece a
+// fit can use (its scratch capacities).
+constexpr uint32_t MIN_STEP_PIECE = 512;
+constexpr uint64_t STEP_PIECES = 12288;
+__host__ __device__ __forceinline__ uint32_t step_piece(uint64_t samples, uint32_t piece, uint32_t mat16) {
+  while (piece >= 2 * MIN_STEP_PIECE && (uint64_t)mat16 * samples < 16 * STEP_PIECES * piece) piece >>= 1;
+  return piece;
+}
 constexpr uint32_t PART_ROUNDS = 16;            // rounds of 32 held in registers
 constexpr uint32_t PART_PIECE = 32 * PART_ROUNDS;
 constexpr uint32_t TILE_ELEMS = 4096;           // partition tile of big segments

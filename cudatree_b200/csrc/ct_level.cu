@@ -277,10 +277,10 @@ __device__ __forceinline__ void select_item(const View& vb, const StepLists& lis
 }
 
 template <typename IdxT, bool Q>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_select(View v, LevelScratch s, uint32_t scan_piece) {
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_select(View v, LevelScratch s) {
   const uint32_t count = min(s.ctr->n_nodes, s.cap_nodes);
   const StepLists sl = *s.step;
-  for_items(count, &s.ctr->claim[ITEM_SELECT], [&](uint32_t w) { select_item<IdxT, Q>(v, sl, s, scan_piece, w); });
+  for_items(count, &s.ctr->claim[ITEM_SELECT], [&](uint32_t w) { select_item<IdxT, Q>(v, sl, s, sl.scan_piece, w); });
 }
 
 // ------------------------------------------------------------------------
@@ -343,13 +343,13 @@ __device__ __forceinline__ void scan_hist_item(const View& vb, const StepLists& 
 }
 
 template <typename IdxT, typename LabT, bool Q>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_hist(View v, LevelScratch s, uint32_t scan_piece) {
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_hist(View v, LevelScratch s) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_carry, s.cap_carry);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_HIST],
-            [&](uint32_t i) { scan_hist_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, s.carry_piece[i]); });
+            [&](uint32_t i) { scan_hist_item<IdxT, LabT, Q>(v, sl, s, sl.scan_piece, cnt, s.carry_piece[i]); });
 }
 
 __device__ __forceinline__ void scan_carry_item(const LevelScratch& s, uint32_t C, uint32_t pi) {
@@ -472,13 +472,13 @@ __device__ __forceinline__ void two_valued_item(const View& vb, const StepLists&
 }
 
 template <typename IdxT, typename LabT, bool Q>
-__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_two_valued(View v, LevelScratch s, uint32_t scan_piece) {
+__global__ void __launch_bounds__(THREADS_PER_BLOCK) k_scan_two_valued(View v, LevelScratch s) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_tv, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_TWO_VALUED],
-            [&](uint32_t i) { two_valued_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, s.tv_pieces[i]); });
+            [&](uint32_t i) { two_valued_item<IdxT, LabT, Q>(v, sl, s, sl.scan_piece, cnt, s.tv_pieces[i]); });
 }
 
 // ------------------------------------------------------------------------
@@ -630,13 +630,13 @@ __device__ __forceinline__ void split_scan_item(const View& vb, const StepLists&
 
 template <typename IdxT, typename LabT, bool Q>
 __global__ void __launch_bounds__(THREADS_PER_BLOCK, 7)  // 72 registers: 28 warps per SM hide more of the scan's latency
-k_split_scan(View v, LevelScratch s, uint32_t scan_piece) {
+k_split_scan(View v, LevelScratch s) {
   extern __shared__ uint32_t smem[];
   uint32_t* cnt = smem + (threadIdx.x >> 5) * 2 * v.n_classes;
   const uint32_t count = live_count(s, s.ctr->n_scan_pieces, s.cap_scan);
   const StepLists sl = *s.step;
   for_items(count, &s.ctr->claim[ITEM_SCAN],
-            [&](uint32_t pi) { split_scan_item<IdxT, LabT, Q>(v, sl, s, scan_piece, cnt, pi); });
+            [&](uint32_t pi) { split_scan_item<IdxT, LabT, Q>(v, sl, s, sl.scan_piece, cnt, pi); });
 }
 
 // ------------------------------------------------------------------------
@@ -1606,18 +1606,18 @@ void split_impl(const View& v, const LevelScratch& s, const LevelCaps& caps, uin
     pf->launched(CT_K_SCAN, 2);
   }
   pf->begin(CT_K_SELECT);
-  k_select<IdxT, Q><<<grid_for(k_select<IdxT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s, scan_piece);
+  k_select<IdxT, Q><<<grid_for(k_select<IdxT, Q>, caps.nodes, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(v, s);
   pf->end();
   pf->launched(CT_K_SELECT);
   pf->begin(CT_K_SCAN);
   k_scan_hist<IdxT, LabT, Q><<<grid_for(k_scan_hist<IdxT, LabT, Q>, caps.carry, sm1, persistent), THREADS_PER_BLOCK,
-                            sm1, st>>>(v, s, scan_piece);
+                            sm1, st>>>(v, s);
   k_scan_carry<<<grid_for(k_scan_carry, caps.carry, 0, persistent), THREADS_PER_BLOCK, 0, st>>>(s, v.n_classes);
   k_split_scan<IdxT, LabT, Q><<<grid_for(k_split_scan<IdxT, LabT, Q>, caps.scan, 2 * sm1, persistent), THREADS_PER_BLOCK,
-                             2 * sm1, st>>>(v, s, scan_piece);
+                             2 * sm1, st>>>(v, s);
   if (v.fbin)
     k_scan_two_valued<IdxT, LabT, Q><<<grid_for(k_scan_two_valued<IdxT, LabT, Q>, caps.scan, sm1, persistent),
-                                    THREADS_PER_BLOCK, sm1, st>>>(v, s, scan_piece);
+                                    THREADS_PER_BLOCK, sm1, st>>>(v, s);
   pf->end();
   pf->launched(CT_K_SCAN, v.fbin ? 4 : 3);
   pf->begin(CT_K_REDUCE);

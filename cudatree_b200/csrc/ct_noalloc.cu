@@ -74,7 +74,7 @@ extern "C" int ct_split_nodes_noalloc(const ct_problem* p, const ct_lists* lists
     }
     s.result = out;
     CT_CUDA_TRY(cudaMemsetAsync(s.ctr, 0, sizeof(Counters), st));
-    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, totals, nullptr, nullptr, nullptr, nullptr}, st));
+    CT_TRY(launch_reset_step(s, n_nodes, StepLists{nodes, totals, nullptr, nullptr, nullptr, nullptr, DEFAULT_SCAN_PIECE}, st));
     CT_TRY(launch_split(v, p->index_bytes, p->label_bytes, s, b, DEFAULT_SCAN_PIECE, false, st));
     Counters h;
     CT_CUDA_TRY(cudaMemcpyAsync(&h, s.ctr, sizeof(h), cudaMemcpyDeviceToHost, st));
