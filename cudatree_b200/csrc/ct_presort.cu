@@ -9,6 +9,11 @@
 //                 then per-digit prefix over the tile's warps.
 // A stable sort of keys that start in row order gives ties in row order,
 // which is the tie rule the split search and the leaf labels rely on.
+// Features with at most two distinct keys (one-hot and other binary columns;
+// feature_flags finds them) take one pass instead of four: the same three
+// kernels with the digit "key is the feature's larger key", a stable
+// partition of the rows in row order.  Each kernel's blocks of the other kind
+// of feature return at once.
 #include "ct_internal.cuh"
 
 namespace ct {
@@ -34,7 +39,18 @@ struct RadixArgs {
   uint32_t first;
   uint32_t last;
   uint32_t index_bytes;
+  uint32_t tv_pass;        // 1: the pass of the two-valued features; 0: a radix pass of the others
+  const uint32_t* two;     // bit f: feature f has at most two distinct keys
+  const uint2* mm;         // per feature: its (smallest, largest) key
 };
+
+__device__ __forceinline__ bool skip_feature(const RadixArgs& a, uint32_t f) {
+  const bool tv = (a.two[f >> 5] >> (f & 31)) & 1u;
+  return tv != (a.tv_pass != 0);
+}
+__device__ __forceinline__ uint32_t digit(const RadixArgs& a, uint32_t f, uint32_t key) {
+  return a.tv_pass ? (key == a.mm[f].y ? 1u : 0u) : (key >> a.shift) & 255u;
+}
 
 __device__ __forceinline__ uint32_t load_key(const RadixArgs& a, uint32_t f, uint32_t i) {
   return a.first ? f32_order(a.x[(size_t)f * a.n + i]) : a.kin[(size_t)f * a.n + i];
@@ -43,22 +59,23 @@ __device__ __forceinline__ uint32_t load_key(const RadixArgs& a, uint32_t f, uin
 __global__ void __launch_bounds__(RS_THREADS) k_digit_hist(RadixArgs a) {
   __shared__ uint32_t h[256];
   const uint32_t tile = blockIdx.x, f = blockIdx.y;
+  if (skip_feature(a, f)) return;
   for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x) h[d] = 0;
   __syncthreads();
   const uint32_t lo = tile * RS_TILE, hi = min(lo + RS_TILE, a.n);
   for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const uint32_t d = (load_key(a, f, i) >> a.shift) & 255u;
-    atomicAdd(&h[d], 1u);
+    atomicAdd(&h[digit(a, f, load_key(a, f, i))], 1u);
   }
   __syncthreads();
   for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x)
     a.hist[((size_t)f * 256 + d) * a.tiles + tile] = h[d];
 }
 
-__global__ void __launch_bounds__(1024) k_digit_scan(uint32_t* hist, uint32_t tiles) {
+__global__ void __launch_bounds__(1024) k_digit_scan(RadixArgs a) {
   __shared__ uint32_t warp_tot[32];
-  const uint32_t f = blockIdx.x;
-  uint32_t* row = hist + (size_t)f * 256 * tiles;
+  const uint32_t f = blockIdx.x, tiles = a.tiles;
+  if (skip_feature(a, f)) return;
+  uint32_t* row = a.hist + (size_t)f * 256 * tiles;
   const uint32_t L = 256 * tiles;
   const uint32_t per = (L + blockDim.x - 1) / blockDim.x;
   const uint32_t lo = min(threadIdx.x * per, L), hi = min(lo + per, L);
@@ -95,6 +112,7 @@ __global__ void __launch_bounds__(1024) k_digit_scan(uint32_t* hist, uint32_t ti
 __global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
   __shared__ uint32_t wcnt[RS_WARPS][256];
   const uint32_t tile = blockIdx.x, f = blockIdx.y;
+  if (skip_feature(a, f)) return;
   const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint32_t d = lane; d < 256; d += 32) wcnt[warp][d] = 0;
   __syncwarp();
@@ -107,7 +125,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
     const bool ok = i < a.n;
     key[r] = ok ? load_key(a, f, i) : 0xffffffffu;
     val[r] = ok ? (a.first ? i : a.vin[(size_t)f * a.n + i]) : 0u;
-    const uint32_t d = ok ? (key[r] >> a.shift) & 255u : 256u;
+    const uint32_t d = ok ? digit(a, f, key[r]) : 256u;
     const unsigned grp = __match_any_sync(FULL, d);
     rank[r] = ok ? wcnt[warp][d] + __popc(grp & lt) : 0u;
     __syncwarp();
@@ -130,7 +148,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_digit_move(RadixArgs a) {
   for (int r = 0; r < RS_ROUNDS; ++r) {
     const uint32_t i = lo + r * 32 + lane;
     if (i >= a.n) continue;
-    const uint32_t d = (key[r] >> a.shift) & 255u;
+    const uint32_t d = digit(a, f, key[r]);
     const uint32_t dst = wcnt[warp][d] + rank[r];
     if (dst >= a.n) continue;
     if (a.last) {
@@ -178,7 +196,8 @@ __global__ void k_transpose(const float* __restrict__ in, uint32_t n_rows, uint3
 size_t presort_workspace_bytes(uint32_t n_rows, uint32_t n_features) {
   const size_t tiles = ceil_div(n_rows, RS_TILE);
   const size_t elems = (size_t)n_rows * n_features;
-  return 4 * elems * sizeof(uint32_t) + (size_t)n_features * 256 * tiles * sizeof(uint32_t) + 5 * 256;
+  return 4 * elems * sizeof(uint32_t) + (size_t)n_features * 256 * tiles * sizeof(uint32_t) +
+         ((n_features + 31) / 32) * sizeof(uint32_t) + feature_flags_work_bytes(n_features) + 7 * 256;
 }
 
 int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t index_bytes, void* out, void* ws,
@@ -194,7 +213,9 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
   uint32_t* k1 = ar.take<uint32_t>(elems);
   uint32_t* v1 = ar.take<uint32_t>(elems);
   uint32_t* hist = ar.take<uint32_t>((size_t)n_features * 256 * tiles);
-  if (!hist) {
+  uint32_t* two = ar.take<uint32_t>((n_features + 31) / 32);
+  char* ffw = ar.take<char>(feature_flags_work_bytes(n_features));  // starts with the (min, max) keys
+  if (!hist || !two || !ffw) {
     set_last_error("presort workspace too small");
     return CT_ERR_OOM;
   }
@@ -205,6 +226,10 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
   a.n = n_rows;
   a.tiles = tiles;
   a.index_bytes = index_bytes;
+  CT_TRY(feature_flags(x_fm, n_rows, n_features, two, nullptr, ffw, st));
+  a.two = two;
+  a.mm = reinterpret_cast<const uint2*>(ffw);
+  a.tv_pass = 0;
   const dim3 grid(tiles, n_features);
   for (uint32_t pass = 0; pass < 4; ++pass) {
     a.shift = pass * 8;
@@ -215,9 +240,17 @@ int presort(const float* x_fm, uint32_t n_rows, uint32_t n_features, uint32_t in
     a.kout = (pass & 1) ? k1 : k0;
     a.vout = (pass & 1) ? v1 : v0;
     k_digit_hist<<<grid, RS_THREADS, 0, st>>>(a);
-    k_digit_scan<<<n_features, 1024, 0, st>>>(hist, tiles);
+    k_digit_scan<<<n_features, 1024, 0, st>>>(a);
     k_digit_move<<<grid, RS_THREADS, 0, st>>>(a);
   }
+  // the two-valued features: one stable partition pass from x to the output
+  a.tv_pass = 1;
+  a.shift = 0;
+  a.first = 1;
+  a.last = 1;
+  k_digit_hist<<<grid, RS_THREADS, 0, st>>>(a);
+  k_digit_scan<<<n_features, 1024, 0, st>>>(a);
+  k_digit_move<<<grid, RS_THREADS, 0, st>>>(a);
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;
 }

@@ -27,10 +27,16 @@ def _data(n, f, c, seed, integer=True):
 @pytest.mark.parametrize("index_bytes", [2, 4])
 def test_presort_stable(cuda_device, index_bytes):
     rng = np.random.default_rng(1)
-    n, f = 9000, 5
+    n, f = 9000, 9
     x = rng.integers(-3, 4, size=(n, f)).astype(np.float32)
     x[rng.random((n, f)) < 0.1] = -0.0
     x[:, 4] = rng.normal(size=n).astype(np.float32) * 1e30
+    # columns of at most two distinct values take the one-pass partition:
+    # one-hot, constant, {-0.0, +0.0, 3} (two keys once -0.0 folds onto +0.0), {-1, 1}
+    x[:, 5] = (rng.random(n) < 0.3).astype(np.float32)
+    x[:, 6] = 2.5
+    x[:, 7] = rng.choice(np.array([-0.0, 0.0, 3.0], np.float32), size=n)
+    x[:, 8] = rng.choice(np.array([-1.0, 1.0], np.float32), size=n)
     gp = G.GpuProblem(x, np.zeros(n, np.int64), 1, 1, index_bytes=index_bytes)
     np.testing.assert_array_equal(gp.presort_np(), O.presort(gp.x_fm_np))
 
