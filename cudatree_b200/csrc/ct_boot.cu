@@ -223,21 +223,24 @@ template <typename IdxT, typename LabT>
 // Feature `ident` (NONE: none) gets the rows in row order instead of its
 // presort: the row list of the virtual features (View::vslot).
 __global__ void k_pack_presort(const IdxT* __restrict__ in, const LabT* __restrict__ labels, IdxT* __restrict__ out,
-                               uint64_t count, uint32_t shift, uint32_t n_rows, uint32_t ident) {
+                               uint64_t count, uint32_t shift, uint32_t n_rows, uint32_t ident, uint64_t skip) {
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (uint64_t)gridDim.x * blockDim.x) {
     const uint32_t f = (uint32_t)(i / n_rows);
+    if (f < 64 && ((skip >> f) & 1ull)) continue;  // a list nothing reads
     const uint32_t r = f == ident ? (uint32_t)(i - (uint64_t)f * n_rows) : (uint32_t)in[i];
     out[i] = (IdxT)(r | ((uint32_t)__ldg(labels + r) << shift));
   }
 }
 
 template <typename IdxT, typename LabT>
-void launch_pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, cudaStream_t st) {
+void launch_pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, uint64_t skip,
+                         cudaStream_t st) {
   const uint64_t count = (uint64_t)p->n_rows * p->n_features;
   const uint32_t blocks = (uint32_t)std::min<uint64_t>((count + 255) / 256, 148u * 16u);
   k_pack_presort<IdxT, LabT><<<blocks, 256, 0, st>>>(reinterpret_cast<const IdxT*>(p->presort),
                                                      reinterpret_cast<const LabT*>(p->labels),
-                                                     reinterpret_cast<IdxT*>(out), count, shift, p->n_rows, ident);
+                                                     reinterpret_cast<IdxT*>(out), count, shift, p->n_rows, ident,
+                                                     skip);
 }
 
 struct BootLayout {
@@ -353,15 +356,17 @@ int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uin
 }
 
 // The presort with each row's label above its row id (entry row | label <<
-// shift), [F][N] at out; out must not overlap the presort.
-int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, cudaStream_t st) {
+// shift), [F][N] at out; out must not overlap the presort.  Feature ident's
+// list is the rows in row order; the lists of the features in skip (below 64)
+// are left unwritten.
+int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, uint64_t skip, cudaStream_t st) {
   CT_ARG_CHECK(p->presort != nullptr, "presort is NULL");
   if (p->index_bytes == 2) {
-    if (p->label_bytes == 1) launch_pack_presort<uint16_t, uint8_t>(p, out, shift, ident, st);
-    else launch_pack_presort<uint16_t, uint16_t>(p, out, shift, ident, st);
+    if (p->label_bytes == 1) launch_pack_presort<uint16_t, uint8_t>(p, out, shift, ident, skip, st);
+    else launch_pack_presort<uint16_t, uint16_t>(p, out, shift, ident, skip, st);
   } else {
-    if (p->label_bytes == 1) launch_pack_presort<uint32_t, uint8_t>(p, out, shift, ident, st);
-    else launch_pack_presort<uint32_t, uint16_t>(p, out, shift, ident, st);
+    if (p->label_bytes == 1) launch_pack_presort<uint32_t, uint8_t>(p, out, shift, ident, skip, st);
+    else launch_pack_presort<uint32_t, uint16_t>(p, out, shift, ident, skip, st);
   }
   CT_CUDA_TRY(cudaGetLastError());
   return CT_OK;

@@ -25,7 +25,7 @@ size_t bootstrap_scratch_bytes(uint32_t n_rows, uint32_t n_features, uint32_t n_
 int bootstrap_many(const ct_problem* p, const ct_lists* l, uint32_t slot_lo, uint32_t n_slots, uint32_t tree_lo,
                    const void* src, uint32_t row_mask, uint64_t skip, uint32_t* n_in_dev, void* ws, size_t wsb,
                    cudaStream_t st);
-int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, cudaStream_t st);
+int pack_presort(const ct_problem* p, void* out, uint32_t shift, uint32_t ident, uint64_t skip, cudaStream_t st);
 
 namespace {
 
@@ -697,7 +697,7 @@ int prepare_features(const ct_problem* p, FitLayout* L, View* v, cudaStream_t st
 int seed_source(const ct_problem* p, const ct_lists* l, const View& v, const void** src, cudaStream_t st) {
   *src = p->presort;
   if (v.lab_shift) {
-    CT_TRY(pack_presort(p, l->si1, v.lab_shift, v.vmask ? v.vslot : NONE, st));
+    CT_TRY(pack_presort(p, l->si1, v.lab_shift, v.vmask ? v.vslot : NONE, virtual_skip(v), st));
     *src = l->si1;
   }
   return CT_OK;
