@@ -62,9 +62,10 @@ typedef struct ct_problem {
  * starts at si[b] + ((size_t)s * n_features + f) * stride elements.  mark
  * holds the [n_slots][n_rows] byte mark table (reference mark_table,
  * random_forest.py:168; the bootstrap's in-bag marks) followed, at the next
- * 256-byte boundary, by the packed [n_slots][bit_words] uint32 left flags
- * that the partition reads (a split's mark fill sets and clears them
- * directly); ct_mark_bytes gives the size. */
+ * 256-byte boundary, by the packed [n_slots][bit_words] uint32 flags that
+ * the partition reads: scratch of each partition call, which clears them
+ * and sets the left rows of its splits (a forest queue's batch sets left
+ * rows and clears right ones); ct_mark_bytes gives the size. */
 /* The partition and compaction kernels copy index tiles with 16-byte TMA
  * bulk copies and may read up to 15 bytes past the last element of the
  * si0/si1 buffers and of the presort: allocate them with >= 16 bytes of
