@@ -1071,18 +1071,22 @@ __global__ void k_gather_trees(ct_tree_buffers tb, const uint32_t* __restrict__ 
 
 // Page-locked staging for the raw read-back, shared by the process and grown
 // on demand (portable across devices).  Page-locked allocation synchronizes
-// the device, so a server reserves its largest size up front.
+// the device and takes tens of ms for a 100-tree forest, so a server reserves
+// its largest size up front, and a growth takes half again the old size
+// (16 MiB steps): forests a little larger than the last do not reallocate.
 struct Staging {
   std::mutex mu;
   void* p = nullptr;
   size_t bytes = 0;
   int grow(size_t need) {  // caller holds mu
     if (bytes >= need) return CT_OK;
+    constexpr size_t STEP = size_t(16) << 20;
+    const size_t want = (std::max(need, bytes + bytes / 2) + STEP - 1) / STEP * STEP;
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
-    CT_CUDA_TRY(cudaHostAlloc(&p, need, cudaHostAllocPortable));
-    bytes = need;
+    CT_CUDA_TRY(cudaHostAlloc(&p, want, cudaHostAllocPortable));
+    bytes = want;
     return CT_OK;
   }
 };
